@@ -1,0 +1,345 @@
+"""Benchmark: Fibonacci STARK proofs/s on B200 (log_n = 24, blowup 4, 80 queries).
+
+One step = one whole proof of the Fibonacci AIR at 2^24 rows (2^26-point
+circle LDE): trace, LDE, trace / quotient / FRI commitments, transcript,
+queries and decommitment, on the device.
+
+  value    proofs/s with the proof state resident in HBM (device path:
+           vx_prover_prove_async back to back on one stream), all ranks.
+  e2e      the same metric through the C ABI with a host buffer
+           (vx_prove_fib: launch, run, copy the proof bytes to the host).
+  p50/p99  per-proof latency of the e2e loop, ms.
+  roofline LDE (interpolate + zero-pad + evaluate) against the measured HBM
+           copy bandwidth; roofline_alu: the trace commitment (Blake2s)
+           against a register-only Blake2s probe on the same GPU.
+
+N > 1 (torchrun): independent replicas, one per GPU, no collective on the
+data path ("replicas only"); barrier + max-over-ranks timing.
+``--impl reference`` times the CPU oracle (a C restatement of the reference's
+path, OpenMP over all host cores) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Fib STARK proofs/s + p50/p99 prove ms, mixed log_n 16-24; LDE HBM GB/s"
+SEED = 0x5EED_2024
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append(parts)
+            except Exception:
+                pass
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(log_n: int):
+    """One proof of the same workload with the CPU oracle on all host cores."""
+    from oracle import oracle as O
+    from vortexstark_b200.workload import fib_inputs
+
+    O.lib()
+    cores = O.get_threads()
+    a, b = fib_inputs(SEED ^ 0xC0FFEE, 1)[0]
+    t0 = time.perf_counter()
+    O.prove(a, b, 20)
+    t20 = time.perf_counter() - t0
+    est = t20 * (1 << (log_n - 20)) * (log_n + 2) / 22.0
+    if est <= 40.0:
+        t0 = time.perf_counter()
+        O.prove(a, b, log_n)
+        dt = time.perf_counter() - t0
+        sample = f"one full log_n={log_n} proof (2^{log_n + 2}-point LDE, 80 queries)"
+        return {"value": 1.0 / dt, "unit": "proofs/s", "cores": cores, "kind": "port", "sample": sample,
+                "seconds": dt}
+    k = log_n - 2
+    t0 = time.perf_counter()
+    O.prove(a, b, k)
+    dt = time.perf_counter() - t0
+    scale = (1 << (log_n - k)) * (log_n + 2) / (k + 2)
+    return {"value": 1.0 / (dt * scale), "unit": "proofs/s", "cores": cores, "kind": "port",
+            "sample": f"one log_n={k} proof ({dt:.2f} s) scaled by the N log N work ratio {scale:.2f} to log_n={log_n}",
+            "seconds": dt}
+
+
+def run_reference(args, rank: int):
+    """CPU oracle arm: each step one proof of the workload (or a bounded
+    sample of it), all host threads."""
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    from vortexstark_b200.workload import fib_inputs
+
+    O.lib()
+    cores = O.get_threads()
+    ins = fib_inputs(SEED, args.steps + args.warmup)
+    for a, b in ins[: args.warmup]:
+        O.prove(a, b, 16)
+    a, b = ins[0]
+    t0 = time.perf_counter()
+    O.prove(a, b, 20)
+    t20 = time.perf_counter() - t0
+    per = t20 * (1 << (args.log_n - 20)) * (args.log_n + 2) / 22.0
+    full = per * args.steps <= 240.0
+    k = args.log_n if full else args.log_n - 2
+    scale = 1.0 if full else (1 << (args.log_n - k)) * (args.log_n + 2) / (k + 2)
+    times = []
+    for a, b in ins[args.warmup:]:
+        t0 = time.perf_counter()
+        O.prove(a, b, k)
+        times.append(time.perf_counter() - t0)
+    total = sum(times) * scale
+    value = args.steps / total
+    sample = (f"each step one full log_n={k} proof" if full else
+              f"each step one log_n={k} proof scaled by the N log N work ratio {scale:.2f} to log_n={args.log_n}")
+    line = {
+        "metric": METRIC, "value": value, "unit": "proofs/s", "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32 (M31)",
+        "data": "synthetic (seeded SplitMix64 public inputs)",
+        "config": {"workload": f"fibonacci_stark log_n={args.log_n} blowup=4 queries=80 (2^{args.log_n + 2}-point LDE)",
+                   "log_n": args.log_n, "blowup_bits": 2, "n_queries": 80, "parallelism": "cpu"},
+        "cpu_baseline": {"value": value, "unit": "proofs/s", "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "proofs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "p50_ms": 1000.0 * statistics.median(times) * scale,
+        "p99_ms": 1000.0 * max(times) * scale,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="vortex", choices=["vortex", "reference"])
+    ap.add_argument("--log-n", type=int, default=24)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    import ctypes as C
+
+    from vortexstark_b200 import _lib, prover
+    from vortexstark_b200.workload import fib_inputs
+
+    L = _lib.lib()
+    log_n = args.log_n
+    cache = prover.ProverCache(log_n)
+    size = cache.size
+    ins = fib_inputs(SEED + rank, args.steps + args.warmup)
+    stream = torch.cuda.Stream()
+    s = stream.cuda_stream
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # warm-up (device path and e2e path)
+    host = torch.empty(size, dtype=torch.uint8, pin_memory=True)
+    out_len = C.c_size_t()
+    for a, b in ins[: args.warmup]:
+        _lib.check(L.vx_prover_prove_async(cache._p, a, b, s))
+        _lib.check(L.vx_prove_fib(a, b, log_n, 2, 80, host.data_ptr(), size, C.byref(out_len)))
+    torch.cuda.synchronize()
+    launches_per_proof = int(L.vx_prover_launches(cache._p))
+
+    clk = ClockSampler(local)
+    clk.start()
+    # ---- device-resident throughput ----
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for a, b in ins[args.warmup:]:
+        _lib.check(L.vx_prover_prove_async(cache._p, a, b, s))
+    e1.record(stream)
+    stream.synchronize()
+    barrier()
+    dev_ms = e0.elapsed_time(e1)
+    _lib.check(L.vx_prover_check(cache._p))
+
+    # ---- end to end through the C ABI, host buffer, per-proof latency ----
+    lat = []
+    t_all = 0.0
+    for a, b in ins[args.warmup:]:
+        ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ea.record(torch.cuda.current_stream())
+        _lib.check(L.vx_prove_fib(a, b, log_n, 2, 80, host.data_ptr(), size, C.byref(out_len)))
+        eb.record(torch.cuda.current_stream())
+        eb.synchronize()
+        ms = ea.elapsed_time(eb)
+        lat.append(ms)
+        t_all += ms
+    barrier()
+    clocks = clk.stop()
+
+    # ---- stage timing: LDE roofline, Merkle ALU roofline ----
+    reps = 5
+    a, b = ins[0]
+    _lib.check(L.vx_prover_stage_async(cache._p, 0, a, b, s))
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * reps)]
+    lde_ms = []
+    for r in range(reps):
+        ev[2 * r].record(stream)
+        _lib.check(L.vx_prover_stage_async(cache._p, 1, a, b, s))
+        _lib.check(L.vx_prover_stage_async(cache._p, 2, a, b, s))
+        ev[2 * r + 1].record(stream)
+        _lib.check(L.vx_prover_stage_async(cache._p, 0, a, b, s))  # regenerate the trace (not timed)
+    stream.synchronize()
+    lde_ms = [ev[2 * r].elapsed_time(ev[2 * r + 1]) for r in range(reps)]
+    n, N = 1 << log_n, 1 << (log_n + 2)
+    lde_bytes = 8 * n + 4 * n + 4 * N
+    lde_t = statistics.median(lde_ms) / 1e3
+    peak, peak_kind = _peaks()
+    lde_gbs = lde_bytes / lde_t / 1e9
+
+    tc = [torch.cuda.Event(enable_timing=True) for _ in range(2 * reps)]
+    for r in range(reps):
+        tc[2 * r].record(stream)
+        _lib.check(L.vx_prover_stage_async(cache._p, 3, a, b, s))
+        tc[2 * r + 1].record(stream)
+    stream.synchronize()
+    tcommit_t = statistics.median([tc[2 * r].elapsed_time(tc[2 * r + 1]) for r in range(reps)]) / 1e3
+    compressions = 2 * N - 1
+    probe_out = torch.empty(148 * 8 * 256, dtype=torch.int32, device="cuda")
+    iters = 256
+    _lib.check(L.vx_probe_blake2s(148 * 8, 256, iters, probe_out.data_ptr(), s))
+    pa, pb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    pa.record(stream)
+    _lib.check(L.vx_probe_blake2s(148 * 8, 256, iters, probe_out.data_ptr(), s))
+    pb.record(stream)
+    stream.synchronize()
+    probe_rate = 148 * 8 * 256 * iters / (pa.elapsed_time(pb) / 1e3)
+    merkle_rate = compressions / tcommit_t
+
+    # max over ranks
+    if dist is not None:
+        t = torch.tensor([dev_ms, t_all], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_ms, t_all = float(t[0]), float(t[1])
+
+    steps = args.steps
+    value = world * steps / (dev_ms / 1e3)
+    e2e = world * steps / (t_all / 1e3)
+    lat.sort()
+    p99 = lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))]
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "proofs/s", "n_gpus": world, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": dev_ms / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32 (M31)", "data": "synthetic (seeded SplitMix64 public inputs)",
+            "config": {"workload": f"fibonacci_stark log_n={log_n} blowup=4 queries=80 (2^{log_n + 2}-point LDE)",
+                       "log_n": log_n, "blowup_bits": 2, "n_queries": 80,
+                       "parallelism": f"replicas x{world}",
+                       "l2": "per-step working set > L2 (LDE 256 MiB + FRI layers 1 GiB); no flush needed"},
+            "e2e": {"value": e2e, "unit": "proofs/s", "h2d_bytes_per_step": 8, "d2h_bytes_per_step": size},
+            "p50_ms": statistics.median(lat), "p99_ms": p99,
+            "lde_hbm_gbs": lde_gbs,
+            "roofline": {"bound": "hbm", "kernel": "LDE (interpolate 2^24 + zero-pad + evaluate 2^26)",
+                         "achieved": lde_gbs, "peak": peak, "unit": "GB/s", "frac": lde_gbs / peak,
+                         "peak_source": peak_kind, "traffic": None,
+                         "algorithmic_bytes": lde_bytes, "time_ms": lde_t * 1e3},
+            "roofline_alu": {"bound": "int-alu (Blake2s)", "kernel": "trace commitment (2^26 leaves)",
+                             "achieved": merkle_rate, "peak": probe_rate, "unit": "compressions/s",
+                             "frac": merkle_rate / probe_rate, "time_ms": tcommit_t * 1e3},
+            "gpu_launches": launches_per_proof * steps,
+            "launches_per_proof": launches_per_proof,
+            "clocks": clocks,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            cb = cpu_baseline(log_n)
+            cb.pop("seconds", None)
+            line["cpu_baseline"] = cb
+        print(json.dumps(line), flush=True)
+    cache.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,225 @@
+/*
+ * vortex_b200.h — C ABI of libvortex_b200.so, the B200 (sm_100a) commitment
+ * path of the VortexSTARK Circle-STARK prover.
+ *
+ * Two groups of entry points:
+ *
+ *  1. Drop-in replacements for the launchers that the reference's Rust FFI
+ *     layer binds (src/cuda/ffi.rs).  Same symbol names, argument order and
+ *     meaning: device pointers for data, host pointers for the small
+ *     parameter arrays (alpha[4], layer offsets), void return, legacy
+ *     default stream unless a `_stream` variant says otherwise.  As in the
+ *     reference, the NTT evaluate/interpolate launchers synchronise the
+ *     device before returning; the others are asynchronous.  A launch
+ *     failure is recorded and can be read with vx_last_error().
+ *
+ *  2. New entry points (prefix vx_) for the device-resident whole-proof
+ *     path: explicit streams, int status codes (VX_OK on success).
+ *
+ * All field data are canonical M31 words (< 2^31 - 1).  QM31 columns are
+ * SoA: four M31 columns.
+ */
+#ifndef VORTEX_B200_H
+#define VORTEX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes of the vx_ API ---- */
+#define VX_OK 0
+#define VX_ERR_ARG 1    /* invalid argument (size, range, null pointer)      */
+#define VX_ERR_CUDA 2   /* a CUDA runtime call failed                        */
+#define VX_ERR_OOM 3    /* device allocation failed                          */
+#define VX_ERR_DEVICE 4 /* a kernel reported an error through its status word */
+
+/* ======================================================================
+ * 1. Reference-compatible launchers (src/cuda/ffi.rs)
+ * ====================================================================== */
+
+/* -- circle NTT, natural order (ffi.rs:260-311; circle_ntt.cu:248-404) -- */
+/* replaces cuda_circle_ntt_evaluate, circle_ntt.cu:248-275 */
+void cuda_circle_ntt_evaluate(uint32_t *d_data, const uint32_t *d_twiddles, const uint32_t *d_circle_twids,
+                              const uint32_t *h_layer_offsets, const uint32_t *h_layer_sizes,
+                              uint32_t n_line_layers, uint32_t n);
+/* replaces cuda_circle_ntt_interpolate, circle_ntt.cu:277-312 */
+void cuda_circle_ntt_interpolate(uint32_t *d_data, const uint32_t *d_itwiddles, const uint32_t *d_circle_itwids,
+                                 const uint32_t *h_layer_offsets, const uint32_t *h_layer_sizes,
+                                 uint32_t n_line_layers, uint32_t n);
+/* replaces cuda_circle_ntt_evaluate_batch, circle_ntt.cu:314-357 (d_columns: device array) */
+void cuda_circle_ntt_evaluate_batch(uint32_t **d_columns, const uint32_t *d_twiddles, const uint32_t *d_circle_twids,
+                                    const uint32_t *h_layer_offsets, const uint32_t *h_layer_sizes,
+                                    uint32_t n_line_layers, uint32_t n, uint32_t n_cols);
+/* replaces cuda_circle_ntt_interpolate_batch, circle_ntt.cu:359-404 */
+void cuda_circle_ntt_interpolate_batch(uint32_t **d_columns, const uint32_t *d_itwiddles,
+                                       const uint32_t *d_circle_itwids, const uint32_t *h_layer_offsets,
+                                       const uint32_t *h_layer_sizes, uint32_t n_line_layers, uint32_t n,
+                                       uint32_t n_cols);
+/* replaces cuda_circle_ntt_layer, circle_ntt.cu:408-420 */
+void cuda_circle_ntt_layer(uint32_t *d_data, const uint32_t *d_twiddles, uint32_t layer_idx, uint32_t n, int forward);
+/* replaces cuda_bit_reverse_m31, circle_ntt.cu:422-427 */
+void cuda_bit_reverse_m31(uint32_t *data, uint32_t log_n);
+/* replaces cuda_permute_hc_to_canonic_brt, permute.cu:30-44 (ffi.rs:317-322) */
+void cuda_permute_hc_to_canonic_brt(const uint32_t *src, uint32_t *dst, uint32_t n, uint32_t log_n);
+/* replaces cuda_permute_canonic_brt_to_hc_natural, permute.cu:46-58 (ffi.rs:328-333) */
+void cuda_permute_canonic_brt_to_hc_natural(const uint32_t *src, uint32_t *dst, uint32_t n, uint32_t log_n);
+
+/* -- twiddles (ffi.rs:431-469; twiddles.cu:147-213; batch_inverse.cu:43-57) -- */
+/* replaces cuda_compute_coset_points, twiddles.cu:177-190 */
+void cuda_compute_coset_points(uint32_t initial_x, uint32_t initial_y, uint32_t step_x, uint32_t step_y,
+                               uint32_t *output_x, uint32_t *output_y, uint32_t n);
+/* replaces cuda_squash_x, twiddles.cu:192-198 */
+void cuda_squash_x(const uint32_t *input, uint32_t *output, uint32_t out_n);
+/* replaces cuda_extract_and_squash, twiddles.cu:200-210 */
+void cuda_extract_and_squash(const uint32_t *input, uint32_t *twiddle_out, uint32_t *squash_out, uint32_t half_n);
+/* replaces cuda_batch_inverse_m31, batch_inverse.cu:45-50 */
+void cuda_batch_inverse_m31(const uint32_t *input, uint32_t *output, uint32_t n);
+/* replaces cuda_batch_inverse_m31_stream, batch_inverse.cu:52-57 */
+void cuda_batch_inverse_m31_stream(const uint32_t *input, uint32_t *output, uint32_t n, void *stream);
+/* replaces cuda_compute_fold_twiddle_sources, twiddles.cu:147-160 */
+void cuda_compute_fold_twiddle_sources(uint32_t initial_x, uint32_t initial_y, uint32_t step_x, uint32_t step_y,
+                                       uint32_t *output, uint32_t n, uint32_t log_n, int extract_y);
+/* replaces cuda_compute_fold_twiddle_sources_stream, twiddles.cu:162-175 */
+void cuda_compute_fold_twiddle_sources_stream(uint32_t initial_x, uint32_t initial_y, uint32_t step_x,
+                                              uint32_t step_y, uint32_t *output, uint32_t n, uint32_t log_n,
+                                              int extract_y, void *stream);
+
+/* -- glue (ffi.rs:471-503; constraint.cu:94-153) -- */
+/* replaces cuda_zero_pad, constraint.cu:108-117 */
+void cuda_zero_pad(const uint32_t *src, uint32_t *dst, uint32_t src_n, uint32_t dst_n);
+/* replaces cuda_fibonacci_quotient, constraint.cu:94-106 (alpha: host [4]) */
+void cuda_fibonacci_quotient(const uint32_t *trace, uint32_t *out0, uint32_t *out1, uint32_t *out2, uint32_t *out3,
+                             const uint32_t *alpha, uint32_t n);
+/* replaces cuda_fibonacci_quotient_chunk, constraint.cu:121-136 */
+void cuda_fibonacci_quotient_chunk(const uint32_t *trace, uint32_t *out0, uint32_t *out1, uint32_t *out2,
+                                   uint32_t *out3, const uint32_t *alpha, uint32_t offset, uint32_t chunk_n,
+                                   uint32_t global_n);
+/* replaces cuda_fibonacci_quotient_chunk_stream, constraint.cu:139-153 */
+void cuda_fibonacci_quotient_chunk_stream(const uint32_t *trace, uint32_t *out0, uint32_t *out1, uint32_t *out2,
+                                          uint32_t *out3, const uint32_t *alpha, uint32_t offset, uint32_t chunk_n,
+                                          uint32_t global_n, void *stream);
+
+/* -- Blake2s Merkle (ffi.rs:776-866, 937-944; blake2s.cu:537-646) -- */
+/* replaces cuda_merkle_hash_leaves, blake2s.cu:539-548 (columns: device array) */
+void cuda_merkle_hash_leaves(const uint32_t *const *columns, uint32_t *hashes, uint32_t n_cols, uint32_t n_leaves);
+/* replaces cuda_merkle_hash_leaves_forge_single, merkle_hash_leaves_forge.cu:20-33 */
+void cuda_merkle_hash_leaves_forge_single(const uint32_t *column, uint32_t *hashes, uint32_t n_leaves);
+/* replaces cuda_merkle_hash_leaves_forge_quad, merkle_hash_leaves_forge.cu:35-51 */
+void cuda_merkle_hash_leaves_forge_quad(const uint32_t *c0, const uint32_t *c1, const uint32_t *c2,
+                                        const uint32_t *c3, uint32_t *hashes, uint32_t n_leaves);
+/* replaces cuda_merkle_hash_nodes, blake2s.cu:550-559 */
+void cuda_merkle_hash_nodes(const uint32_t *children, uint32_t *parents, uint32_t n_parents);
+/* replaces cuda_merkle_reduce_to_root, blake2s.cu:562-569 (n_nodes <= 1024, power of two) */
+void cuda_merkle_reduce_to_root(const uint32_t *nodes, uint32_t *root_out, uint32_t n_nodes);
+/* replaces cuda_merkle_commit_small_soa4, blake2s.cu:573-584 (n_leaves <= 2048) */
+void cuda_merkle_commit_small_soa4(const uint32_t *col0, const uint32_t *col1, const uint32_t *col2,
+                                   const uint32_t *col3, uint32_t *root_out, uint32_t n_leaves);
+/* replaces cuda_merkle_hash_leaves_merge_soa4, blake2s.cu:588-600 */
+void cuda_merkle_hash_leaves_merge_soa4(const uint32_t *col0, const uint32_t *col1, const uint32_t *col2,
+                                        const uint32_t *col3, uint32_t *parents, uint32_t n_leaves);
+/* replaces cuda_merkle_tiled_soa4, blake2s.cu:604-615 (one root per 1024 leaves) */
+void cuda_merkle_tiled_soa4(const uint32_t *col0, const uint32_t *col1, const uint32_t *col2, const uint32_t *col3,
+                            uint32_t *subtree_roots, uint32_t n_leaves);
+/* replaces cuda_merkle_tiled_soa4_stream, blake2s.cu:618-630 */
+void cuda_merkle_tiled_soa4_stream(const uint32_t *col0, const uint32_t *col1, const uint32_t *col2,
+                                   const uint32_t *col3, uint32_t *subtree_roots, uint32_t n_leaves, void *stream);
+/* replaces cuda_merkle_tiled_generic, blake2s.cu:634-644 (columns: device array) */
+void cuda_merkle_tiled_generic(const uint32_t *const *columns, uint32_t *subtree_roots, uint32_t n_cols,
+                               uint32_t n_leaves);
+/* replaces cuda_build_leaves_lifted, merkle_leaves_lifted.cu:104-120.
+ * schedule: device array of {uint32 col_indices[16]; uint32 n_cols; uint32 log_size} */
+void cuda_build_leaves_lifted(const uint32_t *const *col_ptrs, const void *schedule, uint32_t n_chunks,
+                              uint32_t lifting_log_size, uint32_t *output_hashes, uint32_t n_leaves);
+
+/* -- FRI folds (ffi.rs:345-425; fri.cu:128-163) -- */
+/* replaces cuda_fold_line_soa, fri.cu:130-145 (alpha: host [4]) */
+void cuda_fold_line_soa(const uint32_t *in0, const uint32_t *in1, const uint32_t *in2, const uint32_t *in3,
+                        const uint32_t *twiddles, uint32_t *out0, uint32_t *out1, uint32_t *out2, uint32_t *out3,
+                        const uint32_t *alpha, uint32_t half_n);
+/* replaces cuda_fold_circle_into_line_soa, fri.cu:147-161 (alpha, alpha_sq: host [4]) */
+void cuda_fold_circle_into_line_soa(uint32_t *dst0, uint32_t *dst1, uint32_t *dst2, uint32_t *dst3,
+                                    const uint32_t *src0, const uint32_t *src1, const uint32_t *src2,
+                                    const uint32_t *src3, const uint32_t *twiddles, const uint32_t *alpha,
+                                    const uint32_t *alpha_sq, uint32_t half_n);
+/* replaces cuda_fold_line_soa_forge, fri_fold_line_forge.cu (same semantics as cuda_fold_line_soa) */
+void cuda_fold_line_soa_forge(const uint32_t *in0, const uint32_t *in1, const uint32_t *in2, const uint32_t *in3,
+                              const uint32_t *twiddles, uint32_t *out0, uint32_t *out1, uint32_t *out2,
+                              uint32_t *out3, const uint32_t *alpha, uint32_t half_n);
+/* replaces cuda_fold_circle_into_line_soa_forge, fri_fold_circle_forge.cu */
+void cuda_fold_circle_into_line_soa_forge(uint32_t *dst0, uint32_t *dst1, uint32_t *dst2, uint32_t *dst3,
+                                          const uint32_t *src0, const uint32_t *src1, const uint32_t *src2,
+                                          const uint32_t *src3, const uint32_t *twiddles, const uint32_t *alpha,
+                                          const uint32_t *alpha_sq, uint32_t half_n);
+
+/* replaces cuda_device_sync, fields.cu:44 */
+void cuda_device_sync(void);
+
+/* ======================================================================
+ * 2. Device-resident whole-proof path (new; no counterpart symbol in the
+ *    reference — it replaces the body of prover.rs:264-619 / 627-1167)
+ * ====================================================================== */
+
+/* Message describing the last failure on the calling host thread. */
+const char *vx_last_error(void);
+/* Library version, major * 10000 + minor * 100 + patch. */
+int vx_version(void);
+
+/* Bytes of a proof in the reference's "KRAK" v1 layout
+ * (stark_cli.rs:1092-1123) for (log_n, blowup_bits, n_queries). */
+size_t vx_proof_size(uint32_t log_n, uint32_t blowup_bits, uint32_t n_queries);
+
+/* One proof slot: device buffers for one in-flight proof of 2^log_n trace
+ * rows with a 2^(log_n+blowup_bits) evaluation domain, plus shared,
+ * device-resident twiddle tables for that size.  4 <= log_n,
+ * log_n + blowup_bits <= 31, blowup_bits >= 1. */
+typedef struct vx_prover vx_prover;
+int vx_prover_create(uint32_t log_n, uint32_t blowup_bits, uint32_t n_queries, vx_prover **out);
+void vx_prover_destroy(vx_prover *p);
+/* Device bytes held by the slot (not counting the shared tables). */
+size_t vx_prover_slot_bytes(const vx_prover *p);
+/* Device bytes of the shared tables for this size. */
+size_t vx_prover_table_bytes(const vx_prover *p);
+/* Enqueue a whole proof of the Fibonacci AIR with public inputs (a, b) on
+ * `stream` (a cudaStream_t; NULL = legacy default).  No host
+ * synchronisation inside; the proof stays in the slot's device buffer. */
+int vx_prover_prove_async(vx_prover *p, uint32_t a, uint32_t b, void *stream);
+/* The proof's stages in order: 0 trace, 1 interpolate, 2 LDE evaluate,
+ * 3 trace commitment, 4 quotient commitment, 5 circle fold + FRI layer 0,
+ * 6 line folds + commitments, 7 last layer + query sampling,
+ * 8 decommitment.  vx_prover_prove_async enqueues all of them; this enqueues
+ * one (each stage reads what the earlier ones left in the slot), for
+ * per-stage timing. */
+#define VX_N_STAGES 9
+int vx_prover_stage_async(vx_prover *p, uint32_t stage, uint32_t a, uint32_t b, void *stream);
+/* Kernels enqueued by the last vx_prover_prove_async of this slot. */
+uint32_t vx_prover_launches(const vx_prover *p);
+/* Enqueue the copy of the slot's proof bytes to host memory `dst`
+ * (vx_proof_size bytes; pinned memory makes it asynchronous). */
+int vx_prover_fetch_async(vx_prover *p, void *dst, void *stream);
+/* Device address and size of the slot's proof bytes. */
+int vx_prover_proof_device(vx_prover *p, const void **dptr, size_t *bytes);
+/* Check the slot's device status word after the stream has drained. */
+int vx_prover_check(vx_prover *p);
+
+/* Synchronous convenience: prove (a, b) at log_n into the host buffer
+ * `out` (capacity `cap`), writing the proof length to *out_len.  Slots and
+ * tables are cached per size and reused by later calls. */
+int vx_prove_fib(uint32_t a, uint32_t b, uint32_t log_n, uint32_t blowup_bits, uint32_t n_queries, uint8_t *out,
+                 size_t cap, size_t *out_len);
+
+/* Blake2s throughput probe: `blocks` x `threads` threads each run `iters`
+ * chained compressions on registers only (no memory traffic) and write one
+ * word to out[thread].  Gives the achievable compressions/s, the ALU
+ * roofline of the Merkle kernels. */
+int vx_probe_blake2s(uint32_t blocks, uint32_t threads, uint32_t iters, uint32_t *out, void *stream);
+
+/* Free every cached slot and table on every device. */
+void vx_release_all(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VORTEX_B200_H */

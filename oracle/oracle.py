@@ -1,0 +1,271 @@
+"""ctypes bindings for the CPU oracle (liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by ``__graft_entry__.smoke()``
+and by the CPU-baseline leg of ``bench.py``.  The product package
+(``vortexstark_b200``) never imports this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+P = 0x7FFFFFFF
+U32P = C.POINTER(C.c_uint32)
+
+
+def build() -> str:
+    """Compile liboracle.so with the committed Makefile (gcc + OpenMP)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True, env={**os.environ, "CC": "gcc"})
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        L.vxo_prove.argtypes = [C.c_uint32] * 5 + [C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(C.c_size_t)]
+        L.vxo_prove.restype = C.c_int
+        L.vxo_verify.argtypes = [C.POINTER(C.c_uint8), C.c_size_t, C.c_uint32, C.c_uint32, C.c_char_p, C.c_size_t]
+        L.vxo_verify.restype = C.c_int
+        L.vxo_proof_size.argtypes = [C.c_uint32] * 3
+        L.vxo_proof_size.restype = C.c_size_t
+        L.vxo_prove_roots.argtypes = [C.c_uint32] * 4 + [U32P] * 3
+        L.vxo_free.argtypes = [C.c_void_p]
+        L.vxo_set_threads.argtypes = [C.c_int]
+        L.vxo_get_threads.restype = C.c_int
+        L.vxo_blake2s.argtypes = [C.c_char_p, C.c_size_t, C.POINTER(C.c_uint8)]
+        L.vxo_twiddles.argtypes = [C.c_void_p, C.c_int, U32P, U32P, U32P]
+        L.vxo_ntt_evaluate.argtypes = [U32P, U32P, U32P, U32P, C.c_uint32]
+        L.vxo_ntt_interpolate.argtypes = [U32P, U32P, U32P, U32P, C.c_uint32]
+        L.vxo_ntt_layer.argtypes = [U32P, U32P, C.c_uint32, C.c_uint64, C.c_int]
+        L.vxo_bit_reverse.argtypes = [U32P, C.c_uint32]
+        L.vxo_permute_hc_to_canonic_brt.argtypes = [U32P, U32P, C.c_uint32]
+        L.vxo_permute_canonic_brt_to_hc.argtypes = [U32P, U32P, C.c_uint32]
+        L.vxo_fibonacci_trace.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, U32P]
+        L.vxo_fibonacci_quotient.argtypes = [U32P, C.c_uint64, U32P, U32P, U32P, U32P, U32P]
+        L.vxo_merkle_root.argtypes = [C.POINTER(U32P), C.c_uint32, C.c_uint32, U32P]
+        L.vxo_lifted_leaves.argtypes = [C.POINTER(U32P), U32P, C.c_uint32, C.c_uint32, U32P]
+        L.vxo_fold_twiddles.argtypes = [C.c_void_p, C.c_int, U32P]
+        L.vxo_fold_line.argtypes = [C.POINTER(U32P), U32P, U32P, C.POINTER(U32P), C.c_uint64]
+        L.vxo_fold_circle_into_line.argtypes = [C.POINTER(U32P), C.POINTER(U32P), U32P, U32P, U32P, C.c_uint64]
+        L.vxo_batch_inverse.argtypes = [U32P, U32P, C.c_size_t]
+        L.vxo_qm31_mul.argtypes = [U32P, U32P, U32P]
+        L.vxo_hash_leaf.argtypes = [U32P, C.c_uint32, U32P]
+        L.vxo_hash_pair.argtypes = [U32P, U32P, U32P]
+        for name in ("subgroup", "half_coset", "half_odds"):
+            f = getattr(L, f"vxo_coset_{name}")
+            f.argtypes = [C.c_uint32]
+            f.restype = Coset
+        L.vxo_coset_at.argtypes = [C.POINTER(Coset), C.c_uint64]
+        L.vxo_coset_at.restype = Point
+        L.vxo_point_pow.argtypes = [Point, C.c_uint64]
+        L.vxo_point_pow.restype = Point
+        L.vxo_point_mul.argtypes = [Point, Point]
+        L.vxo_point_mul.restype = Point
+        _lib = L
+    return _lib
+
+
+class Point(C.Structure):
+    _fields_ = [("x", C.c_uint32), ("y", C.c_uint32)]
+
+
+class Coset(C.Structure):
+    _fields_ = [("initial", Point), ("step", Point), ("log_size", C.c_uint32)]
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.uint32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(U32P)
+
+
+def coset(kind: str, log_size: int) -> Coset:
+    return getattr(lib(), f"vxo_coset_{kind}")(log_size)
+
+
+def set_threads(n: int) -> None:
+    lib().vxo_set_threads(int(n))
+
+
+def get_threads() -> int:
+    return int(lib().vxo_get_threads())
+
+
+def prove(a: int, b: int, log_n: int, blowup_bits: int = 2, n_queries: int = 80) -> bytes:
+    L = lib()
+    out = C.POINTER(C.c_uint8)()
+    n = C.c_size_t()
+    rc = L.vxo_prove(a, b, log_n, blowup_bits, n_queries, C.byref(out), C.byref(n))
+    if rc:
+        raise ValueError(f"oracle prove rejected its arguments (rc={rc})")
+    try:
+        return C.string_at(out, n.value)
+    finally:
+        L.vxo_free(out)
+
+
+def verify(proof: bytes, blowup_bits: int = 2, n_queries: int = 80) -> tuple[int, str]:
+    buf = (C.c_uint8 * len(proof)).from_buffer_copy(proof)
+    msg = C.create_string_buffer(256)
+    rc = lib().vxo_verify(buf, len(proof), blowup_bits, n_queries, msg, 256)
+    return rc, msg.value.decode()
+
+
+def proof_size(log_n: int, blowup_bits: int = 2, n_queries: int = 80) -> int:
+    return int(lib().vxo_proof_size(log_n, blowup_bits, n_queries))
+
+
+def prove_roots(a: int, b: int, log_n: int, blowup_bits: int = 2):
+    le = log_n + blowup_bits
+    tr = np.zeros(8, np.uint32)
+    qr = np.zeros(8, np.uint32)
+    fr = np.zeros(8 * (le - 3), np.uint32)
+    rc = lib().vxo_prove_roots(a, b, log_n, blowup_bits, _p(tr), _p(qr), _p(fr))
+    if rc:
+        raise ValueError("bad arguments")
+    return tr, qr, fr.reshape(-1, 8)
+
+
+def blake2s(data: bytes) -> bytes:
+    out = (C.c_uint8 * 32)()
+    lib().vxo_blake2s(data, len(data), out)
+    return bytes(out)
+
+
+def twiddles(cs: Coset, inverse: bool):
+    m = 1 << cs.log_size
+    line = np.zeros(max(m - 1, 1), np.uint32)
+    circ = np.zeros(max(m // 2, 1), np.uint32)
+    offs = np.zeros(32, np.uint32)
+    lib().vxo_twiddles(C.byref(cs), int(inverse), _p(line), _p(circ), _p(offs))
+    n_line = max(cs.log_size - 1, 0)
+    return line[: m - 1], circ[: m // 2], offs[:n_line]
+
+
+def ntt_evaluate(data: np.ndarray, cs: Coset) -> np.ndarray:
+    d = np.ascontiguousarray(data, dtype=np.uint32).copy()
+    line, circ, offs = twiddles(cs, False)
+    offs32 = np.zeros(32, np.uint32)
+    offs32[: len(offs)] = offs
+    lib().vxo_ntt_evaluate(_p(d), _p(line), _p(circ), _p(offs32), cs.log_size)
+    return d
+
+
+def ntt_interpolate(data: np.ndarray, cs: Coset) -> np.ndarray:
+    d = np.ascontiguousarray(data, dtype=np.uint32).copy()
+    line, circ, offs = twiddles(cs, True)
+    offs32 = np.zeros(32, np.uint32)
+    offs32[: len(offs)] = offs
+    lib().vxo_ntt_interpolate(_p(d), _p(line), _p(circ), _p(offs32), cs.log_size)
+    return d
+
+
+def ntt_layer(data: np.ndarray, tw: np.ndarray, layer_idx: int, forward: bool) -> np.ndarray:
+    d = np.ascontiguousarray(data, dtype=np.uint32).copy()
+    t = np.ascontiguousarray(tw, dtype=np.uint32)
+    lib().vxo_ntt_layer(_p(d), _p(t), layer_idx, len(d), int(forward))
+    return d
+
+
+def bit_reverse(data: np.ndarray) -> np.ndarray:
+    d = np.ascontiguousarray(data, dtype=np.uint32).copy()
+    lib().vxo_bit_reverse(_p(d), int(len(d)).bit_length() - 1)
+    return d
+
+
+def permute_hc_to_canonic_brt(data: np.ndarray) -> np.ndarray:
+    s = np.ascontiguousarray(data, dtype=np.uint32)
+    d = np.zeros_like(s)
+    lib().vxo_permute_hc_to_canonic_brt(_p(s), _p(d), int(len(s)).bit_length() - 1)
+    return d
+
+
+def permute_canonic_brt_to_hc(data: np.ndarray) -> np.ndarray:
+    s = np.ascontiguousarray(data, dtype=np.uint32)
+    d = np.zeros_like(s)
+    lib().vxo_permute_canonic_brt_to_hc(_p(s), _p(d), int(len(s)).bit_length() - 1)
+    return d
+
+
+def fibonacci_trace(a: int, b: int, log_n: int) -> np.ndarray:
+    out = np.zeros(1 << log_n, np.uint32)
+    lib().vxo_fibonacci_trace(a, b, log_n, _p(out))
+    return out
+
+
+def fibonacci_quotient(ev: np.ndarray, alpha) -> np.ndarray:
+    ev = np.ascontiguousarray(ev, dtype=np.uint32)
+    q = np.zeros((4, len(ev)), np.uint32)
+    al = np.array(alpha, np.uint32)
+    lib().vxo_fibonacci_quotient(_p(ev), len(ev), _p(al), _p(q[0]), _p(q[1]), _p(q[2]), _p(q[3]))
+    return q
+
+
+def merkle_root(cols) -> np.ndarray:
+    cols = [np.ascontiguousarray(c, dtype=np.uint32) for c in cols]
+    arr = (U32P * len(cols))(*[_p(c) for c in cols])
+    out = np.zeros(8, np.uint32)
+    lib().vxo_merkle_root(arr, len(cols), int(len(cols[0])).bit_length() - 1, _p(out))
+    return out
+
+
+def lifted_leaves(cols, lifting_log: int) -> np.ndarray:
+    cols = [np.ascontiguousarray(c, dtype=np.uint32) for c in cols]
+    logs = np.array([int(len(c)).bit_length() - 1 for c in cols], np.uint32)
+    arr = (U32P * len(cols))(*[_p(c) for c in cols])
+    out = np.zeros((1 << lifting_log) * 8, np.uint32)
+    lib().vxo_lifted_leaves(arr, _p(logs), len(cols), lifting_log, _p(out))
+    return out.reshape(-1, 8)
+
+
+def fold_twiddles(cs: Coset, extract_y: bool) -> np.ndarray:
+    out = np.zeros(1 << (cs.log_size - 1), np.uint32)
+    lib().vxo_fold_twiddles(C.byref(cs), int(extract_y), _p(out))
+    return out
+
+
+def fold_line(src: np.ndarray, tw: np.ndarray, alpha) -> np.ndarray:
+    src = np.ascontiguousarray(src, dtype=np.uint32)
+    half = src.shape[1] // 2
+    out = np.zeros((4, half), np.uint32)
+    ins = (U32P * 4)(*[_p(src[c]) for c in range(4)])
+    outs = (U32P * 4)(*[_p(out[c]) for c in range(4)])
+    al = np.array(alpha, np.uint32)
+    lib().vxo_fold_line(ins, _p(np.ascontiguousarray(tw, dtype=np.uint32)), _p(al), outs, half)
+    return out
+
+
+def fold_circle_into_line(dst: np.ndarray, src: np.ndarray, tw: np.ndarray, alpha) -> np.ndarray:
+    src = np.ascontiguousarray(src, dtype=np.uint32)
+    dst = np.ascontiguousarray(dst, dtype=np.uint32).copy()
+    half = src.shape[1] // 2
+    al = np.array(alpha, np.uint32)
+    al2 = qm31_mul(al, al)
+    ins = (U32P * 4)(*[_p(src[c]) for c in range(4)])
+    outs = (U32P * 4)(*[_p(dst[c]) for c in range(4)])
+    lib().vxo_fold_circle_into_line(outs, ins, _p(np.ascontiguousarray(tw, dtype=np.uint32)), _p(al), _p(al2), half)
+    return dst
+
+
+def batch_inverse(x: np.ndarray) -> np.ndarray:
+    x = np.ascontiguousarray(x, dtype=np.uint32)
+    out = np.zeros_like(x)
+    lib().vxo_batch_inverse(_p(x), _p(out), len(x))
+    return out
+
+
+def qm31_mul(a, b) -> np.ndarray:
+    a = np.array(a, np.uint32)
+    b = np.array(b, np.uint32)
+    out = np.zeros(4, np.uint32)
+    lib().vxo_qm31_mul(_p(a), _p(b), _p(out))
+    return out

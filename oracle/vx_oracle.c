@@ -1,0 +1,815 @@
+/*
+ * vx_oracle.c — CPU restatement of the VortexSTARK Fibonacci commitment
+ * path.  TEST INFRASTRUCTURE ONLY (the checker and the CPU baseline); the
+ * product library never links or calls it.
+ *
+ * Each function follows the reference file:line cited in vx_oracle.h.
+ * Parallel loops (OpenMP) only split independent elements, so outputs do
+ * not depend on the thread count.
+ */
+#include "vx_oracle.h"
+#include <stdlib.h>
+#include <string.h>
+#include <stdio.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define P VXO_P
+
+/* ------------------------------------------------------------------ */
+/* field: src/field/m31.rs:24-35, cm31.rs, qm31.rs:110-133            */
+/* ------------------------------------------------------------------ */
+static inline uint32_t m_red(uint64_t v) {
+    uint32_t lo = (uint32_t)(v & P), hi = (uint32_t)(v >> 31), r = lo + hi;
+    return r >= P ? r - P : r;
+}
+static inline uint32_t m_add(uint32_t a, uint32_t b) { uint32_t r = a + b; return r >= P ? r - P : r; }
+static inline uint32_t m_sub(uint32_t a, uint32_t b) { return a >= b ? a - b : a + P - b; }
+static inline uint32_t m_mul(uint32_t a, uint32_t b) { return m_red((uint64_t)a * b); }
+static inline uint32_t m_neg(uint32_t a) { return a ? P - a : 0; }
+static inline uint32_t m_dbl(uint32_t a) { uint32_t r = a << 1; return r >= P ? r - P : r; }
+static uint32_t m_pow(uint32_t a, uint32_t e) {
+    uint32_t r = 1, b = a;
+    while (e) { if (e & 1) r = m_mul(r, b); b = m_mul(b, b); e >>= 1; }
+    return r;
+}
+uint32_t vxo_m31_mul(uint32_t a, uint32_t b) { return m_mul(a, b); }
+uint32_t vxo_m31_inv(uint32_t a) { return m_pow(a, P - 2); }
+
+typedef struct { uint32_t a, b; } cm;
+static inline cm cm_add(cm x, cm y) { return (cm){m_add(x.a, y.a), m_add(x.b, y.b)}; }
+static inline cm cm_sub(cm x, cm y) { return (cm){m_sub(x.a, y.a), m_sub(x.b, y.b)}; }
+static inline cm cm_mul(cm x, cm y) {
+    return (cm){m_sub(m_mul(x.a, y.a), m_mul(x.b, y.b)), m_add(m_mul(x.a, y.b), m_mul(x.b, y.a))};
+}
+typedef struct { uint32_t v[4]; } qm;
+static inline qm q_add(qm x, qm y) { qm r; for (int i = 0; i < 4; i++) r.v[i] = m_add(x.v[i], y.v[i]); return r; }
+static inline qm q_sub(qm x, qm y) { qm r; for (int i = 0; i < 4; i++) r.v[i] = m_sub(x.v[i], y.v[i]); return r; }
+static inline qm q_mulm(qm x, uint32_t s) { qm r; for (int i = 0; i < 4; i++) r.v[i] = m_mul(x.v[i], s); return r; }
+/* (a + bu)(c + du) = (ac + bd(2+i)) + (ad + bc)u  — qm31.rs:138-155 */
+static inline qm q_mul(qm x, qm y) {
+    cm xa = {x.v[0], x.v[1]}, xb = {x.v[2], x.v[3]}, ya = {y.v[0], y.v[1]}, yb = {y.v[2], y.v[3]};
+    cm ac = cm_mul(xa, ya), bd = cm_mul(xb, yb), ad = cm_mul(xa, yb), bc = cm_mul(xb, ya);
+    cm bdu = {m_sub(m_dbl(bd.a), bd.b), m_add(bd.a, m_dbl(bd.b))};
+    cm ra = cm_add(ac, bdu), rb = cm_add(ad, bc);
+    qm r = {{ra.a, ra.b, rb.a, rb.b}};
+    return r;
+}
+void vxo_qm31_mul(const uint32_t a[4], const uint32_t b[4], uint32_t out[4]) {
+    qm x, y; memcpy(x.v, a, 16); memcpy(y.v, b, 16);
+    qm r = q_mul(x, y); memcpy(out, r.v, 16);
+}
+
+/* ------------------------------------------------------------------ */
+/* circle group: src/circle.rs:10-185                                 */
+/* ------------------------------------------------------------------ */
+static const vxo_point GEN = {2u, 1268011823u};
+static const vxo_point IDENT = {1u, 0u};
+vxo_point vxo_point_mul(vxo_point a, vxo_point b) {
+    vxo_point r = {m_sub(m_mul(a.x, b.x), m_mul(a.y, b.y)), m_add(m_mul(a.x, b.y), m_mul(a.y, b.x))};
+    return r;
+}
+vxo_point vxo_point_pow(vxo_point a, uint64_t k) {
+    vxo_point r = IDENT, b = a;
+    while (k) { if (k & 1) r = vxo_point_mul(r, b); b = vxo_point_mul(b, b); k >>= 1; }
+    return r;
+}
+static vxo_point rep_double(vxo_point p, uint32_t n) { for (uint32_t i = 0; i < n; i++) p = vxo_point_mul(p, p); return p; }
+vxo_coset vxo_coset_subgroup(uint32_t k) {
+    vxo_coset c = {IDENT, rep_double(GEN, 31 - k), k}; return c;
+}
+vxo_coset vxo_coset_half_coset(uint32_t k) {
+    vxo_coset c = {rep_double(GEN, 30 - k), rep_double(GEN, 31 - k), k}; return c;
+}
+vxo_coset vxo_coset_half_odds(uint32_t k) {
+    vxo_coset c = {rep_double(GEN, k >= 29 ? 0 : 29 - k), rep_double(GEN, 31 - k), k}; return c;
+}
+vxo_point vxo_coset_at(const vxo_coset *c, uint64_t i) {
+    return vxo_point_mul(c->initial, vxo_point_pow(c->step, (uint32_t)i));
+}
+
+/* all points p_j = initial * step^j, j < m (exact, so any evaluation order
+ * gives the reference's coset_points values — twiddles.cu:80-105) */
+static void coset_points(const vxo_coset *c, uint32_t *xs, uint32_t *ys) {
+    uint64_t m = 1ull << c->log_size;
+    const uint64_t CH = 4096;
+    int64_t nch = (int64_t)((m + CH - 1) / CH);
+    #pragma omp parallel for schedule(static)
+    for (int64_t ci = 0; ci < nch; ci++) {
+        uint64_t j0 = (uint64_t)ci * CH, j1 = j0 + CH < m ? j0 + CH : m;
+        vxo_point p = vxo_coset_at(c, j0);
+        for (uint64_t j = j0; j < j1; j++) {
+            if (xs) xs[j] = p.x;
+            if (ys) ys[j] = p.y;
+            p = vxo_point_mul(p, c->step);
+        }
+    }
+}
+
+/* Montgomery batch inverse over aligned chunks of 64, exactly as the
+ * reference kernel (batch_inverse.cu:8-41): a zero input maps to zero, and
+ * the running prefix starts from the chunk's first element itself, so a zero
+ * at a chunk's first slot makes the whole chunk's product (and hence every
+ * output of that chunk) zero.  Reached only by the circle-fold twiddles of
+ * subgroup(31), whose point 0 is the identity (y = 0). */
+void vxo_batch_inverse(const uint32_t *in, uint32_t *out, size_t n) {
+    const size_t CH = 64;
+    int64_t nch = (int64_t)((n + CH - 1) / CH);
+    #pragma omp parallel for schedule(static)
+    for (int64_t ci = 0; ci < nch; ci++) {
+        size_t s = (size_t)ci * CH, e = s + CH < n ? s + CH : n;
+        uint32_t pre[64], val[64];
+        for (size_t i = s; i < e; i++) val[i - s] = in[i];
+        pre[0] = val[0];
+        for (size_t i = 1; i < e - s; i++) pre[i] = val[i] ? m_mul(pre[i - 1], val[i]) : pre[i - 1];
+        uint32_t inv = m_pow(pre[e - s - 1], P - 2);
+        for (size_t i = e - s - 1; i > 0; i--) {
+            if (!val[i]) { out[s + i] = 0; continue; }
+            out[s + i] = m_mul(inv, pre[i - 1]);
+            inv = m_mul(inv, val[i]);
+        }
+        out[s] = val[0] ? inv : 0;
+    }
+}
+
+/* circle.rs:357-435 (compute_twiddles / compute_itwiddles) */
+void vxo_twiddles(const vxo_coset *c, int inverse, uint32_t *line, uint32_t *circle, uint32_t *offsets) {
+    uint32_t k = c->log_size;
+    uint64_t m = 1ull << k;
+    uint32_t *xs = (uint32_t *)malloc(m * 4), *ys = (uint32_t *)malloc(m * 4);
+    coset_points(c, xs, ys);
+    memcpy(circle, ys, (m / 2) * 4);
+    uint32_t n_line = k > 0 ? k - 1 : 0;
+    uint64_t cur_n = m, off = 0;
+    uint32_t *cur = xs, *nxt = ys; /* ys no longer needed: reuse as scratch */
+    for (uint32_t l = 0; l < n_line; l++) {
+        uint64_t ls = cur_n / 2;
+        offsets[l] = (uint32_t)off;
+        #pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < (int64_t)ls; i++) {
+            uint32_t x = cur[2 * i];
+            line[off + i] = x;
+            uint32_t x2 = m_mul(x, x);
+            nxt[i] = m_sub(m_add(x2, x2), 1);
+        }
+        off += ls; cur_n = ls;
+        uint32_t *t = cur; cur = nxt; nxt = t;
+    }
+    free(xs); free(ys);
+    if (inverse) {
+        if (off) vxo_batch_inverse(line, line, off);
+        vxo_batch_inverse(circle, circle, m / 2);
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* circle NTT: circle_ntt.cu:74-117 (butterflies), 248-312 (order)    */
+/* ------------------------------------------------------------------ */
+void vxo_ntt_layer(uint32_t *d, const uint32_t *tw, uint32_t L, uint64_t n, int fwd) {
+    int64_t half = (int64_t)(n / 2);
+    uint64_t stride = 1ull << L;
+    #pragma omp parallel for schedule(static)
+    for (int64_t tid = 0; tid < half; tid++) {
+        uint64_t h = (uint64_t)tid >> L, l = (uint64_t)tid & (stride - 1);
+        uint64_t i0 = (h << (L + 1)) + l, i1 = i0 + stride;
+        uint32_t v0 = d[i0], v1 = d[i1], t = tw[h];
+        if (fwd) { uint32_t tmp = m_mul(v1, t); d[i1] = m_sub(v0, tmp); d[i0] = m_add(v0, tmp); }
+        else { d[i0] = m_add(v0, v1); d[i1] = m_mul(m_sub(v0, v1), t); }
+    }
+}
+void vxo_ntt_evaluate(uint32_t *d, const uint32_t *line, const uint32_t *circle, const uint32_t *offsets, uint32_t k) {
+    uint64_t n = 1ull << k;
+    uint32_t n_line = k > 0 ? k - 1 : 0;
+    for (int l = (int)n_line - 1; l >= 0; l--) vxo_ntt_layer(d, line + offsets[l], (uint32_t)l + 1, n, 1);
+    if (k > 0) vxo_ntt_layer(d, circle, 0, n, 1);
+}
+void vxo_ntt_interpolate(uint32_t *d, const uint32_t *iline, const uint32_t *icircle, const uint32_t *offsets, uint32_t k) {
+    uint64_t n = 1ull << k;
+    uint32_t n_line = k > 0 ? k - 1 : 0;
+    if (k > 0) vxo_ntt_layer(d, icircle, 0, n, 0);
+    for (uint32_t l = 0; l < n_line; l++) vxo_ntt_layer(d, iline + offsets[l], l + 1, n, 0);
+    uint32_t e = (30u * k) % 31u;
+    uint32_t inv_n = e == 0 ? 1u : (1u << e);
+    #pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)n; i++) d[i] = m_mul(d[i], inv_n);
+}
+static void with_tables(uint32_t *d, const vxo_coset *c, int inverse) {
+    uint64_t m = 1ull << c->log_size;
+    uint32_t *line = (uint32_t *)malloc((m > 1 ? m - 1 : 1) * 4), *circ = (uint32_t *)malloc((m / 2 + 1) * 4);
+    uint32_t offs[32];
+    vxo_twiddles(c, inverse, line, circ, offs);
+    if (inverse) vxo_ntt_interpolate(d, line, circ, offs, c->log_size);
+    else vxo_ntt_evaluate(d, line, circ, offs, c->log_size);
+    free(line); free(circ);
+}
+void vxo_evaluate_on(uint32_t *d, const vxo_coset *c) { with_tables(d, c, 0); }
+void vxo_interpolate_on(uint32_t *d, const vxo_coset *c) { with_tables(d, c, 1); }
+
+static inline uint64_t brev(uint64_t i, uint32_t bits) {
+    if (!bits) return 0;
+    uint64_t r = 0;
+    for (uint32_t b = 0; b < bits; b++) { r = (r << 1) | (i & 1); i >>= 1; }
+    return r;
+}
+void vxo_bit_reverse(uint32_t *d, uint32_t log_n) {
+    int64_t n = (int64_t)1 << log_n;
+    #pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; i++) {
+        uint64_t j = brev((uint64_t)i, log_n);
+        if ((uint64_t)i < j) { uint32_t t = d[i]; d[i] = d[j]; d[j] = t; }
+    }
+}
+static inline uint64_t hc_to_brt(uint64_t k, uint32_t log_n) {
+    uint64_t n = 1ull << log_n;
+    uint64_t cn = (k & 1) ? n - 1 - k / 2 : k / 2;
+    return brev(cn, log_n);
+}
+void vxo_permute_hc_to_canonic_brt(const uint32_t *src, uint32_t *dst, uint32_t log_n) {
+    int64_t n = (int64_t)1 << log_n;
+    #pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < n; k++) dst[hc_to_brt((uint64_t)k, log_n)] = src[k];
+}
+void vxo_permute_canonic_brt_to_hc(const uint32_t *src, uint32_t *dst, uint32_t log_n) {
+    int64_t n = (int64_t)1 << log_n;
+    #pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < n; k++) dst[k] = src[hc_to_brt((uint64_t)k, log_n)];
+}
+
+/* ------------------------------------------------------------------ */
+/* trace + quotient: air.rs:85-189, constraint.cu:10-64               */
+/* ------------------------------------------------------------------ */
+/* (F(k), F(k+1)) by 2x2 matrix power — air.rs:85-131 */
+static void fib_at(uint32_t a, uint32_t b, uint64_t k, uint32_t *fk, uint32_t *fk1) {
+    uint32_t m00 = 1, m01 = 0, m10 = 0, m11 = 1, b00 = 1, b01 = 1, b10 = 1, b11 = 0;
+    while (k) {
+        if (k & 1) {
+            uint32_t t00 = m_add(m_mul(m00, b00), m_mul(m01, b10)), t01 = m_add(m_mul(m00, b01), m_mul(m01, b11));
+            uint32_t t10 = m_add(m_mul(m10, b00), m_mul(m11, b10)), t11 = m_add(m_mul(m10, b01), m_mul(m11, b11));
+            m00 = t00; m01 = t01; m10 = t10; m11 = t11;
+        }
+        uint32_t t00 = m_add(m_mul(b00, b00), m_mul(b01, b10)), t01 = m_add(m_mul(b00, b01), m_mul(b01, b11));
+        uint32_t t10 = m_add(m_mul(b10, b00), m_mul(b11, b10)), t11 = m_add(m_mul(b10, b01), m_mul(b11, b11));
+        b00 = t00; b01 = t01; b10 = t10; b11 = t11;
+        k >>= 1;
+    }
+    *fk = m_add(m_mul(m10, b), m_mul(m11, a));
+    *fk1 = m_add(m_mul(m00, b), m_mul(m01, a));
+}
+void vxo_fibonacci_trace(uint32_t a, uint32_t b, uint32_t log_n, uint32_t *out) {
+    uint64_t n = 1ull << log_n;
+    const uint64_t CH = 1ull << 16;
+    int64_t nch = (int64_t)((n + CH - 1) / CH);
+    #pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < nch; c++) {
+        uint64_t s = (uint64_t)c * CH, e = s + CH < n ? s + CH : n;
+        uint32_t f0, f1;
+        fib_at(a, b, s, &f0, &f1);
+        out[s] = f0;
+        if (s + 1 < e) out[s + 1] = f1;
+        for (uint64_t i = s + 2; i < e; i++) out[i] = m_add(out[i - 1], out[i - 2]);
+    }
+}
+void vxo_fibonacci_quotient(const uint32_t *t, uint64_t n, const uint32_t alpha[4],
+                            uint32_t *q0, uint32_t *q1, uint32_t *q2, uint32_t *q3) {
+    #pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)n; i++) {
+        uint32_t c = m_sub(t[(i + 2) % n], m_add(t[(i + 1) % n], t[i]));
+        q0[i] = m_mul(alpha[0], c); q1[i] = m_mul(alpha[1], c);
+        q2[i] = m_mul(alpha[2], c); q3[i] = m_mul(alpha[3], c);
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* Blake2s-256 (RFC 7693; channel.rs:216-298, blake2s.cuh:55-136)      */
+/* ------------------------------------------------------------------ */
+static const uint32_t IV[8] = {0x6A09E667u, 0xBB67AE85u, 0x3C6EF372u, 0xA54FF53Au,
+                               0x510E527Fu, 0x9B05688Cu, 0x1F83D9ABu, 0x5BE0CD19u};
+static const uint8_t SIG[10][16] = {
+    {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15}, {14, 10, 4, 8, 9, 15, 13, 6, 1, 12, 0, 2, 11, 7, 5, 3},
+    {11, 8, 12, 0, 5, 2, 15, 13, 10, 14, 3, 6, 7, 1, 9, 4}, {7, 9, 3, 1, 13, 12, 11, 14, 2, 6, 5, 10, 4, 0, 15, 8},
+    {9, 0, 5, 7, 2, 4, 10, 15, 14, 1, 11, 12, 6, 8, 3, 13}, {2, 12, 6, 10, 0, 11, 8, 3, 4, 13, 7, 5, 15, 14, 1, 9},
+    {12, 5, 1, 15, 14, 13, 4, 10, 0, 7, 6, 3, 9, 2, 8, 11}, {13, 11, 7, 14, 12, 1, 3, 9, 5, 0, 15, 4, 8, 6, 2, 10},
+    {6, 15, 14, 9, 11, 3, 0, 8, 12, 2, 13, 7, 1, 4, 10, 5}, {10, 2, 8, 4, 7, 6, 1, 5, 15, 11, 9, 14, 3, 12, 13, 0}};
+static inline uint32_t rotr(uint32_t x, int n) { return (x >> n) | (x << (32 - n)); }
+#define GM(a, b, c, d, x, y) do { \
+    v[a] = v[a] + v[b] + (x); v[d] = rotr(v[d] ^ v[a], 16); v[c] = v[c] + v[d]; v[b] = rotr(v[b] ^ v[c], 12); \
+    v[a] = v[a] + v[b] + (y); v[d] = rotr(v[d] ^ v[a], 8); v[c] = v[c] + v[d]; v[b] = rotr(v[b] ^ v[c], 7); } while (0)
+void vxo_blake2s_compress_words(uint32_t h[8], const uint32_t m[16], uint32_t t, uint32_t f) {
+    uint32_t v[16];
+    for (int i = 0; i < 8; i++) { v[i] = h[i]; v[i + 8] = IV[i]; }
+    v[12] ^= t; v[14] ^= f;
+    for (int r = 0; r < 10; r++) {
+        const uint8_t *s = SIG[r];
+        GM(0, 4, 8, 12, m[s[0]], m[s[1]]); GM(1, 5, 9, 13, m[s[2]], m[s[3]]);
+        GM(2, 6, 10, 14, m[s[4]], m[s[5]]); GM(3, 7, 11, 15, m[s[6]], m[s[7]]);
+        GM(0, 5, 10, 15, m[s[8]], m[s[9]]); GM(1, 6, 11, 12, m[s[10]], m[s[11]]);
+        GM(2, 7, 8, 13, m[s[12]], m[s[13]]); GM(3, 4, 9, 14, m[s[14]], m[s[15]]);
+    }
+    for (int i = 0; i < 8; i++) h[i] ^= v[i] ^ v[i + 8];
+}
+static inline uint32_t ld32(const uint8_t *p) { return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24); }
+static inline void st32(uint8_t *p, uint32_t v) { p[0] = (uint8_t)v; p[1] = (uint8_t)(v >> 8); p[2] = (uint8_t)(v >> 16); p[3] = (uint8_t)(v >> 24); }
+void vxo_blake2s(const uint8_t *in, size_t len, uint8_t out[32]) {
+    uint32_t h[8];
+    for (int i = 0; i < 8; i++) h[i] = IV[i];
+    h[0] ^= 0x01010020u;
+    uint32_t m[16];
+    size_t off = 0;
+    while (len - off > 64) {
+        for (int i = 0; i < 16; i++) m[i] = ld32(in + off + 4 * i);
+        off += 64;
+        vxo_blake2s_compress_words(h, m, (uint32_t)off, 0);
+    }
+    uint8_t blk[64] = {0};
+    memcpy(blk, in + off, len - off);
+    for (int i = 0; i < 16; i++) m[i] = ld32(blk + 4 * i);
+    vxo_blake2s_compress_words(h, m, (uint32_t)len, 0xFFFFFFFFu);
+    for (int i = 0; i < 8; i++) st32(out + 4 * i, h[i]);
+}
+/* single-block word hash: t = 4*n (n <= 16), the GPU leaf convention */
+static inline void hash_words16(const uint32_t *w, uint32_t n, uint32_t out[8]) {
+    uint32_t m[16] = {0};
+    if (n > 16) n = 16;
+    for (uint32_t i = 0; i < n; i++) m[i] = w[i];
+    for (int i = 0; i < 8; i++) out[i] = IV[i];
+    out[0] ^= 0x01010020u;
+    vxo_blake2s_compress_words(out, m, 4 * n, 0xFFFFFFFFu);
+}
+void vxo_hash_leaf(const uint32_t *w, uint32_t n, uint32_t out[8]) { hash_words16(w, n, out); }
+void vxo_hash_pair(const uint32_t l[8], const uint32_t r[8], uint32_t out[8]) {
+    uint32_t m[16];
+    memcpy(m, l, 32); memcpy(m + 8, r, 32);
+    hash_words16(m, 16, out);
+}
+
+/* ------------------------------------------------------------------ */
+/* Merkle: merkle.rs:28-130 (layout), 455-497 (paths), 520-566        */
+/* ------------------------------------------------------------------ */
+void vxo_tree_build(vxo_tree *t, const uint32_t *const *cols, uint32_t n_cols, uint32_t log_n) {
+    t->log_n = log_n;
+    t->levels = (uint32_t **)calloc(log_n + 1, sizeof(uint32_t *));
+    uint64_t n = 1ull << log_n;
+    uint32_t *lv = (uint32_t *)malloc(n * 32);
+    uint32_t nc = n_cols > 16 ? 16 : n_cols;
+    #pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)n; i++) {
+        uint32_t w[16];
+        for (uint32_t c = 0; c < nc; c++) w[c] = cols[c][i];
+        hash_words16(w, nc, lv + 8 * i);
+    }
+    t->levels[0] = lv;
+    for (uint32_t l = 1; l <= log_n; l++) {
+        uint64_t m = n >> l;
+        uint32_t *up = (uint32_t *)malloc(m * 32), *dn = t->levels[l - 1];
+        #pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < (int64_t)m; i++) vxo_hash_pair(dn + 16 * i, dn + 16 * i + 8, up + 8 * i);
+        t->levels[l] = up;
+    }
+}
+void vxo_tree_free(vxo_tree *t) {
+    if (!t->levels) return;
+    for (uint32_t l = 0; l <= t->log_n; l++) free(t->levels[l]);
+    free(t->levels); t->levels = NULL;
+}
+void vxo_tree_root(const vxo_tree *t, uint32_t out[8]) { memcpy(out, t->levels[t->log_n], 32); }
+void vxo_tree_path(const vxo_tree *t, uint64_t idx, uint32_t *out) {
+    for (uint32_t l = 0; l < t->log_n; l++) {
+        memcpy(out + 8 * l, t->levels[l] + 8 * (idx ^ 1), 32);
+        idx >>= 1;
+    }
+}
+void vxo_merkle_root(const uint32_t *const *cols, uint32_t n_cols, uint32_t log_n, uint32_t out[8]) {
+    vxo_tree t; vxo_tree_build(&t, cols, n_cols, log_n); vxo_tree_root(&t, out); vxo_tree_free(&t);
+}
+int vxo_verify_path(const uint32_t root[8], const uint32_t leaf[8], uint64_t idx, const uint32_t *path, uint32_t depth) {
+    uint32_t cur[8];
+    memcpy(cur, leaf, 32);
+    for (uint32_t l = 0; l < depth; l++) {
+        uint32_t nx[8];
+        if (idx & 1) vxo_hash_pair(path + 8 * l, cur, nx); else vxo_hash_pair(cur, path + 8 * l, nx);
+        memcpy(cur, nx, 32);
+        idx >>= 1;
+    }
+    return memcmp(cur, root, 32) == 0;
+}
+void vxo_lifted_leaves(const uint32_t *const *cols, const uint32_t *log_sizes, uint32_t n_cols,
+                       uint32_t S, uint32_t *out) {
+    uint64_t n = 1ull << S;
+    #pragma omp parallel for schedule(static)
+    for (int64_t idx = 0; idx < (int64_t)n; idx++) {
+        uint8_t *buf = (uint8_t *)malloc(4 * (size_t)n_cols + 1);
+        for (uint32_t c = 0; c < n_cols; c++) {
+            uint32_t L = log_sizes[c];
+            uint64_t row = (L == S) ? (uint64_t)idx : ((((uint64_t)idx >> (S - L + 1)) << 1) | ((uint64_t)idx & 1));
+            st32(buf + 4 * c, cols[c][row]);
+        }
+        uint8_t dg[32];
+        vxo_blake2s(buf, 4 * (size_t)n_cols, dg);
+        for (int i = 0; i < 8; i++) out[8 * idx + i] = ld32(dg + 4 * i);
+        free(buf);
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* FRI: fri.rs:73-224 (twiddles, folds), twiddles.cu:23-52            */
+/* ------------------------------------------------------------------ */
+void vxo_fold_twiddles(const vxo_coset *dom, int extract_y, uint32_t *out) {
+    uint32_t k = dom->log_size;
+    int64_t half = (int64_t)1 << (k - 1);
+    uint32_t *src = (uint32_t *)malloc((size_t)half * 4);
+    #pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < half; i++) {
+        vxo_point p = vxo_coset_at(dom, brev((uint64_t)i << 1, k));
+        src[i] = extract_y ? p.y : p.x;
+    }
+    vxo_batch_inverse(src, out, (size_t)half);
+    free(src);
+}
+void vxo_fold_line(const uint32_t *const in[4], const uint32_t *tw, const uint32_t alpha[4],
+                   uint32_t *const out[4], uint64_t half_n) {
+    qm al; memcpy(al.v, alpha, 16);
+    #pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)half_n; i++) {
+        qm f0, f1;
+        for (int c = 0; c < 4; c++) { f0.v[c] = in[c][2 * i]; f1.v[c] = in[c][2 * i + 1]; }
+        qm r = q_add(q_add(f0, f1), q_mul(al, q_mulm(q_sub(f0, f1), tw[i])));
+        for (int c = 0; c < 4; c++) out[c][i] = r.v[c];
+    }
+}
+void vxo_fold_circle_into_line(uint32_t *const dst[4], const uint32_t *const src[4], const uint32_t *tw,
+                               const uint32_t alpha[4], const uint32_t alpha_sq[4], uint64_t half_n) {
+    qm al, al2; memcpy(al.v, alpha, 16); memcpy(al2.v, alpha_sq, 16);
+    #pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)half_n; i++) {
+        qm f0, f1, prev;
+        for (int c = 0; c < 4; c++) { f0.v[c] = src[c][2 * i]; f1.v[c] = src[c][2 * i + 1]; prev.v[c] = dst[c][i]; }
+        qm fp = q_add(q_add(f0, f1), q_mul(al, q_mulm(q_sub(f0, f1), tw[i])));
+        qm r = q_add(q_mul(prev, al2), fp);
+        for (int c = 0; c < 4; c++) dst[c][i] = r.v[c];
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* channel: channel.rs:15-185                                         */
+/* ------------------------------------------------------------------ */
+void vxo_channel_init(vxo_channel *ch) { memset(ch->state, 0, 32); ch->n_draws = 0; }
+void vxo_channel_mix_digest(vxo_channel *ch, const uint32_t d[8]) {
+    uint8_t in[64];
+    memcpy(in, ch->state, 32);
+    for (int i = 0; i < 8; i++) st32(in + 32 + 4 * i, d[i]);
+    vxo_blake2s(in, 64, ch->state);
+    ch->n_draws = 0;
+}
+void vxo_channel_mix_felts(vxo_channel *ch, const uint32_t *f, size_t nf) {
+    if (!nf) return;
+    size_t len = 32 + 16 * nf;
+    uint8_t *in = (uint8_t *)malloc(len);
+    memcpy(in, ch->state, 32);
+    for (size_t i = 0; i < 4 * nf; i++) st32(in + 32 + 4 * i, f[i]);
+    vxo_blake2s(in, len, ch->state);
+    free(in);
+    ch->n_draws = 0;
+}
+static void squeeze(vxo_channel *ch, uint8_t out[32]) {
+    uint8_t in[37];
+    memcpy(in, ch->state, 32);
+    st32(in + 32, ch->n_draws);
+    in[36] = 0;
+    ch->n_draws++;
+    vxo_blake2s(in, 37, out);
+}
+void vxo_channel_draw_felt(vxo_channel *ch, uint32_t out[4]) {
+    for (;;) {
+        uint8_t b[32];
+        squeeze(ch, b);
+        uint32_t w[8];
+        int ok = 1;
+        for (int i = 0; i < 8; i++) { w[i] = ld32(b + 4 * i); if (w[i] >= 2 * P) ok = 0; }
+        if (ok) { for (int i = 0; i < 4; i++) out[i] = w[i] % P; return; }
+    }
+}
+uint64_t vxo_channel_draw_number(vxo_channel *ch, uint64_t bound) {
+    uint8_t b[32];
+    squeeze(ch, b);
+    uint64_t raw = (uint64_t)ld32(b) | ((uint64_t)ld32(b + 4) << 32);
+    return raw % bound;
+}
+void vxo_channel_draw_query_indices(vxo_channel *ch, uint32_t log_domain, uint32_t n, uint32_t *out) {
+    uint32_t mask = (uint32_t)((1ull << log_domain) - 1), got = 0;
+    while (got < n) {
+        uint8_t b[32];
+        squeeze(ch, b);
+        for (int i = 0; i < 8 && got < n; i++) out[got++] = ld32(b + 4 * i) & mask;
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* whole proof: prover.rs:264-619, bytes: stark_cli.rs:1051-1123      */
+/* ------------------------------------------------------------------ */
+typedef struct { uint8_t *p; size_t n, cap; } wbuf;
+static void wr(wbuf *w, uint32_t v) {
+    if (w->n + 4 > w->cap) { w->cap = w->cap * 2 + 4096; w->p = (uint8_t *)realloc(w->p, w->cap); }
+    st32(w->p + w->n, v); w->n += 4;
+}
+static void wrs(wbuf *w, const uint32_t *s, size_t k) { for (size_t i = 0; i < k; i++) wr(w, s[i]); }
+
+size_t vxo_proof_size(uint32_t log_n, uint32_t B, uint32_t nq) {
+    uint32_t le = log_n + B, nfri = le - 3;
+    size_t s = 4 * (5 + 8 + 8 + 1 + 8 * (size_t)nfri + 1 + 4 * 8 + 1 + nq);
+    s += 4 + 8 * (size_t)nq + 2 * (size_t)nq * (4 + 32 * (size_t)le);
+    s += 4 + 32 * (size_t)nq + 2 * (size_t)nq * (4 + 32 * (size_t)le);
+    s += 4;
+    for (uint32_t k = 0; k < nfri; k++) {
+        uint32_t d = le - 1 - k;
+        s += 4 + 32 * (size_t)nq + 2 * (size_t)nq * (4 + 32 * (size_t)d);
+    }
+    return s;
+}
+
+/* one decommitment block: n, values, sibling values, paths, sibling paths */
+static void write_decom(wbuf *w, const vxo_tree *t, const uint32_t *const *cols, uint32_t nc,
+                        const uint64_t *idx, uint32_t nq) {
+    wr(w, nq);
+    for (uint32_t q = 0; q < nq; q++) for (uint32_t c = 0; c < nc; c++) wr(w, cols[c][idx[q]]);
+    for (uint32_t q = 0; q < nq; q++) for (uint32_t c = 0; c < nc; c++) wr(w, cols[c][idx[q] ^ 1]);
+    uint32_t *path = (uint32_t *)malloc(((size_t)t->log_n + 1) * 32);
+    for (int s = 0; s < 2; s++)
+        for (uint32_t q = 0; q < nq; q++) {
+            vxo_tree_path(t, idx[q] ^ (uint64_t)s, path);
+            wr(w, t->log_n);
+            wrs(w, path, 8 * (size_t)t->log_n);
+        }
+    free(path);
+}
+
+static vxo_coset eval_domain(uint32_t le) { return le <= 30 ? vxo_coset_half_coset(le) : vxo_coset_subgroup(le); }
+
+static int prove_impl(uint32_t a, uint32_t b, uint32_t log_n, uint32_t B, uint32_t nq,
+                      uint8_t **out, size_t *out_len, uint32_t *roots_out) {
+    if (log_n < 4 || log_n + B > 31 || a >= P || b >= P) return 1;
+    uint32_t le = log_n + B;
+    uint64_t n = 1ull << log_n, N = 1ull << le;
+    /* trace -> interpolate on half_coset(log_n) */
+    uint32_t *eval = (uint32_t *)calloc(N, 4);
+    vxo_fibonacci_trace(a, b, log_n, eval);
+    vxo_coset tdom = vxo_coset_half_coset(log_n);
+    vxo_interpolate_on(eval, &tdom);
+    /* zero pad (already zero) -> evaluate on the eval domain */
+    vxo_coset edom = eval_domain(le);
+    vxo_evaluate_on(eval, &edom);
+    (void)n;
+    /* trace commitment */
+    vxo_tree ttree;
+    const uint32_t *tcols[1] = {eval};
+    vxo_tree_build(&ttree, tcols, 1, le);
+    uint32_t troot[8]; vxo_tree_root(&ttree, troot);
+    vxo_channel ch; vxo_channel_init(&ch);
+    vxo_channel_mix_digest(&ch, troot);
+    uint32_t alpha[4]; vxo_channel_draw_felt(&ch, alpha);
+    /* quotient + commitment */
+    uint32_t *q[4];
+    for (int c = 0; c < 4; c++) q[c] = (uint32_t *)malloc(N * 4);
+    vxo_fibonacci_quotient(eval, N, alpha, q[0], q[1], q[2], q[3]);
+    vxo_tree qtree;
+    vxo_tree_build(&qtree, (const uint32_t *const *)q, 4, le);
+    uint32_t qroot[8]; vxo_tree_root(&qtree, qroot);
+    vxo_channel_mix_digest(&ch, qroot);
+    /* FRI */
+    uint32_t nfri = le - 3;
+    uint32_t **lay = (uint32_t **)calloc((size_t)nfri * 4, sizeof(uint32_t *));
+    vxo_tree *ftree = (vxo_tree *)calloc(nfri, sizeof(vxo_tree));
+    uint32_t *froots = (uint32_t *)malloc((size_t)nfri * 32);
+    uint32_t fa[4]; vxo_channel_draw_felt(&ch, fa);
+    uint32_t fa2[4]; vxo_qm31_mul(fa, fa, fa2);
+    uint32_t *tw = (uint32_t *)malloc((N / 2) * 4);
+    vxo_fold_twiddles(&edom, 1, tw);
+    for (int c = 0; c < 4; c++) lay[c] = (uint32_t *)calloc(N / 2, 4);
+    vxo_fold_circle_into_line(lay, (const uint32_t *const *)q, tw, fa, fa2, N / 2);
+    uint32_t cur = le - 1;
+    vxo_tree_build(&ftree[0], (const uint32_t *const *)lay, 4, cur);
+    vxo_tree_root(&ftree[0], froots);
+    vxo_channel_mix_digest(&ch, froots);
+    for (uint32_t k = 1; k < nfri; k++) {
+        uint32_t al[4]; vxo_channel_draw_felt(&ch, al);
+        vxo_coset dom = vxo_coset_half_odds(cur);
+        uint64_t half = 1ull << (cur - 1);
+        vxo_fold_twiddles(&dom, 0, tw);
+        for (int c = 0; c < 4; c++) lay[4 * k + c] = (uint32_t *)malloc(half * 4);
+        vxo_fold_line((const uint32_t *const *)(lay + 4 * (k - 1)), tw, al, lay + 4 * k, half);
+        cur--;
+        vxo_tree_build(&ftree[k], (const uint32_t *const *)(lay + 4 * k), 4, cur);
+        vxo_tree_root(&ftree[k], froots + 8 * k);
+        vxo_channel_mix_digest(&ch, froots + 8 * k);
+    }
+    free(tw);
+    /* last layer (8 QM31) -> mix_felts -> queries */
+    uint32_t last[32];
+    for (int i = 0; i < 8; i++) for (int c = 0; c < 4; c++) last[4 * i + c] = lay[4 * (nfri - 1) + c][i];
+    vxo_channel_mix_felts(&ch, last, 8);
+    uint64_t *qi = (uint64_t *)malloc(sizeof(uint64_t) * (nq ? nq : 1));
+    for (uint32_t j = 0; j < nq; j++) qi[j] = vxo_channel_draw_number(&ch, N);
+
+    if (roots_out) {
+        memcpy(roots_out, troot, 32); memcpy(roots_out + 8, qroot, 32);
+        memcpy(roots_out + 16, froots, (size_t)nfri * 32);
+    }
+    if (out) {
+        wbuf w = {NULL, 0, 0};
+        w.cap = vxo_proof_size(log_n, B, nq); w.p = (uint8_t *)malloc(w.cap);
+        wr(&w, 0x4B52414Bu); wr(&w, 1); wr(&w, log_n); wr(&w, a); wr(&w, b);
+        wrs(&w, troot, 8); wrs(&w, qroot, 8);
+        wr(&w, nfri); wrs(&w, froots, 8 * (size_t)nfri);
+        wr(&w, 8); wrs(&w, last, 32);
+        wr(&w, nq); for (uint32_t j = 0; j < nq; j++) wr(&w, (uint32_t)qi[j]);
+        write_decom(&w, &ttree, tcols, 1, qi, nq);
+        write_decom(&w, &qtree, (const uint32_t *const *)q, 4, qi, nq);
+        wr(&w, nfri);
+        uint64_t *fi = (uint64_t *)malloc(sizeof(uint64_t) * (nq ? nq : 1));
+        for (uint32_t j = 0; j < nq; j++) fi[j] = qi[j] >> 1;
+        for (uint32_t k = 0; k < nfri; k++) {
+            write_decom(&w, &ftree[k], (const uint32_t *const *)(lay + 4 * k), 4, fi, nq);
+            for (uint32_t j = 0; j < nq; j++) fi[j] >>= 1;
+        }
+        free(fi);
+        *out = w.p; *out_len = w.n;
+    }
+    free(qi);
+    for (uint32_t k = 0; k < nfri; k++) { vxo_tree_free(&ftree[k]); for (int c = 0; c < 4; c++) free(lay[4 * k + c]); }
+    free(ftree); free(lay); free(froots);
+    vxo_tree_free(&qtree); for (int c = 0; c < 4; c++) free(q[c]);
+    vxo_tree_free(&ttree); free(eval);
+    return 0;
+}
+int vxo_prove(uint32_t a, uint32_t b, uint32_t log_n, uint32_t B, uint32_t nq, uint8_t **out, size_t *out_len) {
+    return prove_impl(a, b, log_n, B, nq, out, out_len, NULL);
+}
+int vxo_prove_roots(uint32_t a, uint32_t b, uint32_t log_n, uint32_t B,
+                    uint32_t *tr, uint32_t *qr, uint32_t *fr) {
+    uint32_t le = log_n + B;
+    uint32_t *r = (uint32_t *)malloc((size_t)(2 + le) * 32);
+    int rc = prove_impl(a, b, log_n, B, 0, NULL, NULL, r);
+    if (!rc) { memcpy(tr, r, 32); memcpy(qr, r + 8, 32); memcpy(fr, r + 16, (size_t)(le - 3) * 32); }
+    free(r);
+    return rc;
+}
+void vxo_free(void *p) { free(p); }
+void vxo_set_threads(int n) {
+#ifdef _OPENMP
+    omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+int vxo_get_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+/* ------------------------------------------------------------------ */
+/* verifier.rs:39-310 over the byte layout                             */
+/* ------------------------------------------------------------------ */
+typedef struct { const uint8_t *p; size_t n, off; int bad; } rbuf;
+static uint32_t rd(rbuf *r) {
+    if (r->off + 4 > r->n) { r->bad = 1; return 0; }
+    uint32_t v = ld32(r->p + r->off); r->off += 4; return v;
+}
+#define FAIL(code, ...) do { if (msg) snprintf(msg, msg_len, __VA_ARGS__); rc = code; goto done; } while (0)
+
+typedef struct { uint32_t n; uint32_t *vals, *svals; uint32_t *paths, *spaths; uint32_t depth_ok; } decom_t;
+static int read_decom(rbuf *r, decom_t *d, uint32_t width, uint32_t depth) {
+    d->n = rd(r);
+    if (r->bad || d->n > (1u << 20)) return 0;
+    d->vals = (uint32_t *)malloc((size_t)d->n * width * 4 + 4);
+    d->svals = (uint32_t *)malloc((size_t)d->n * width * 4 + 4);
+    d->paths = (uint32_t *)malloc((size_t)d->n * depth * 32 + 4);
+    d->spaths = (uint32_t *)malloc((size_t)d->n * depth * 32 + 4);
+    d->depth_ok = 1;
+    for (size_t i = 0; i < (size_t)d->n * width; i++) d->vals[i] = rd(r);
+    for (size_t i = 0; i < (size_t)d->n * width; i++) d->svals[i] = rd(r);
+    for (int s = 0; s < 2; s++)
+        for (uint32_t q = 0; q < d->n; q++) {
+            uint32_t dep = rd(r);
+            if (dep != depth) { d->depth_ok = 0; r->bad = 1; return 0; }
+            uint32_t *dst = (s ? d->spaths : d->paths) + (size_t)q * depth * 8;
+            for (uint32_t i = 0; i < depth * 8; i++) dst[i] = rd(r);
+        }
+    return !r->bad;
+}
+static void free_decom(decom_t *d) { free(d->vals); free(d->svals); free(d->paths); free(d->spaths); }
+static int check_decom(const decom_t *d, const uint32_t root[8], const uint64_t *idx, uint32_t width, uint32_t depth, uint32_t nq) {
+    if (d->n != nq) return 0;
+    for (uint32_t q = 0; q < nq; q++) {
+        uint32_t h[8];
+        hash_words16(d->vals + (size_t)q * width, width, h);
+        if (!vxo_verify_path(root, h, idx[q], d->paths + (size_t)q * depth * 8, depth)) return 0;
+        hash_words16(d->svals + (size_t)q * width, width, h);
+        if (!vxo_verify_path(root, h, idx[q] ^ 1, d->spaths + (size_t)q * depth * 8, depth)) return 0;
+    }
+    return 1;
+}
+static qm fold_pair(qm f0, qm f1, qm al, uint32_t tw) {
+    return q_add(q_add(f0, f1), q_mul(al, q_mulm(q_sub(f0, f1), tw)));
+}
+static uint32_t fold_tw_at(const vxo_coset *dom, uint64_t fi, int circle) {
+    vxo_point p = vxo_coset_at(dom, brev(fi << 1, dom->log_size));
+    return vxo_m31_inv(circle ? p.y : p.x);
+}
+int vxo_verify(const uint8_t *proof, size_t len, uint32_t B, uint32_t nq, char *msg, size_t msg_len) {
+    int rc = 0;
+    rbuf r = {proof, len, 0, 0};
+    decom_t td = {0}, qd = {0}, *fd = NULL;
+    uint32_t nfd = 0, nfri = 0, *froots = NULL, *fal = NULL;
+    uint64_t *qi = NULL, *fi = NULL;
+    if (rd(&r) != 0x4B52414Bu) FAIL(1, "bad magic");
+    if (rd(&r) != 1) FAIL(1, "bad version");
+    uint32_t log_n = rd(&r), a = rd(&r), b = rd(&r);
+    if (r.bad || log_n < 1 || log_n + B > 31) FAIL(1, "bad log_n");
+    uint32_t le = log_n + B;
+    uint64_t N = 1ull << le;
+    if (a >= P || b >= P) FAIL(2, "public inputs out of M31 range");
+    uint32_t troot[8], qroot[8];
+    for (int i = 0; i < 8; i++) troot[i] = rd(&r);
+    for (int i = 0; i < 8; i++) qroot[i] = rd(&r);
+    nfri = rd(&r);
+    if (r.bad || nfri > 64) FAIL(1, "bad fri count");
+    froots = (uint32_t *)malloc((size_t)nfri * 32 + 4);
+    for (uint32_t i = 0; i < 8 * nfri; i++) froots[i] = rd(&r);
+    uint32_t nlast = rd(&r);
+    if (r.bad || nlast > 64) FAIL(1, "bad last layer count");
+    uint32_t last[256];
+    for (uint32_t i = 0; i < 4 * nlast; i++) last[i] = rd(&r);
+    uint32_t nqp = rd(&r);
+    if (r.bad || nqp > (1u << 20)) FAIL(1, "bad query count");
+    qi = (uint64_t *)malloc(sizeof(uint64_t) * (nqp + 1));
+    for (uint32_t j = 0; j < nqp; j++) qi[j] = rd(&r);
+    if (nqp != nq) FAIL(3, "expected %u queries, got %u", nq, nqp);
+    if (!read_decom(&r, &td, 1, le)) FAIL(1, "truncated trace decommitment");
+    if (!read_decom(&r, &qd, 4, le)) FAIL(1, "truncated quotient decommitment");
+    nfd = rd(&r);
+    if (r.bad || nfd != nfri) FAIL(1, "bad fri decommitment count");
+    fd = (decom_t *)calloc(nfd + 1, sizeof(decom_t));
+    for (uint32_t k = 0; k < nfd; k++)
+        if (!read_decom(&r, &fd[k], 4, le - 1 - k)) FAIL(1, "truncated fri decommitment %u", k);
+    if (r.off != len) FAIL(1, "trailing bytes");
+
+    /* replay transcript — verifier.rs:56-96 */
+    vxo_channel ch; vxo_channel_init(&ch);
+    vxo_channel_mix_digest(&ch, troot);
+    uint32_t tmp[4]; vxo_channel_draw_felt(&ch, tmp);
+    vxo_channel_mix_digest(&ch, qroot);
+    fal = (uint32_t *)malloc(((size_t)nfri + 1) * 16);
+    vxo_channel_draw_felt(&ch, fal);
+    for (uint32_t k = 0; k < nfri; k++) { vxo_channel_mix_digest(&ch, froots + 8 * k); vxo_channel_draw_felt(&ch, fal + 4 * (k + 1)); }
+    if (nfri != le - 3) FAIL(4, "expected %u FRI layers, got %u", le - 3, nfri);
+    if (nlast != 8) FAIL(4, "expected 8 last-layer values, got %u", nlast);
+    vxo_channel_mix_felts(&ch, last, nlast);
+    for (uint32_t j = 0; j < nq; j++) if (vxo_channel_draw_number(&ch, N) != qi[j]) FAIL(5, "query indices don't match Fiat-Shamir derivation");
+    static const uint32_t Z[8] = {0};
+    if (!memcmp(troot, Z, 32)) FAIL(6, "trace commitment is zero");
+    if (!memcmp(qroot, Z, 32)) FAIL(6, "quotient commitment is zero");
+    if (!check_decom(&td, troot, qi, 1, le, nq)) FAIL(7, "trace auth path invalid");
+    if (!check_decom(&qd, qroot, qi, 4, le, nq)) FAIL(7, "quotient auth path invalid");
+    fi = (uint64_t *)malloc(sizeof(uint64_t) * (nq + 1));
+    for (uint32_t j = 0; j < nq; j++) fi[j] = qi[j] >> 1;
+    for (uint32_t k = 0; k < nfd; k++) {
+        if (!check_decom(&fd[k], froots + 8 * k, fi, 4, le - 1 - k, nq)) FAIL(7, "FRI layer %u auth path invalid", k);
+        for (uint32_t j = 0; j < nq; j++) fi[j] >>= 1;
+    }
+    /* fold equations — verifier.rs:153-233 */
+    for (uint32_t j = 0; j < nq; j++) {
+        uint64_t ci = qi[j];
+        uint32_t cl = le;
+        vxo_coset dom = eval_domain(cl);
+        qm v, s, f0, f1, al, exp, act;
+        memcpy(v.v, qd.vals + 4 * j, 16); memcpy(s.v, qd.svals + 4 * j, 16);
+        if (ci & 1) { f0 = s; f1 = v; } else { f0 = v; f1 = s; }
+        memcpy(al.v, fal, 16);
+        exp = fold_pair(f0, f1, al, fold_tw_at(&dom, ci >> 1, 1));
+        memcpy(act.v, fd[0].vals + 4 * j, 16);
+        if (memcmp(exp.v, act.v, 16)) FAIL(8, "circle fold mismatch at query %u", j);
+        ci >>= 1; cl--;
+        for (uint32_t k = 0; k + 1 < nfd; k++) {
+            vxo_coset ld = vxo_coset_half_odds(cl);
+            memcpy(v.v, fd[k].vals + 4 * j, 16); memcpy(s.v, fd[k].svals + 4 * j, 16);
+            if (ci & 1) { f0 = s; f1 = v; } else { f0 = v; f1 = s; }
+            memcpy(al.v, fal + 4 * (k + 1), 16);
+            exp = fold_pair(f0, f1, al, fold_tw_at(&ld, ci >> 1, 0));
+            memcpy(act.v, fd[k + 1].vals + 4 * j, 16);
+            if (memcmp(exp.v, act.v, 16)) FAIL(8, "line fold mismatch at query %u layer %u", j, k);
+            ci >>= 1; cl--;
+        }
+        if (nfd > 0) {
+            if (ci >= nlast) FAIL(9, "last layer index out of bounds");
+            if (memcmp(fd[nfd - 1].vals + 4 * j, last + 4 * ci, 16)) FAIL(9, "last layer mismatch at query %u", j);
+        }
+    }
+done:
+    free_decom(&td); free_decom(&qd);
+    if (fd) { for (uint32_t k = 0; k < nfd; k++) free_decom(&fd[k]); free(fd); }
+    free(froots); free(fal); free(qi); free(fi);
+    return rc;
+}

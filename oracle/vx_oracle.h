@@ -1,0 +1,131 @@
+/*
+ * vx_oracle.h — CPU restatement of the VortexSTARK Fibonacci commitment path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker: the tests, the
+ * smoke entry and the CPU-baseline leg of the benchmark load it to produce
+ * expected outputs.  The product path (vortexstark_b200) never calls it.
+ *
+ * Every function restates the reference's arithmetic bit-exactly; the
+ * reference file:line it follows is cited beside each declaration.
+ * Pinning: Blake2s is checked against Python hashlib.blake2s, the group
+ * facts against src/circle.rs:586-622, the last-layer polynomial KAT
+ * against src/fri.rs:513-580, and the whole path against an independent
+ * pure-Python restatement (oracle/pyoracle.py) and against the reference's
+ * own CUDA kernels compiled from source (oracle/_ref, run on a B200).
+ */
+#ifndef VX_ORACLE_H
+#define VX_ORACLE_H
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VXO_P 0x7FFFFFFFu
+
+/* ---- field (src/field/m31.rs:24-35, qm31.rs:110-133) ---- */
+uint32_t vxo_m31_mul(uint32_t a, uint32_t b);
+uint32_t vxo_m31_inv(uint32_t a);
+void vxo_qm31_mul(const uint32_t a[4], const uint32_t b[4], uint32_t out[4]);
+
+/* ---- circle group (src/circle.rs:10-268) ---- */
+typedef struct { uint32_t x, y; } vxo_point;
+typedef struct { vxo_point initial, step; uint32_t log_size; } vxo_coset;
+vxo_point vxo_point_mul(vxo_point a, vxo_point b);
+vxo_point vxo_point_pow(vxo_point a, uint64_t k);
+vxo_coset vxo_coset_subgroup(uint32_t log_size);   /* circle.rs:101-109 */
+vxo_coset vxo_coset_half_coset(uint32_t log_size); /* circle.rs:113-122 */
+vxo_coset vxo_coset_half_odds(uint32_t log_size);  /* circle.rs:132-143 */
+vxo_point vxo_coset_at(const vxo_coset *c, uint64_t i); /* circle.rs:183-185 */
+
+/* ---- twiddles (circle.rs:357-550, twiddles.cu:80-142, batch_inverse.cu) ----
+ * line: m-1 words, layer l at offset offsets[l] with m>>(l+1) words;
+ * circle: m/2 words.  inverse != 0 gives elementwise inverses (0 -> 0). */
+void vxo_twiddles(const vxo_coset *c, int inverse, uint32_t *line, uint32_t *circle,
+                  uint32_t *offsets);
+void vxo_batch_inverse(const uint32_t *in, uint32_t *out, size_t n);
+
+/* ---- circle NTT (circle_ntt.cu:74-117, 248-312) ---- */
+void vxo_ntt_layer(uint32_t *d, const uint32_t *tw, uint32_t layer_idx, uint64_t n, int forward);
+void vxo_ntt_evaluate(uint32_t *d, const uint32_t *line, const uint32_t *circle,
+                      const uint32_t *offsets, uint32_t log_n);
+void vxo_ntt_interpolate(uint32_t *d, const uint32_t *iline, const uint32_t *icircle,
+                         const uint32_t *offsets, uint32_t log_n);
+/* whole-coset helpers that build their own tables */
+void vxo_evaluate_on(uint32_t *d, const vxo_coset *c);
+void vxo_interpolate_on(uint32_t *d, const vxo_coset *c);
+
+/* ---- bit reverse / permute (circle_ntt.cu:234-244, circle.rs:192-226) ---- */
+void vxo_bit_reverse(uint32_t *d, uint32_t log_n);
+void vxo_permute_hc_to_canonic_brt(const uint32_t *src, uint32_t *dst, uint32_t log_n);
+void vxo_permute_canonic_brt_to_hc(const uint32_t *src, uint32_t *dst, uint32_t log_n);
+
+/* ---- glue (constraint.cu:10-90) ---- */
+void vxo_fibonacci_trace(uint32_t a, uint32_t b, uint32_t log_n, uint32_t *out); /* air.rs:136-189 */
+void vxo_fibonacci_quotient(const uint32_t *eval, uint64_t n, const uint32_t alpha[4],
+                            uint32_t *q0, uint32_t *q1, uint32_t *q2, uint32_t *q3);
+
+/* ---- Blake2s (channel.rs:216-298, blake2s.cuh:70-136) ---- */
+void vxo_blake2s(const uint8_t *in, size_t len, uint8_t out[32]);
+void vxo_hash_leaf(const uint32_t *words, uint32_t n_words, uint32_t out[8]); /* merkle.rs:570-593 */
+void vxo_hash_pair(const uint32_t l[8], const uint32_t r[8], uint32_t out[8]); /* merkle.rs:864-884 */
+void vxo_blake2s_compress_words(uint32_t h[8], const uint32_t m[16], uint32_t t, uint32_t f);
+
+/* ---- Merkle (merkle.rs:28-130, 455-497, 841-851) ----
+ * Full tree as an array of levels: level 0 = leaves (n*8 words), top = root.
+ * cols: n_cols pointers to n-word columns; leaf = hash of the first
+ * min(n_cols,16) words of the row (blake2s.cu:25-53). */
+typedef struct { uint32_t log_n; uint32_t **levels; } vxo_tree;
+void vxo_tree_build(vxo_tree *t, const uint32_t *const *cols, uint32_t n_cols, uint32_t log_n);
+void vxo_tree_free(vxo_tree *t);
+void vxo_tree_root(const vxo_tree *t, uint32_t out[8]);
+void vxo_tree_path(const vxo_tree *t, uint64_t idx, uint32_t *out /* log_n*8 */);
+void vxo_merkle_root(const uint32_t *const *cols, uint32_t n_cols, uint32_t log_n, uint32_t out[8]);
+int vxo_verify_path(const uint32_t root[8], const uint32_t leaf[8], uint64_t idx,
+                    const uint32_t *path, uint32_t depth); /* merkle.rs:520-566 */
+/* Lifted multi-size leaves (merkle_leaves_lifted.cu:25-98): columns sorted by
+ * ascending log size; leaf idx reads row ((idx >> (S-L+1)) << 1) | (idx & 1). */
+void vxo_lifted_leaves(const uint32_t *const *cols, const uint32_t *log_sizes, uint32_t n_cols,
+                       uint32_t lifting_log, uint32_t *out /* 2^S * 8 */);
+
+/* ---- FRI (fri.rs:73-224, 411-427; fri.cu:58-126) ---- */
+void vxo_fold_twiddles(const vxo_coset *domain, int extract_y, uint32_t *out /* size/2 */);
+void vxo_fold_line(const uint32_t *const in[4], const uint32_t *tw, const uint32_t alpha[4],
+                   uint32_t *const out[4], uint64_t half_n);
+void vxo_fold_circle_into_line(uint32_t *const dst[4], const uint32_t *const src[4],
+                               const uint32_t *tw, const uint32_t alpha[4],
+                               const uint32_t alpha_sq[4], uint64_t half_n);
+
+/* ---- channel (channel.rs:15-185) ---- */
+typedef struct { uint8_t state[32]; uint32_t n_draws; } vxo_channel;
+void vxo_channel_init(vxo_channel *ch);
+void vxo_channel_mix_digest(vxo_channel *ch, const uint32_t d[8]);
+void vxo_channel_mix_felts(vxo_channel *ch, const uint32_t *felts, size_t n_felts);
+void vxo_channel_draw_felt(vxo_channel *ch, uint32_t out[4]);
+uint64_t vxo_channel_draw_number(vxo_channel *ch, uint64_t bound);
+void vxo_channel_draw_query_indices(vxo_channel *ch, uint32_t log_domain, uint32_t n, uint32_t *out);
+
+/* ---- whole proof (prover.rs:264-619; stark_cli.rs:1051-1123) ----
+ * Returns the proof in the reference's "KRAK" v1 byte layout.  The caller
+ * frees *out with vxo_free.  Returns 0 on success. */
+int vxo_prove(uint32_t a, uint32_t b, uint32_t log_n, uint32_t blowup_bits, uint32_t n_queries,
+              uint8_t **out, size_t *out_len);
+/* Proof size in bytes for (log_n, blowup_bits, n_queries). */
+size_t vxo_proof_size(uint32_t log_n, uint32_t blowup_bits, uint32_t n_queries);
+/* verifier.rs:39-310 on the byte layout; returns 0 if accepted, else a
+ * positive code; msg (if non-NULL) receives a short reason. */
+int vxo_verify(const uint8_t *proof, size_t len, uint32_t blowup_bits, uint32_t n_queries,
+               char *msg, size_t msg_len);
+/* Commitment values of a proof, for diagnostics: trace root, quotient
+ * root, fri roots (count = log_eval-3). */
+int vxo_prove_roots(uint32_t a, uint32_t b, uint32_t log_n, uint32_t blowup_bits,
+                    uint32_t *trace_root, uint32_t *quotient_root, uint32_t *fri_roots);
+void vxo_free(void *p);
+void vxo_set_threads(int n);
+int vxo_get_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,274 @@
+"""Every reference-compatible launcher of libvortex_b200 against the oracle.
+
+Bit-exact equality on seeded inputs (all arithmetic is exact integer work).
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from gpu_util import empty, to_dev, to_host
+from vortexstark_b200 import _lib
+from vortexstark_b200.workload import m31_array
+
+pytestmark = pytest.mark.gpu
+P = 0x7FFFFFFF
+
+
+@pytest.fixture(scope="module")
+def L():
+    return _lib.lib()
+
+
+def _cos(oracle, kind, k):
+    from vortexstark_b200.circle import Coset
+    pc = {"half_coset": Coset.half_coset, "half_odds": Coset.half_odds, "subgroup": Coset.subgroup}[kind](k)
+    return pc, oracle.coset(kind, k)
+
+
+@pytest.mark.parametrize("kind", ["half_coset", "half_odds", "subgroup"])
+@pytest.mark.parametrize("k", [1, 2, 3, 5, 8, 12])
+def test_twiddle_tables(oracle, kind, k):
+    from vortexstark_b200.circle import compute_forward_twiddles_gpu, compute_inverse_twiddles_gpu
+    pc, oc = _cos(oracle, kind, k)
+    line, circ, offs, sizes = compute_forward_twiddles_gpu(pc)
+    oline, ocirc, ooffs = oracle.twiddles(oc, False)
+    assert np.array_equal(to_host(circ, 1 << (k - 1)), ocirc)
+    # the flat line table has 2^k - 1 slots of which the layers fill 2^k - 2
+    # (circle.rs:479); the last slot is never written or read
+    assert np.array_equal(to_host(line, (1 << k) - 2), oline[:(1 << k) - 2])
+    assert list(offs) == ooffs.tolist()
+    il, ic, _, _ = compute_inverse_twiddles_gpu(pc)
+    oil, oic, _ = oracle.twiddles(oc, True)
+    assert np.array_equal(to_host(ic, 1 << (k - 1)), oic)
+    assert np.array_equal(to_host(il, (1 << k) - 2), oil[:(1 << k) - 2])
+
+
+@pytest.mark.parametrize("kind", ["half_coset", "half_odds", "subgroup"])
+@pytest.mark.parametrize("k", [1, 2, 4, 7, 11, 12, 13, 16, 20])
+def test_ntt_evaluate_interpolate(oracle, kind, k):
+    from vortexstark_b200 import ntt
+    pc, oc = _cos(oracle, kind, k)
+    cache = ntt.TwiddleCache(pc)
+    x = m31_array(1000 + k, 1 << k)
+    d = to_dev(x)
+    ntt.evaluate(d, cache)
+    ev = to_host(d)
+    assert np.array_equal(ev, oracle.ntt_evaluate(x, oc))
+    ntt.interpolate(d, cache)
+    assert np.array_equal(to_host(d), oracle.ntt_interpolate(ev, oc))
+    if kind == "half_coset":
+        assert np.array_equal(to_host(d), x)  # round trip (ntt.rs:386-449)
+
+
+def test_ntt_large_round_trip(oracle):
+    from vortexstark_b200 import ntt
+    from vortexstark_b200.circle import Coset
+    k = 24
+    cache = ntt.TwiddleCache(Coset.half_coset(k))
+    x = m31_array(24, 1 << k)
+    d = to_dev(x)
+    ntt.evaluate(d, cache)
+    ev = to_host(d)
+    assert np.array_equal(ev[:4096], oracle.ntt_evaluate(x, oracle.coset("half_coset", k))[:4096])
+    ntt.interpolate(d, cache)
+    assert np.array_equal(to_host(d), x)
+
+
+@pytest.mark.parametrize("k", [6, 13])
+def test_ntt_batch(oracle, k):
+    from vortexstark_b200 import ntt
+    pc, oc = _cos(oracle, "half_coset", k)
+    cache = ntt.TwiddleCache(pc)
+    xs = [m31_array(50 + i, 1 << k) for i in range(5)]
+    ds = [to_dev(x) for x in xs]
+    ntt.evaluate_batch(ds, cache)
+    evs = [to_host(d) for d in ds]
+    for x, e in zip(xs, evs):
+        assert np.array_equal(e, oracle.ntt_evaluate(x, oc))
+    ntt.interpolate_batch(ds, cache)
+    for x, d in zip(xs, ds):
+        assert np.array_equal(to_host(d), x)
+
+
+def test_ntt_single_layers(oracle, L):
+    """prover.rs:2491-2574 through cuda_circle_ntt_layer."""
+    from vortexstark_b200.circle import Coset, compute_forward_twiddles_gpu
+    k = 10
+    line, circ, offs, sizes = compute_forward_twiddles_gpu(Coset.half_coset(k))
+    x = m31_array(7, 1 << k)
+    d = to_dev(x)
+    for l in range(k - 2, -1, -1):
+        L.cuda_circle_ntt_layer(d.data_ptr(), line.data_ptr() + 4 * offs[l], l + 1, 1 << k, 1)
+    L.cuda_circle_ntt_layer(d.data_ptr(), circ.data_ptr(), 0, 1 << k, 1)
+    assert np.array_equal(to_host(d), oracle.ntt_evaluate(x, oracle.coset("half_coset", k)))
+
+
+@pytest.mark.parametrize("k", [1, 5, 10, 17])
+def test_bit_reverse_and_permute(oracle, L, k):
+    x = m31_array(k, 1 << k)
+    d = to_dev(x)
+    L.cuda_bit_reverse_m31(d.data_ptr(), k)
+    assert np.array_equal(to_host(d), oracle.bit_reverse(x))
+    s, t = to_dev(x), empty(1 << k)
+    L.cuda_permute_hc_to_canonic_brt(s.data_ptr(), t.data_ptr(), 1 << k, k)
+    assert np.array_equal(to_host(t, 1 << k), oracle.permute_hc_to_canonic_brt(x))
+    u = empty(1 << k)
+    L.cuda_permute_canonic_brt_to_hc_natural(t.data_ptr(), u.data_ptr(), 1 << k, k)
+    assert np.array_equal(to_host(u, 1 << k), x)
+
+
+def test_batch_inverse(oracle, L):
+    x = m31_array(5, 10000)
+    x[0] = 0
+    x[640] = 0
+    x[777] = 0
+    x[9999] = 0
+    d, o = to_dev(x), empty(len(x))
+    L.cuda_batch_inverse_m31(d.data_ptr(), o.data_ptr(), len(x))
+    assert np.array_equal(to_host(o, len(x)), oracle.batch_inverse(x))
+
+
+@pytest.mark.parametrize("kind,ey", [("half_coset", 1), ("half_odds", 0), ("subgroup", 1), ("half_coset", 0)])
+@pytest.mark.parametrize("k", [2, 7, 15])
+def test_fold_twiddles(oracle, kind, ey, k):
+    from vortexstark_b200.fri import compute_fold_twiddles_on_demand
+    pc, oc = _cos(oracle, kind, k)
+    got = to_host(compute_fold_twiddles_on_demand(pc, bool(ey)), 1 << (k - 1))
+    assert np.array_equal(got, oracle.fold_twiddles(oc, bool(ey)))
+
+
+def test_zero_pad_and_quotient(oracle, L):
+    n, N = 1 << 10, 1 << 12
+    x = m31_array(3, n)
+    s, d = to_dev(x), empty(N)
+    L.cuda_zero_pad(s.data_ptr(), d.data_ptr(), n, N)
+    pad = to_host(d, N)
+    assert np.array_equal(pad[:n], x) and not pad[n:].any()
+    ev = m31_array(4, N)
+    alpha = (123, 456, 789, 1011)
+    dev = to_dev(ev)
+    q = [empty(N) for _ in range(4)]
+    L.cuda_fibonacci_quotient(dev.data_ptr(), *[c.data_ptr() for c in q], (C.c_uint32 * 4)(*alpha), N)
+    want = oracle.fibonacci_quotient(ev, alpha)
+    for c in range(4):
+        assert np.array_equal(to_host(q[c], N), want[c])
+    qc = [empty(512) for _ in range(4)]
+    L.cuda_fibonacci_quotient_chunk(dev.data_ptr(), *[c.data_ptr() for c in qc], (C.c_uint32 * 4)(*alpha), N - 512,
+                                    512, N)
+    for c in range(4):
+        assert np.array_equal(to_host(qc[c], 512), want[c][N - 512:])
+
+
+def _ptrs(ts):
+    import torch
+    return torch.tensor([t.data_ptr() for t in ts], dtype=torch.int64, device="cuda")
+
+
+def _tree_levels(oracle, cols):
+    """Oracle leaf and node hashes level by level (list of (n, 8) arrays)."""
+    from oracle import pyoracle as Y
+    nc = min(len(cols), 16)
+    leaves = np.array([Y.leaf([int(c[i]) for c in cols[:nc]]) for i in range(len(cols[0]))], np.uint32)
+    levels = [leaves]
+    while len(levels[-1]) > 1:
+        lv = levels[-1]
+        levels.append(np.array([Y.node(list(lv[2 * i]), list(lv[2 * i + 1])) for i in range(len(lv) // 2)], np.uint32))
+    return levels
+
+
+@pytest.mark.parametrize("ncols", [1, 4, 7, 16, 20])
+def test_merkle_leaves_nodes(oracle, L, ncols):
+    n = 256
+    cols = [m31_array(100 * ncols + i, n) for i in range(ncols)]
+    dcols = [to_dev(c) for c in cols]
+    lv = _tree_levels(oracle, cols)
+    out = empty(8 * n)
+    L.cuda_merkle_hash_leaves(_ptrs(dcols).data_ptr(), out.data_ptr(), ncols, n)
+    assert np.array_equal(to_host(out).reshape(-1, 8), lv[0])
+    if ncols in (1, 4):
+        o2 = empty(8 * n)
+        if ncols == 1:
+            L.cuda_merkle_hash_leaves_forge_single(dcols[0].data_ptr(), o2.data_ptr(), n)
+        else:
+            L.cuda_merkle_hash_leaves_forge_quad(*[c.data_ptr() for c in dcols], o2.data_ptr(), n)
+        assert np.array_equal(to_host(o2).reshape(-1, 8), lv[0])
+    par = empty(4 * n)
+    L.cuda_merkle_hash_nodes(out.data_ptr(), par.data_ptr(), n // 2)
+    assert np.array_equal(to_host(par).reshape(-1, 8), lv[1])
+    root = empty(8)
+    L.cuda_merkle_reduce_to_root(par.data_ptr(), root.data_ptr(), n // 2)
+    assert np.array_equal(to_host(root, 8), lv[-1][0])
+
+
+def test_merkle_soa4_variants(oracle, L):
+    n = 2048
+    cols = [m31_array(900 + i, n) for i in range(4)]
+    d = [to_dev(c) for c in cols]
+    lv = _tree_levels(oracle, cols)
+    root = empty(8)
+    L.cuda_merkle_commit_small_soa4(*[c.data_ptr() for c in d], root.data_ptr(), n)
+    assert np.array_equal(to_host(root, 8), lv[-1][0])
+    par = empty(4 * n)
+    L.cuda_merkle_hash_leaves_merge_soa4(*[c.data_ptr() for c in d], par.data_ptr(), n)
+    assert np.array_equal(to_host(par).reshape(-1, 8), lv[1])
+    sub = empty(16)
+    L.cuda_merkle_tiled_soa4(*[c.data_ptr() for c in d], sub.data_ptr(), n)
+    assert np.array_equal(to_host(sub).reshape(-1, 8), lv[10])
+    sub2 = empty(16)
+    L.cuda_merkle_tiled_generic(_ptrs(d).data_ptr(), sub2.data_ptr(), 4, n)
+    assert np.array_equal(to_host(sub2).reshape(-1, 8), lv[10])
+
+
+@pytest.mark.parametrize("log_n,ncols", [(12, 1), (16, 4), (20, 1)])
+def test_merkle_tree_root_and_paths(oracle, log_n, ncols):
+    from vortexstark_b200.merkle import MerkleTree, hash_leaf, verify_auth_path
+    cols = [m31_array(7 * log_n + i, 1 << log_n) for i in range(ncols)]
+    d = [to_dev(c) for c in cols]
+    want = oracle.merkle_root(cols)
+    r1, subs = MerkleTree.commit_root_only_with_subtrees(d, log_n)
+    assert r1 == tuple(want.tolist())
+    t = MerkleTree.commit(d, log_n)
+    assert t.root() == tuple(want.tolist())
+    idx = [0, 1, 5, (1 << log_n) - 1, 12345 % (1 << log_n)]
+    for i, pth in zip(idx, t.batch_auth_paths(idx)):
+        assert verify_auth_path(want.tolist(), hash_leaf([int(c[i]) for c in cols]), i, pth)
+
+
+def test_lifted_leaves(oracle):
+    from vortexstark_b200.merkle import build_leaves_lifted
+    sizes = [6] * 3 + [8] * 17 + [10] * 14   # 34 columns, ascending sizes
+    cols = [m31_array(300 + i, 1 << s) for i, s in enumerate(sizes)]
+    out = build_leaves_lifted([to_dev(c) for c in cols], 10)
+    assert np.array_equal(to_host(out).reshape(-1, 8), oracle.lifted_leaves(cols, 10))
+
+
+@pytest.mark.parametrize("k", [4, 9, 16])
+def test_folds(oracle, k):
+    from vortexstark_b200 import fri
+    from vortexstark_b200.circle import Coset
+    src = np.stack([m31_array(40 * k + c, 1 << k) for c in range(4)])
+    alpha = (42, 99, 7, 13)
+    col = fri.SecureColumn.from_words(src)
+    tw = fri.compute_fold_twiddles_on_demand(Coset.half_odds(k), False)
+    out = fri.fold_line_with_twiddles(col, alpha, tw)
+    want = oracle.fold_line(src, oracle.fold_twiddles(oracle.coset("half_odds", k), False), alpha)
+    assert np.array_equal(out.to_words(), want)
+    dst = fri.SecureColumn.zeros(1 << (k - 1))
+    twc = fri.compute_fold_twiddles_on_demand(Coset.half_coset(k), True)
+    fri.fold_circle_into_line_with_twiddles(dst, col, alpha, twc)
+    wantc = oracle.fold_circle_into_line(np.zeros((4, 1 << (k - 1)), np.uint32), src,
+                                         oracle.fold_twiddles(oracle.coset("half_coset", k), True), alpha)
+    assert np.array_equal(dst.to_words(), wantc)
+    # accumulate into a non-zero destination (dst * alpha^2 + f')
+    prev = np.stack([m31_array(7 + c, 1 << (k - 1)) for c in range(4)])
+    dst2 = fri.SecureColumn.from_words(prev)
+    fri.fold_circle_into_line_with_twiddles(dst2, col, alpha, twc)
+    want2 = oracle.fold_circle_into_line(prev, src, oracle.fold_twiddles(oracle.coset("half_coset", k), True), alpha)
+    assert np.array_equal(dst2.to_words(), want2)
+
+
+def test_no_launch_errors(L):
+    import torch
+    torch.cuda.synchronize()
+    assert _lib.last_error() == ""

@@ -1,0 +1,562 @@
+// Reference-compatible launchers (the symbols src/cuda/ffi.rs binds).
+//
+// Each keeps the reference's signature and semantics: device pointers for
+// data, host pointers for alpha[4] and layer offsets, legacy default stream
+// unless a stream is passed, and cudaDeviceSynchronize at the end of the NTT
+// evaluate / interpolate launchers (circle_ntt.cu:274, 311).  The kernels
+// are this library's own.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "vx_common.cuh"
+#include "vx_field.cuh"
+#include "vx_merkle.cuh"
+#include "vx_ntt.cuh"
+#include "vx_twiddles.cuh"
+
+namespace vx {
+
+static thread_local std::string t_err;
+
+void set_last_error(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    t_err = buf;
+    (void)code;
+}
+
+namespace {
+
+inline uint32_t log2_exact(uint64_t n) {
+    uint32_t l = 0;
+    while ((1ull << l) < n) l++;
+    return l;
+}
+
+// ---- twiddle helpers for arbitrary (initial, step) points ----
+// p_j = initial * step^j, 16 consecutive points per thread (twiddles.cu:80-105).
+__global__ void coset_points_kernel(cpoint init, cpoint step, uint32_t *xs, uint32_t *ys, uint64_t n) {
+    uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t j0 = t * 16ull;
+    if (j0 >= n) return;
+    cpoint p = pmul(init, ppow(step, j0));
+    uint64_t j1 = j0 + 16ull < n ? j0 + 16ull : n;
+    for (uint64_t j = j0; j < j1; j++) {
+        xs[j] = p.x;
+        ys[j] = p.y;
+        p = pmul(p, step);
+    }
+}
+
+__global__ void extract_squash_kernel(const uint32_t *in, uint32_t *tw_out, uint32_t *sq_out, uint64_t half_n) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= half_n) return;
+    uint32_t x = in[2 * i];
+    if (tw_out) tw_out[i] = x;
+    uint32_t x2 = mmul(x, x);
+    sq_out[i] = msub(madd(x2, x2), 1u);
+}
+
+// coord(initial * step^brev(2i, log_n)), i < n/2 (twiddles.cu:23-52).
+__global__ void fold_sources_generic_kernel(cpoint init, cpoint step, uint32_t *out, uint64_t half, uint32_t log_n,
+                                            int extract_y) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= half) return;
+    cpoint p = pmul(init, ppow(step, brev_bits((uint32_t)(i << 1), log_n)));
+    out[i] = extract_y ? p.y : p.x;
+}
+
+// ---- glue (constraint.cu) ----
+__global__ void zero_pad_kernel(const uint32_t *src, uint32_t *dst, uint64_t src_n, uint64_t dst_n) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= dst_n) return;
+    dst[i] = i < src_n ? src[i] : 0u;
+}
+
+__global__ void quotient_kernel(const uint32_t *tr, uint32_t *o0, uint32_t *o1, uint32_t *o2, uint32_t *o3,
+                                uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint64_t offset, uint64_t chunk,
+                                uint64_t global_n) {
+    uint64_t li = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (li >= chunk) return;
+    uint64_t i = offset + li;
+    uint32_t t0 = tr[i], t1 = tr[(i + 1) % global_n], t2 = tr[(i + 2) % global_n];
+    uint32_t c = msub(t2, madd(t1, t0));
+    o0[li] = mmul(a0, c); o1[li] = mmul(a1, c); o2[li] = mmul(a2, c); o3[li] = mmul(a3, c);
+}
+
+// ---- bit reverse / permute ----
+__global__ void bit_reverse_kernel(uint32_t *d, uint32_t log_n, uint64_t n) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint64_t j = brev_bits((uint32_t)i, log_n);
+    if (i < j) { uint32_t t = d[i]; d[i] = d[j]; d[j] = t; }
+}
+
+__device__ __forceinline__ uint64_t hc_to_canonic_brt(uint64_t k, uint64_t n, uint32_t log_n) {
+    uint64_t cn = (k & 1ull) ? n - 1ull - (k >> 1) : (k >> 1);
+    return brev_bits((uint32_t)cn, log_n);
+}
+
+// permute.cu:30-58: forward scatters dst[j(k)] = src[k]; inverse gathers.
+__global__ void permute_kernel(const uint32_t *src, uint32_t *dst, uint64_t n, uint32_t log_n, int inverse) {
+    uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    uint64_t j = hc_to_canonic_brt(k, n, log_n);
+    if (inverse) dst[k] = src[j]; else dst[j] = src[k];
+}
+
+// ---- Merkle helpers ----
+template <class Src>
+__global__ void leaf_hash_kernel(Src src, uint32_t *hashes, uint64_t n) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    src.init();
+    uint32_t m[16];
+#pragma unroll
+    for (int w = 0; w < 16; w++) m[w] = 0u;
+    uint32_t nb = src.load(i, m);
+    uint32_t h[8];
+    blake2s_block(h, m, nb);
+    store_hash(hashes + 8 * i, h);
+}
+
+__global__ void node_hash_kernel(const uint32_t *children, uint32_t *parents, uint64_t n) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t m[16];
+    const uint4 *c = (const uint4 *)(children + 16 * i);
+    uint4 a = c[0], b = c[1], d = c[2], e = c[3];
+    m[0] = a.x; m[1] = a.y; m[2] = a.z; m[3] = a.w; m[4] = b.x; m[5] = b.y; m[6] = b.z; m[7] = b.w;
+    m[8] = d.x; m[9] = d.y; m[10] = d.z; m[11] = d.w; m[12] = e.x; m[13] = e.y; m[14] = e.z; m[15] = e.w;
+    uint32_t h[8];
+    blake2s_block(h, m, 64u);
+    store_hash(parents + 8 * i, h);
+}
+
+// Reduce the 8-word hashes in sh[0 .. 8*cnt) to sh[0..8) (block-wide).
+__device__ void block_reduce_hashes(uint32_t *sh, uint32_t cnt) {
+    for (; cnt > 1; cnt >>= 1) {
+        uint32_t h[8];
+        uint32_t t = threadIdx.x;
+        bool act = t < cnt / 2;
+        if (act) blake2s_node(h, sh + 16 * t, sh + 16 * t + 8);
+        __syncthreads();
+        if (act)
+            for (int w = 0; w < 8; w++) sh[8 * t + w] = h[w];
+        __syncthreads();
+    }
+}
+
+__global__ void reduce_to_root_kernel(const uint32_t *nodes, uint32_t *root, uint32_t n) {
+    extern __shared__ uint32_t sh[];
+    for (uint32_t i = threadIdx.x; i < 8 * n; i += blockDim.x) sh[i] = nodes[i];
+    __syncthreads();
+    block_reduce_hashes(sh, n);
+    if (threadIdx.x < 8) root[threadIdx.x] = sh[threadIdx.x];
+}
+
+// Tile of 2^tile_log leaves per block, 2^(tile_log-4) threads each hashing
+// 16 leaves into a subtree root, then a shared-memory reduction.
+template <class Src>
+__global__ void tile_root_kernel(Src src, uint32_t *roots, uint32_t tile_log) {
+    extern __shared__ uint32_t sh[];
+    src.init();
+    uint64_t base = ((uint64_t)blockIdx.x << tile_log) + ((uint64_t)threadIdx.x << 4);
+    uint32_t h[8];
+    subtree_root(src, base, 4, h);
+    for (int w = 0; w < 8; w++) sh[8 * threadIdx.x + w] = h[w];
+    __syncthreads();
+    block_reduce_hashes(sh, blockDim.x);
+    if (threadIdx.x < 8) roots[8ull * blockIdx.x + threadIdx.x] = sh[threadIdx.x];
+}
+
+// Whole small tree of n <= 2048 leaves in one block (blake2s.cu:92-189).
+template <class Src>
+__global__ void small_tree_kernel(Src src, uint32_t *root, uint32_t n) {
+    extern __shared__ uint32_t sh[];
+    src.init();
+    uint32_t t = threadIdx.x;
+    if (2 * t + 1 < n) {
+        uint32_t l[8], r[8], m[16];
+        for (int w = 0; w < 16; w++) m[w] = 0u;
+        uint32_t nb = src.load(2 * t, m);
+        blake2s_block(l, m, nb);
+        for (int w = 0; w < 16; w++) m[w] = 0u;
+        nb = src.load(2 * t + 1, m);
+        blake2s_block(r, m, nb);
+        uint32_t h[8];
+        blake2s_node(h, l, r);
+        for (int w = 0; w < 8; w++) sh[8 * t + w] = h[w];
+    }
+    __syncthreads();
+    block_reduce_hashes(sh, n / 2);
+    if (t < 8) root[t] = sh[t];
+}
+
+template <class Src>
+__global__ void leaf_merge_kernel(Src src, uint32_t *parents, uint64_t n_pairs) {
+    uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_pairs) return;
+    src.init();
+    uint32_t l[8], r[8], m[16];
+    for (int w = 0; w < 16; w++) m[w] = 0u;
+    uint32_t nb = src.load(2 * t, m);
+    blake2s_block(l, m, nb);
+    for (int w = 0; w < 16; w++) m[w] = 0u;
+    nb = src.load(2 * t + 1, m);
+    blake2s_block(r, m, nb);
+    uint32_t h[8];
+    blake2s_node(h, l, r);
+    store_hash(parents + 8 * t, h);
+}
+
+// Lifted multi-size leaf (merkle_leaves_lifted.cu:33-98): the LE words of
+// every column's lifted row, columns in schedule order, hashed as one
+// Blake2s message (full blocks non-final while data follows; the last block
+// final even when full).
+struct LiftChunk {
+    uint32_t col_indices[16];
+    uint32_t n_cols;
+    uint32_t log_size;
+};
+__global__ void lifted_leaves_kernel(const uint32_t *const *cols, const LiftChunk *sched, uint32_t n_chunks,
+                                     uint32_t S, uint32_t *out, uint64_t n) {
+    uint64_t leaf = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (leaf >= n) return;
+    uint32_t total = 0;
+    for (uint32_t c = 0; c < n_chunks; c++) total += sched[c].n_cols;
+    uint32_t h[8];
+    blake2s_init(h);
+    uint32_t buf[16];
+    for (int w = 0; w < 16; w++) buf[w] = 0u;
+    uint32_t pos = 0, seen = 0, bytes = 0;
+    for (uint32_t c = 0; c < n_chunks; c++) {
+        LiftChunk ch = sched[c];
+        uint32_t L = ch.log_size;
+        uint64_t row = (L == S) ? leaf : (((leaf >> (S - L + 1)) << 1) | (leaf & 1ull));
+        for (uint32_t i = 0; i < ch.n_cols; i++) {
+            uint32_t v = cols[ch.col_indices[i]][row];
+            // register-resident buffer: select the slot without dynamic indexing
+#pragma unroll
+            for (int w = 0; w < 16; w++) if ((uint32_t)w == pos) buf[w] = v;
+            pos++;
+            seen++;
+            if (pos == 16 && seen < total) {
+                bytes += 64;
+                blake2s_compress(h, buf, bytes, false);
+                pos = 0;
+#pragma unroll
+                for (int w = 0; w < 16; w++) buf[w] = 0u;
+            }
+        }
+    }
+    bytes += 4 * pos;
+    blake2s_compress(h, buf, bytes, true);
+    store_hash(out + 8 * leaf, h);
+}
+
+// ---- FRI folds with host-side alpha (fri.cu:58-126) ----
+__global__ void fold_line_kernel(const uint32_t *i0, const uint32_t *i1, const uint32_t *i2, const uint32_t *i3,
+                                 const uint32_t *tw, uint32_t *o0, uint32_t *o1, uint32_t *o2, uint32_t *o3, qm31 al,
+                                 uint64_t half) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= half) return;
+    qm31 f0{{i0[2 * i], i1[2 * i], i2[2 * i], i3[2 * i]}}, f1{{i0[2 * i + 1], i1[2 * i + 1], i2[2 * i + 1], i3[2 * i + 1]}};
+    qm31 r = qadd(qadd(f0, f1), qmul(al, qmulm(qsub(f0, f1), tw[i])));
+    o0[i] = r.v[0]; o1[i] = r.v[1]; o2[i] = r.v[2]; o3[i] = r.v[3];
+}
+__global__ void fold_circle_kernel(uint32_t *d0, uint32_t *d1, uint32_t *d2, uint32_t *d3, const uint32_t *s0,
+                                   const uint32_t *s1, const uint32_t *s2, const uint32_t *s3, const uint32_t *tw,
+                                   qm31 al, qm31 al2, uint64_t half) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= half) return;
+    qm31 f0{{s0[2 * i], s1[2 * i], s2[2 * i], s3[2 * i]}}, f1{{s0[2 * i + 1], s1[2 * i + 1], s2[2 * i + 1], s3[2 * i + 1]}};
+    qm31 fp = qadd(qadd(f0, f1), qmul(al, qmulm(qsub(f0, f1), tw[i])));
+    qm31 prev{{d0[i], d1[i], d2[i], d3[i]}};
+    qm31 r = qadd(qmul(prev, al2), fp);
+    d0[i] = r.v[0]; d1[i] = r.v[1]; d2[i] = r.v[2]; d3[i] = r.v[3];
+}
+
+NttTables ref_tables(const uint32_t *line, const uint32_t *circle, const uint32_t *h_offsets, uint32_t n_line) {
+    NttTables t{line, circle, {}};
+    for (uint32_t l = 0; l < n_line && l < 32; l++) t.off[l] = h_offsets[l];
+    return t;
+}
+
+// Reference order (circle_ntt.cu:248-312) as per-layer launches, used when
+// the caller's layer count is not the full transform.
+void ref_layers(uint32_t *d, const uint32_t *line, const uint32_t *circle, const uint32_t *h_off, uint32_t n_line,
+                uint32_t log_n, bool forward) {
+    if (forward) {
+        for (int l = (int)n_line - 1; l >= 0; l--) ntt_single_layer(d, line + h_off[l], (uint32_t)l + 1, log_n, true, 0);
+        ntt_single_layer(d, circle, 0, log_n, true, 0);
+    } else {
+        ntt_single_layer(d, circle, 0, log_n, false, 0);
+        for (uint32_t l = 0; l < n_line; l++) ntt_single_layer(d, line + h_off[l], l + 1, log_n, false, 0);
+    }
+}
+
+__global__ void scale_kernel(uint32_t *d, uint32_t s, uint64_t n) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) d[i] = mmul(d[i], s);
+}
+
+}  // namespace
+}  // namespace vx
+
+using namespace vx;
+
+extern "C" {
+
+const char *vx_last_error(void) { return t_err.c_str(); }
+int vx_version(void) { return 100; }
+
+// ---------------- NTT ----------------
+void cuda_circle_ntt_evaluate(uint32_t *d, const uint32_t *tw, const uint32_t *ctw, const uint32_t *h_off,
+                              const uint32_t *h_sizes, uint32_t n_line, uint32_t n) {
+    (void)h_sizes;
+    uint32_t log_n = log2_exact(n);
+    if (n_line + 1 == log_n) {
+        cudaError_t e = ntt_transform(d, nullptr, 0, 1, log_n, ref_tables(tw, ctw, h_off, n_line), true, nullptr, 0, 0);
+        if (e != cudaSuccess) set_last_error(VX_ERR_CUDA, "cuda_circle_ntt_evaluate: %s", cudaGetErrorString(e));
+    } else {
+        ref_layers(d, tw, ctw, h_off, n_line, log_n, true);
+        VX_LAUNCH_CHECK();
+    }
+    cudaDeviceSynchronize();
+}
+
+void cuda_circle_ntt_interpolate(uint32_t *d, const uint32_t *itw, const uint32_t *ictw, const uint32_t *h_off,
+                                 const uint32_t *h_sizes, uint32_t n_line, uint32_t n) {
+    (void)h_sizes;
+    uint32_t log_n = log2_exact(n);
+    if (n_line + 1 == log_n) {
+        cudaError_t e = ntt_transform(d, nullptr, 0, 1, log_n, ref_tables(itw, ictw, h_off, n_line), false, nullptr, 0, 0);
+        if (e != cudaSuccess) set_last_error(VX_ERR_CUDA, "cuda_circle_ntt_interpolate: %s", cudaGetErrorString(e));
+    } else {
+        ref_layers(d, itw, ictw, h_off, n_line, log_n, false);
+        uint32_t e2 = (30u * log_n) % 31u;
+        scale_kernel<<<blocks_for(n, 256), 256>>>(d, e2 == 0 ? 1u : (1u << e2), n);
+        VX_LAUNCH_CHECK();
+    }
+    cudaDeviceSynchronize();
+}
+
+void cuda_circle_ntt_evaluate_batch(uint32_t **cols, const uint32_t *tw, const uint32_t *ctw, const uint32_t *h_off,
+                                    const uint32_t *h_sizes, uint32_t n_line, uint32_t n, uint32_t n_cols) {
+    (void)h_sizes;
+    uint32_t log_n = log2_exact(n);
+    if (n_cols) {
+        cudaError_t e = ntt_transform(nullptr, cols, 0, n_cols, log_n, ref_tables(tw, ctw, h_off, n_line), true, nullptr, 0, 0);
+        if (e != cudaSuccess) set_last_error(VX_ERR_CUDA, "cuda_circle_ntt_evaluate_batch: %s", cudaGetErrorString(e));
+    }
+    cudaDeviceSynchronize();
+}
+
+void cuda_circle_ntt_interpolate_batch(uint32_t **cols, const uint32_t *itw, const uint32_t *ictw,
+                                       const uint32_t *h_off, const uint32_t *h_sizes, uint32_t n_line, uint32_t n,
+                                       uint32_t n_cols) {
+    (void)h_sizes;
+    uint32_t log_n = log2_exact(n);
+    if (n_cols) {
+        cudaError_t e = ntt_transform(nullptr, cols, 0, n_cols, log_n, ref_tables(itw, ictw, h_off, n_line), false, nullptr, 0, 0);
+        if (e != cudaSuccess) set_last_error(VX_ERR_CUDA, "cuda_circle_ntt_interpolate_batch: %s", cudaGetErrorString(e));
+    }
+    cudaDeviceSynchronize();
+}
+
+void cuda_circle_ntt_layer(uint32_t *d, const uint32_t *tw, uint32_t layer_idx, uint32_t n, int forward) {
+    ntt_single_layer(d, tw, layer_idx, log2_exact(n), forward != 0, 0);
+    VX_LAUNCH_CHECK();
+}
+
+void cuda_bit_reverse_m31(uint32_t *data, uint32_t log_n) {
+    uint64_t n = 1ull << log_n;
+    bit_reverse_kernel<<<blocks_for(n, 256), 256>>>(data, log_n, n);
+    VX_LAUNCH_CHECK();
+}
+
+void cuda_permute_hc_to_canonic_brt(const uint32_t *src, uint32_t *dst, uint32_t n, uint32_t log_n) {
+    permute_kernel<<<blocks_for(n, 256), 256>>>(src, dst, n, log_n, 0);
+    VX_LAUNCH_CHECK();
+}
+
+void cuda_permute_canonic_brt_to_hc_natural(const uint32_t *src, uint32_t *dst, uint32_t n, uint32_t log_n) {
+    permute_kernel<<<blocks_for(n, 256), 256>>>(src, dst, n, log_n, 1);
+    VX_LAUNCH_CHECK();
+}
+
+// ---------------- twiddles ----------------
+void cuda_compute_coset_points(uint32_t ix, uint32_t iy, uint32_t sx, uint32_t sy, uint32_t *xs, uint32_t *ys,
+                               uint32_t n) {
+    uint64_t thr = (n + 15ull) / 16ull;
+    coset_points_kernel<<<blocks_for(thr, 256), 256>>>(cpoint{ix, iy}, cpoint{sx, sy}, xs, ys, n);
+    VX_LAUNCH_CHECK();
+}
+
+void cuda_squash_x(const uint32_t *in, uint32_t *out, uint32_t out_n) {
+    extract_squash_kernel<<<blocks_for(out_n, 256), 256>>>(in, nullptr, out, out_n);
+    VX_LAUNCH_CHECK();
+}
+
+void cuda_extract_and_squash(const uint32_t *in, uint32_t *tw_out, uint32_t *sq_out, uint32_t half_n) {
+    extract_squash_kernel<<<blocks_for(half_n, 256), 256>>>(in, tw_out, sq_out, half_n);
+    VX_LAUNCH_CHECK();
+}
+
+void cuda_batch_inverse_m31(const uint32_t *in, uint32_t *out, uint32_t n) {
+    cudaError_t e = batch_inverse(in, out, n, 0);
+    if (e != cudaSuccess) set_last_error(VX_ERR_CUDA, "cuda_batch_inverse_m31: %s", cudaGetErrorString(e));
+}
+
+void cuda_batch_inverse_m31_stream(const uint32_t *in, uint32_t *out, uint32_t n, void *stream) {
+    cudaError_t e = batch_inverse(in, out, n, (cudaStream_t)stream);
+    if (e != cudaSuccess) set_last_error(VX_ERR_CUDA, "cuda_batch_inverse_m31_stream: %s", cudaGetErrorString(e));
+}
+
+void cuda_compute_fold_twiddle_sources_stream(uint32_t ix, uint32_t iy, uint32_t sx, uint32_t sy, uint32_t *out,
+                                              uint32_t n, uint32_t log_n, int extract_y, void *stream) {
+    uint64_t half = n / 2;
+    fold_sources_generic_kernel<<<blocks_for(half, 256), 256, 0, (cudaStream_t)stream>>>(cpoint{ix, iy}, cpoint{sx, sy},
+                                                                                        out, half, log_n, extract_y);
+    VX_LAUNCH_CHECK();
+}
+
+void cuda_compute_fold_twiddle_sources(uint32_t ix, uint32_t iy, uint32_t sx, uint32_t sy, uint32_t *out, uint32_t n,
+                                       uint32_t log_n, int extract_y) {
+    cuda_compute_fold_twiddle_sources_stream(ix, iy, sx, sy, out, n, log_n, extract_y, nullptr);
+}
+
+// ---------------- glue ----------------
+void cuda_zero_pad(const uint32_t *src, uint32_t *dst, uint32_t src_n, uint32_t dst_n) {
+    zero_pad_kernel<<<blocks_for(dst_n, 256), 256>>>(src, dst, src_n, dst_n);
+    VX_LAUNCH_CHECK();
+}
+
+void cuda_fibonacci_quotient_chunk_stream(const uint32_t *tr, uint32_t *o0, uint32_t *o1, uint32_t *o2, uint32_t *o3,
+                                          const uint32_t *al, uint32_t offset, uint32_t chunk_n, uint32_t global_n,
+                                          void *stream) {
+    quotient_kernel<<<blocks_for(chunk_n, 256), 256, 0, (cudaStream_t)stream>>>(tr, o0, o1, o2, o3, al[0], al[1], al[2],
+                                                                               al[3], offset, chunk_n, global_n);
+    VX_LAUNCH_CHECK();
+}
+
+void cuda_fibonacci_quotient_chunk(const uint32_t *tr, uint32_t *o0, uint32_t *o1, uint32_t *o2, uint32_t *o3,
+                                   const uint32_t *al, uint32_t offset, uint32_t chunk_n, uint32_t global_n) {
+    cuda_fibonacci_quotient_chunk_stream(tr, o0, o1, o2, o3, al, offset, chunk_n, global_n, nullptr);
+}
+
+void cuda_fibonacci_quotient(const uint32_t *tr, uint32_t *o0, uint32_t *o1, uint32_t *o2, uint32_t *o3,
+                             const uint32_t *al, uint32_t n) {
+    cuda_fibonacci_quotient_chunk_stream(tr, o0, o1, o2, o3, al, 0, n, n, nullptr);
+}
+
+// ---------------- Merkle ----------------
+void cuda_merkle_hash_leaves(const uint32_t *const *cols, uint32_t *hashes, uint32_t n_cols, uint32_t n_leaves) {
+    leaf_hash_kernel<<<blocks_for(n_leaves, 128), 128>>>(LeafCols{cols, n_cols}, hashes, n_leaves);
+    VX_LAUNCH_CHECK();
+}
+
+void cuda_merkle_hash_leaves_forge_single(const uint32_t *col, uint32_t *hashes, uint32_t n_leaves) {
+    leaf_hash_kernel<<<blocks_for(n_leaves, 128), 128>>>(LeafM31{col}, hashes, n_leaves);
+    VX_LAUNCH_CHECK();
+}
+
+void cuda_merkle_hash_leaves_forge_quad(const uint32_t *c0, const uint32_t *c1, const uint32_t *c2,
+                                        const uint32_t *c3, uint32_t *hashes, uint32_t n_leaves) {
+    leaf_hash_kernel<<<blocks_for(n_leaves, 128), 128>>>(LeafSoA4{c0, c1, c2, c3}, hashes, n_leaves);
+    VX_LAUNCH_CHECK();
+}
+
+void cuda_merkle_hash_nodes(const uint32_t *children, uint32_t *parents, uint32_t n_parents) {
+    node_hash_kernel<<<blocks_for(n_parents, 128), 128>>>(children, parents, n_parents);
+    VX_LAUNCH_CHECK();
+}
+
+void cuda_merkle_reduce_to_root(const uint32_t *nodes, uint32_t *root, uint32_t n) {
+    if (n == 0 || n > 1024) { set_last_error(VX_ERR_ARG, "cuda_merkle_reduce_to_root: n_nodes must be in [1, 1024]"); return; }
+    uint32_t thr = n / 2 < 32 ? 32 : n / 2;
+    reduce_to_root_kernel<<<1, thr, 32 * n>>>(nodes, root, n);
+    VX_LAUNCH_CHECK();
+}
+
+void cuda_merkle_commit_small_soa4(const uint32_t *c0, const uint32_t *c1, const uint32_t *c2, const uint32_t *c3,
+                                   uint32_t *root, uint32_t n_leaves) {
+    if (n_leaves < 2 || n_leaves > 2048) { set_last_error(VX_ERR_ARG, "cuda_merkle_commit_small_soa4: n_leaves must be in [2, 2048]"); return; }
+    uint32_t thr = n_leaves / 2 < 32 ? 32 : n_leaves / 2;
+    small_tree_kernel<<<1, thr, 16 * n_leaves>>>(LeafSoA4{c0, c1, c2, c3}, root, n_leaves);
+    VX_LAUNCH_CHECK();
+}
+
+void cuda_merkle_hash_leaves_merge_soa4(const uint32_t *c0, const uint32_t *c1, const uint32_t *c2,
+                                        const uint32_t *c3, uint32_t *parents, uint32_t n_leaves) {
+    uint64_t pairs = n_leaves / 2;
+    leaf_merge_kernel<<<blocks_for(pairs, 128), 128>>>(LeafSoA4{c0, c1, c2, c3}, parents, pairs);
+    VX_LAUNCH_CHECK();
+}
+
+void cuda_merkle_tiled_soa4_stream(const uint32_t *c0, const uint32_t *c1, const uint32_t *c2, const uint32_t *c3,
+                                   uint32_t *roots, uint32_t n_leaves, void *stream) {
+    uint32_t tiles = n_leaves / 1024u;
+    if (!tiles) return;
+    tile_root_kernel<<<tiles, 64, 64 * 32, (cudaStream_t)stream>>>(LeafSoA4{c0, c1, c2, c3}, roots, 10u);
+    VX_LAUNCH_CHECK();
+}
+
+void cuda_merkle_tiled_soa4(const uint32_t *c0, const uint32_t *c1, const uint32_t *c2, const uint32_t *c3,
+                            uint32_t *roots, uint32_t n_leaves) {
+    cuda_merkle_tiled_soa4_stream(c0, c1, c2, c3, roots, n_leaves, nullptr);
+}
+
+void cuda_merkle_tiled_generic(const uint32_t *const *cols, uint32_t *roots, uint32_t n_cols, uint32_t n_leaves) {
+    uint32_t tiles = n_leaves / 1024u;
+    if (!tiles) return;
+    tile_root_kernel<<<tiles, 64, 64 * 32>>>(LeafCols{cols, n_cols}, roots, 10u);
+    VX_LAUNCH_CHECK();
+}
+
+void cuda_build_leaves_lifted(const uint32_t *const *cols, const void *schedule, uint32_t n_chunks, uint32_t S,
+                              uint32_t *out, uint32_t n_leaves) {
+    lifted_leaves_kernel<<<blocks_for(n_leaves, 128), 128>>>(cols, (const LiftChunk *)schedule, n_chunks, S, out,
+                                                             n_leaves);
+    VX_LAUNCH_CHECK();
+}
+
+// ---------------- FRI ----------------
+void cuda_fold_line_soa(const uint32_t *i0, const uint32_t *i1, const uint32_t *i2, const uint32_t *i3,
+                        const uint32_t *tw, uint32_t *o0, uint32_t *o1, uint32_t *o2, uint32_t *o3,
+                        const uint32_t *alpha, uint32_t half_n) {
+    qm31 al{{alpha[0], alpha[1], alpha[2], alpha[3]}};
+    fold_line_kernel<<<blocks_for(half_n, 256), 256>>>(i0, i1, i2, i3, tw, o0, o1, o2, o3, al, half_n);
+    VX_LAUNCH_CHECK();
+}
+
+void cuda_fold_circle_into_line_soa(uint32_t *d0, uint32_t *d1, uint32_t *d2, uint32_t *d3, const uint32_t *s0,
+                                    const uint32_t *s1, const uint32_t *s2, const uint32_t *s3, const uint32_t *tw,
+                                    const uint32_t *alpha, const uint32_t *alpha_sq, uint32_t half_n) {
+    qm31 al{{alpha[0], alpha[1], alpha[2], alpha[3]}}, al2{{alpha_sq[0], alpha_sq[1], alpha_sq[2], alpha_sq[3]}};
+    fold_circle_kernel<<<blocks_for(half_n, 256), 256>>>(d0, d1, d2, d3, s0, s1, s2, s3, tw, al, al2, half_n);
+    VX_LAUNCH_CHECK();
+}
+
+void cuda_fold_line_soa_forge(const uint32_t *i0, const uint32_t *i1, const uint32_t *i2, const uint32_t *i3,
+                              const uint32_t *tw, uint32_t *o0, uint32_t *o1, uint32_t *o2, uint32_t *o3,
+                              const uint32_t *alpha, uint32_t half_n) {
+    cuda_fold_line_soa(i0, i1, i2, i3, tw, o0, o1, o2, o3, alpha, half_n);
+}
+
+void cuda_fold_circle_into_line_soa_forge(uint32_t *d0, uint32_t *d1, uint32_t *d2, uint32_t *d3, const uint32_t *s0,
+                                          const uint32_t *s1, const uint32_t *s2, const uint32_t *s3,
+                                          const uint32_t *tw, const uint32_t *alpha, const uint32_t *alpha_sq,
+                                          uint32_t half_n) {
+    cuda_fold_circle_into_line_soa(d0, d1, d2, d3, s0, s1, s2, s3, tw, alpha, alpha_sq, half_n);
+}
+
+void cuda_device_sync(void) { cudaDeviceSynchronize(); }
+
+}  // extern "C"

@@ -1,0 +1,46 @@
+// Circle NTT in the reference's natural-order layout, as multi-layer passes.
+//
+// Layer L (stride 2^L) pairs i0 and i0 + 2^L and uses the twiddle indexed by
+// h = i0 >> (L + 1): line table l = L - 1 for L >= 1, the circle table for
+// L = 0 (circle_ntt.cu:89-117).  Forward runs L = k-1 .. 0 with
+// v0' = v0 + v1 t, v1' = v0 - v1 t; inverse runs L = 0 .. k-1 with
+// v0' = v0 + v1, v1' = (v0 - v1) t, then scales by 2^-k (circle_ntt.cu:248-312).
+//
+// A pass applies the layers of one bit range [s, s + r) to tiles of
+// 2^r rows x 2^w columns held in shared memory; every element of a tile has
+// the same bits outside [s, s + r) except the w low column bits, so each
+// global row segment is 2^w contiguous words (w = min(s, 3) keeps segments at
+// one 32-byte sector).  A transform of 2^k points runs in ceil(k / 11) passes.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace vx {
+
+struct NttTables {
+    const uint32_t *line;     // flat line twiddles, layer l at line + off[l]
+    const uint32_t *circle;   // circle twiddles (n/2)
+    uint32_t off[32];
+};
+
+// Enqueue a full forward (evaluate) or inverse (interpolate, with 1/n scale)
+// transform of `n_cols` columns of 2^log_n points.  Columns are either
+// `dev_cols[c]` (device array of pointers) or `data + c * col_stride`.
+// For the LDE, `src` (coefficients, 2^src_log words) replaces the first pass's
+// input: element g reads src[g & (2^src_log - 1)], and the top
+// (log_n - src_log) layers, which only replicate zero-padded coefficients,
+// are skipped.  src == nullptr means in place.
+cudaError_t ntt_transform(uint32_t *data, uint32_t *const *dev_cols, uint64_t col_stride, uint32_t n_cols,
+                          uint32_t log_n, const NttTables &tw, bool forward, const uint32_t *src,
+                          uint32_t src_log, cudaStream_t stream);
+
+// One butterfly layer over the whole array (reference cuda_circle_ntt_layer).
+cudaError_t ntt_single_layer(uint32_t *data, const uint32_t *tw, uint32_t layer_idx, uint32_t log_n, bool forward,
+                             cudaStream_t stream);
+
+// Reference table layout for a coset of 2^log_n points: line twiddles
+// (2^log_n - 1 words) and circle twiddles (2^(log_n-1) words); offsets of
+// line layer l are  sum_{j<l} 2^(log_n-1-j).
+void ntt_table_offsets(uint32_t log_n, uint32_t off[32]);
+
+}  // namespace vx

@@ -1,0 +1,664 @@
+// Device-resident Fibonacci prover (prover.rs:264-619 restated for B200).
+//
+// One proof is a fixed sequence of kernels on one stream with no host
+// synchronisation: trace generation, iNTT, LDE, trace commitment, quotient
+// commitment (quotient recomputed from the LDE inside the hashing kernel),
+// circle fold fused with the first FRI commitment, line folds fused with their
+// commitments, the Fiat-Shamir transcript on the device, query sampling and
+// decommitment written straight into the proof's byte layout.
+#include <cstdarg>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "vx_common.cuh"
+#include "vx_field.cuh"
+#include "vx_merkle.cuh"
+#include "vx_ntt.cuh"
+#include "vx_prover.cuh"
+#include "vx_twiddles.cuh"
+
+namespace vx {
+
+// ---------------------------------------------------------------------
+// proof layout (stark_cli.rs:1092-1123)
+// ---------------------------------------------------------------------
+static void decom_layout(DecomLayout *d, uint64_t *w, uint32_t nq, uint32_t width, uint32_t depth) {
+    d->width = width; d->depth = depth;
+    d->n = (*w)++;
+    d->vals = *w; *w += (uint64_t)nq * width;
+    d->svals = *w; *w += (uint64_t)nq * width;
+    d->paths = *w; *w += (uint64_t)nq * (1 + 8ull * depth);
+    d->spaths = *w; *w += (uint64_t)nq * (1 + 8ull * depth);
+}
+
+void proof_layout(uint32_t log_n, uint32_t blowup, uint32_t nq, ProofLayout *L) {
+    memset(L, 0, sizeof(*L));
+    L->log_n = log_n; L->blowup = blowup; L->le = log_n + blowup; L->nfri = L->le - 3; L->nq = nq;
+    uint64_t w = 0;
+    L->magic = w; w += 5;                 // magic, version, log_n, a, b
+    L->troot = w; w += 8;
+    L->qroot = w; w += 8;
+    L->nfri_w = w++;
+    L->froots = w; w += 8ull * L->nfri;
+    L->nlast = w++;
+    L->last = w; w += 32;
+    L->nq_w = w++;
+    L->qidx = w; w += nq;
+    decom_layout(&L->trace, &w, nq, 1, L->le);
+    decom_layout(&L->quot, &w, nq, 4, L->le);
+    L->nfd = w++;
+    for (uint32_t k = 0; k < L->nfri; k++) decom_layout(&L->fri[k], &w, nq, 4, L->le - 1 - k);
+    L->words = w;
+}
+
+// Constant words of the layout (everything except a, b, roots, last layer,
+// query indices, values and path hashes).
+static void proof_template(const ProofLayout &L, std::vector<uint32_t> &t) {
+    t.assign(L.words, 0u);
+    t[L.magic] = 0x4B52414Bu; t[L.magic + 1] = 1u; t[L.magic + 2] = L.log_n;
+    t[L.nfri_w] = L.nfri;
+    t[L.nlast] = 8u;
+    t[L.nq_w] = L.nq;
+    auto dec = [&](const DecomLayout &d) {
+        t[d.n] = L.nq;
+        for (uint32_t q = 0; q < L.nq; q++) {
+            t[d.paths + (uint64_t)q * (1 + 8ull * d.depth)] = d.depth;
+            t[d.spaths + (uint64_t)q * (1 + 8ull * d.depth)] = d.depth;
+        }
+    };
+    dec(L.trace); dec(L.quot);
+    t[L.nfd] = L.nfri;
+    for (uint32_t k = 0; k < L.nfri; k++) dec(L.fri[k]);
+}
+
+// ---------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------
+namespace {
+
+// (F(k), F(k+1)) of the sequence F(0)=a, F(1)=b by 2x2 matrix power (air.rs:85-131).
+__device__ void fib_at(uint32_t a, uint32_t b, uint64_t k, uint32_t &fk, uint32_t &fk1) {
+    uint32_t m00 = 1, m01 = 0, m10 = 0, m11 = 1, b00 = 1, b01 = 1, b10 = 1, b11 = 0;
+    while (k) {
+        if (k & 1) {
+            uint32_t t00 = madd(mmul(m00, b00), mmul(m01, b10)), t01 = madd(mmul(m00, b01), mmul(m01, b11));
+            uint32_t t10 = madd(mmul(m10, b00), mmul(m11, b10)), t11 = madd(mmul(m10, b01), mmul(m11, b11));
+            m00 = t00; m01 = t01; m10 = t10; m11 = t11;
+        }
+        uint32_t t00 = madd(mmul(b00, b00), mmul(b01, b10)), t01 = madd(mmul(b00, b01), mmul(b01, b11));
+        uint32_t t10 = madd(mmul(b10, b00), mmul(b11, b10)), t11 = madd(mmul(b10, b01), mmul(b11, b11));
+        b00 = t00; b01 = t01; b10 = t10; b11 = t11;
+        k >>= 1;
+    }
+    fk = madd(mmul(m10, b), mmul(m11, a));
+    fk1 = madd(mmul(m00, b), mmul(m01, a));
+}
+
+// Fibonacci trace t0 = a, t1 = b, t_{i+2} = t_i + t_{i+1} (air.rs:16-25),
+// chunks of 32 rows per thread seeded by fib_at.  Also stamps (a, b) into
+// the proof header.
+__global__ void fib_trace_kernel(uint32_t a, uint32_t b, uint32_t *out, uint64_t n, uint32_t *proof_ab) {
+    uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t C = 32;
+    uint64_t s = t * C;
+    if (t == 0) { proof_ab[0] = a; proof_ab[1] = b; }
+    if (s >= n) return;
+    uint32_t f0, f1;
+    fib_at(a, b, s, f0, f1);
+    uint32_t cnt = (uint32_t)((n - s) < C ? (n - s) : C);
+    out[s] = f0;
+    if (cnt > 1) out[s + 1] = f1;
+    for (uint32_t i = 2; i < cnt; i++) {
+        uint32_t f2 = madd(f0, f1);
+        out[s + i] = f2;
+        f0 = f1; f1 = f2;
+    }
+}
+
+// ---- device transcript: channel.rs:31-119 ----
+__device__ void chan_squeeze(const uint32_t state[8], uint32_t n_draws, uint32_t out[8]) {
+    uint32_t m[16];
+#pragma unroll
+    for (int i = 0; i < 8; i++) m[i] = state[i];
+    m[8] = n_draws;
+#pragma unroll
+    for (int i = 9; i < 16; i++) m[i] = 0u;  // byte 36 is the 0x00 domain byte
+    blake2s_block(out, m, 37u);
+}
+
+// draw_felt (channel.rs:65-84): squeeze until all 8 words < 2P, take words
+// 0..3 mod P.  Bounded: after 64 rejections (probability ~2^-1700) the
+// status word is set and zeros are returned.
+__device__ void chan_draw_felt(DevChannel *ch, uint32_t out[4]) {
+    for (int it = 0; it < 64; it++) {
+        uint32_t w[8];
+        chan_squeeze(ch->state, ch->n_draws, w);
+        ch->n_draws++;
+        bool ok = true;
+#pragma unroll
+        for (int i = 0; i < 8; i++) ok &= w[i] < 2u * VX_P;
+        if (ok) {
+#pragma unroll
+            for (int i = 0; i < 4; i++) out[i] = w[i] % VX_P;
+            return;
+        }
+    }
+    ch->err = 1u;
+    out[0] = out[1] = out[2] = out[3] = 0u;
+}
+
+// mix_digest(root) (channel.rs:31-40), copy the root into the proof, then
+// optionally draw the next challenge.
+__global__ void chan_commit_kernel(DevChannel *ch, const uint32_t *root, uint32_t *proof_root, uint32_t *alpha_out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    uint32_t m[16];
+#pragma unroll
+    for (int i = 0; i < 8; i++) { m[i] = ch->state[i]; m[8 + i] = root[i]; proof_root[i] = root[i]; }
+    uint32_t h[8];
+    blake2s_block(h, m, 64u);
+#pragma unroll
+    for (int i = 0; i < 8; i++) ch->state[i] = h[i];
+    ch->n_draws = 0;
+    if (alpha_out) chan_draw_felt(ch, alpha_out);
+}
+
+// mix_felts(last layer) (channel.rs:46-59) then n_queries x draw_number(N)
+// (channel.rs:93-97, prover.rs:1056-1059).  Draw j squeezes with
+// n_draws = j, so the draws run in parallel.
+__global__ void chan_queries_kernel(DevChannel *ch, const uint32_t *l0, const uint32_t *l1, const uint32_t *l2,
+                                    const uint32_t *l3, uint32_t *proof_last, uint64_t bound, uint32_t nq,
+                                    uint32_t *qidx, uint32_t *proof_qidx) {
+    __shared__ uint32_t st[8];
+    if (threadIdx.x == 0) {
+        uint32_t buf[40];
+        for (int i = 0; i < 8; i++) buf[i] = ch->state[i];
+        for (int i = 0; i < 8; i++) {
+            buf[8 + 4 * i] = l0[i]; buf[9 + 4 * i] = l1[i]; buf[10 + 4 * i] = l2[i]; buf[11 + 4 * i] = l3[i];
+        }
+        for (int i = 0; i < 32; i++) proof_last[i] = buf[8 + i];
+        uint32_t h[8];
+        blake2s_words(h, buf, 160u);
+        for (int i = 0; i < 8; i++) { ch->state[i] = h[i]; st[i] = h[i]; }
+        ch->n_draws = nq;
+    }
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < nq; j += blockDim.x) {
+        uint32_t w[8];
+        chan_squeeze(st, j, w);
+        uint64_t raw = (uint64_t)w[0] | ((uint64_t)w[1] << 32);
+        uint32_t v = (uint32_t)(raw % bound);
+        qidx[j] = v;
+        proof_qidx[j] = v;
+    }
+}
+
+// ---- fused fold + commitment leaf sources (fri.cu:58-126) ----
+// Circle fold of the quotient into FRI layer 0: output j pairs q[2j], q[2j+1].
+struct LeafCircleFold {
+    LeafQuotient q;
+    const uint32_t *tw;
+    const uint32_t *alpha_ptr;
+    uint32_t *o0, *o1, *o2, *o3;
+    qm31 al;
+    __device__ __forceinline__ void init() {
+        q.init();
+        al = {{alpha_ptr[0], alpha_ptr[1], alpha_ptr[2], alpha_ptr[3]}};
+    }
+    __device__ __forceinline__ uint32_t load(uint64_t j, uint32_t m[16]) const {
+        qm31 f0 = q.value(2 * j), f1 = q.value(2 * j + 1);
+        qm31 r = qadd(qadd(f0, f1), qmul(al, qmulm(qsub(f0, f1), __ldg(tw + j))));
+        o0[j] = r.v[0]; o1[j] = r.v[1]; o2[j] = r.v[2]; o3[j] = r.v[3];
+        m[0] = r.v[0]; m[1] = r.v[1]; m[2] = r.v[2]; m[3] = r.v[3];
+        return 16u;
+    }
+};
+// Line fold of FRI layer k-1 into layer k.
+struct LeafLineFold {
+    const uint32_t *i0, *i1, *i2, *i3;
+    const uint32_t *tw;
+    const uint32_t *alpha_ptr;
+    uint32_t *o0, *o1, *o2, *o3;
+    qm31 al;
+    __device__ __forceinline__ void init() { al = {{alpha_ptr[0], alpha_ptr[1], alpha_ptr[2], alpha_ptr[3]}}; }
+    __device__ __forceinline__ uint32_t load(uint64_t j, uint32_t m[16]) const {
+        uint2 a0 = __ldg((const uint2 *)i0 + j), a1 = __ldg((const uint2 *)i1 + j);
+        uint2 a2 = __ldg((const uint2 *)i2 + j), a3 = __ldg((const uint2 *)i3 + j);
+        qm31 f0{{a0.x, a1.x, a2.x, a3.x}}, f1{{a0.y, a1.y, a2.y, a3.y}};
+        qm31 r = qadd(qadd(f0, f1), qmul(al, qmulm(qsub(f0, f1), __ldg(tw + j))));
+        o0[j] = r.v[0]; o1[j] = r.v[1]; o2[j] = r.v[2]; o3[j] = r.v[3];
+        m[0] = r.v[0]; m[1] = r.v[1]; m[2] = r.v[2]; m[3] = r.v[3];
+        return 16u;
+    }
+};
+
+// Query values and sibling values of every committed column, written
+// into the proof.  Thread (tree, q): tree 0 = trace, 1 = quotient, 2 + k
+// = FRI layer k.
+struct ValuesArgs {
+    const uint32_t *eval;
+    uint64_t mask;
+    const uint32_t *alpha_q;
+    const uint32_t *fri[32][4];
+    uint64_t vals[34], svals[34];
+    uint32_t nfri;
+};
+__global__ void decommit_values_kernel(ValuesArgs a, const uint32_t *qidx, uint32_t nq, uint32_t *proof) {
+    uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t ntree = 2 + a.nfri;
+    if (tid >= ntree * nq) return;
+    uint32_t tree = tid / nq, q = tid % nq;
+    uint64_t i = qidx[q];
+    if (tree == 0) {
+        proof[a.vals[0] + q] = a.eval[i];
+        proof[a.svals[0] + q] = a.eval[i ^ 1];
+    } else if (tree == 1) {
+        LeafQuotient src{a.eval, a.mask, a.alpha_q, {0, 0, 0, 0}};
+        src.init();
+        qm31 v = src.value(i), s = src.value(i ^ 1);
+        for (int c = 0; c < 4; c++) { proof[a.vals[1] + 4 * q + c] = v.v[c]; proof[a.svals[1] + 4 * q + c] = s.v[c]; }
+    } else {
+        uint32_t k = tree - 2;
+        uint64_t j = i >> (k + 1);
+        for (int c = 0; c < 4; c++) {
+            proof[a.vals[tree] + 4 * q + c] = a.fri[k][c][j];
+            proof[a.svals[tree] + 4 * q + c] = a.fri[k][c][j ^ 1];
+        }
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------
+// tables and slots
+// ---------------------------------------------------------------------
+static uint64_t align_words(uint64_t w) { return (w + 63) & ~63ull; }  // 256-byte alignment
+
+static int tables_create(int device, uint32_t log_n, uint32_t blowup, SizeTables **out) {
+    auto *t = new SizeTables();
+    memset(t, 0, sizeof(*t));
+    t->device = device; t->log_n = log_n; t->blowup = blowup; t->le = log_n + blowup;
+    uint64_t n = 1ull << log_n, N = 1ull << t->le;
+    uint64_t w = 0;
+    uint64_t o_itl = w; w += align_words(n - 1);
+    uint64_t o_itc = w; w += align_words(n / 2);
+    uint64_t o_ftl = w; w += align_words(N - 1);
+    uint64_t o_ftc = w; w += align_words(N / 2);
+    uint64_t o_fc = w; w += align_words(N / 2);
+    uint64_t o_fl = w;
+    for (uint32_t l = t->le - 1; l >= 4; l--) { t->fold_line_off[l] = w - o_fl; w += align_words(1ull << (l - 1)); }
+    void *blk = nullptr;
+    if (cudaMalloc(&blk, w * 4) != cudaSuccess) {
+        cudaGetLastError();
+        delete t;
+        set_last_error(VX_ERR_OOM, "cudaMalloc of %llu bytes for twiddle tables failed", (unsigned long long)(w * 4));
+        return VX_ERR_OOM;
+    }
+    uint32_t *b = (uint32_t *)blk;
+    t->block = blk;
+    t->itw_line = b + o_itl; t->itw_circle = b + o_itc;
+    t->ftw_line = b + o_ftl; t->ftw_circle = b + o_ftc;
+    t->fold_circle = b + o_fc; t->fold_line = b + o_fl;
+    ntt_table_offsets(log_n, t->itw_off);
+    ntt_table_offsets(t->le, t->ftw_off);
+    cudaStream_t s = nullptr;
+    cudaError_t e = build_ntt_tables(ecoset_half_coset(log_n), true, t->itw_line, t->itw_circle, s);
+    if (e == cudaSuccess) e = build_ntt_tables(ecoset_eval_domain(t->le), false, t->ftw_line, t->ftw_circle, s);
+    if (e == cudaSuccess) e = build_fold_twiddles(ecoset_eval_domain(t->le), true, t->fold_circle, s);
+    for (uint32_t l = t->le - 1; l >= 4 && e == cudaSuccess; l--)
+        e = build_fold_twiddles(ecoset_half_odds(l), false, t->fold_line + t->fold_line_off[l], s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        cudaFree(blk);
+        delete t;
+        set_last_error(VX_ERR_CUDA, "building twiddle tables: %s", cudaGetErrorString(e));
+        return VX_ERR_CUDA;
+    }
+    *out = t;
+    return VX_OK;
+}
+
+static void tables_destroy(SizeTables *t) {
+    if (!t) return;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(t->device);
+    cudaFree(t->block);
+    cudaSetDevice(cur);
+    delete t;
+}
+
+static size_t tables_bytes(const SizeTables *t) {
+    uint64_t n = 1ull << t->log_n, N = 1ull << t->le;
+    return (size_t)(4 * ((n - 1) + n / 2 + (N - 1) + N / 2 + N / 2 + N / 2));
+}
+
+// Per-(device, log_n, blowup) shared tables.
+static std::mutex g_tab_mu;
+static std::map<std::tuple<int, uint32_t, uint32_t>, std::pair<SizeTables *, int>> g_tables;
+
+static int tables_acquire(uint32_t log_n, uint32_t blowup, SizeTables **out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) { set_last_error(VX_ERR_CUDA, "cudaGetDevice failed"); return VX_ERR_CUDA; }
+    std::lock_guard<std::mutex> lk(g_tab_mu);
+    auto key = std::make_tuple(dev, log_n, blowup);
+    auto it = g_tables.find(key);
+    if (it != g_tables.end()) { it->second.second++; *out = it->second.first; return VX_OK; }
+    SizeTables *t = nullptr;
+    int rc = tables_create(dev, log_n, blowup, &t);
+    if (rc) return rc;
+    g_tables[key] = {t, 1};
+    *out = t;
+    return VX_OK;
+}
+
+static void tables_release(SizeTables *t) {
+    std::lock_guard<std::mutex> lk(g_tab_mu);
+    for (auto it = g_tables.begin(); it != g_tables.end(); ++it) {
+        if (it->second.first == t) {
+            if (--it->second.second == 0) { tables_destroy(t); g_tables.erase(it); }
+            return;
+        }
+    }
+}
+
+}  // namespace vx
+
+struct vx_prover {
+    vx::ProofSlot s;
+    int device;
+    uint32_t launches;  // kernels enqueued by the last vx_prover_prove_async
+};
+
+using namespace vx;
+
+extern "C" size_t vx_proof_size(uint32_t log_n, uint32_t blowup_bits, uint32_t n_queries) {
+    if (log_n < 4 || blowup_bits < 1 || log_n + blowup_bits > 31) return 0;
+    ProofLayout L;
+    proof_layout(log_n, blowup_bits, n_queries, &L);
+    return (size_t)(L.words * 4);
+}
+
+extern "C" int vx_prover_create(uint32_t log_n, uint32_t blowup_bits, uint32_t n_queries, vx_prover **out) {
+    VX_CHECK_ARG(out != nullptr, "vx_prover_create: out is null");
+    VX_CHECK_ARG(log_n >= 4 && blowup_bits >= 1 && log_n + blowup_bits <= 31,
+                 "vx_prover_create: need log_n >= 4, blowup_bits >= 1, log_n + blowup_bits <= 31 (got %u, %u)",
+                 log_n, blowup_bits);
+    VX_CHECK_ARG(n_queries >= 1 && n_queries <= 4096, "vx_prover_create: n_queries must be in [1, 4096]");
+    auto *p = new vx_prover();
+    memset(&p->s, 0, sizeof(p->s));
+    cudaGetDevice(&p->device);
+    ProofSlot &S = p->s;
+    int rc = tables_acquire(log_n, blowup_bits, &S.tw);
+    if (rc) { delete p; return rc; }
+    proof_layout(log_n, blowup_bits, n_queries, &S.L);
+    const ProofLayout &L = S.L;
+    uint32_t le = L.le;
+    uint64_t n = 1ull << log_n, N = 1ull << le;
+    // carve one allocation
+    uint64_t w = 0;
+    uint64_t o_coeffs = w; w += align_words(n);
+    uint64_t o_eval = w; w += align_words(N);
+    uint64_t o_fri[32];
+    for (uint32_t k = 0; k < L.nfri; k++) { o_fri[k] = w; w += 4 * align_words(1ull << (le - 1 - k)); }
+    uint64_t o_tt = w; w += align_words(tree_pool_words(le));
+    uint64_t o_qt = w; w += align_words(tree_pool_words(le));
+    uint64_t o_ft[32];
+    for (uint32_t k = 0; k < L.nfri; k++) { o_ft[k] = w; w += align_words(tree_pool_words(le - 1 - k)); }
+    uint64_t o_chan = w; w += align_words(sizeof(DevChannel) / 4 + 1);
+    uint64_t o_aq = w; w += align_words(4);
+    uint64_t o_af = w; w += align_words(4ull * (L.nfri + 1));
+    uint64_t o_qi = w; w += align_words(n_queries);
+    uint64_t o_proof = w; w += align_words(L.words);
+    void *blk = nullptr;
+    if (cudaMalloc(&blk, w * 4) != cudaSuccess) {
+        cudaGetLastError();
+        tables_release(S.tw);
+        delete p;
+        set_last_error(VX_ERR_OOM, "cudaMalloc of %llu bytes for a proof slot failed", (unsigned long long)(w * 4));
+        return VX_ERR_OOM;
+    }
+    uint32_t *b = (uint32_t *)blk;
+    S.block = blk;
+    S.block_bytes = w * 4;
+    S.coeffs = b + o_coeffs;
+    S.eval = b + o_eval;
+    for (uint32_t k = 0; k < L.nfri; k++) {
+        uint64_t sz = align_words(1ull << (le - 1 - k));
+        for (int c = 0; c < 4; c++) S.fri[k][c] = b + o_fri[k] + c * sz;
+    }
+    tree_plan(le, b + o_tt, &S.trace_lv);
+    tree_plan(le, b + o_qt, &S.quot_lv);
+    for (uint32_t k = 0; k < L.nfri; k++) tree_plan(le - 1 - k, b + o_ft[k], &S.fri_lv[k]);
+    S.chan = (DevChannel *)(b + o_chan);
+    S.alpha_q = b + o_aq;
+    S.alpha_f = b + o_af;
+    S.qidx = b + o_qi;
+    S.proof = b + o_proof;
+    std::vector<uint32_t> tmpl;
+    proof_template(L, tmpl);
+    cudaError_t e = cudaMemcpy(S.proof, tmpl.data(), L.words * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(S.chan, 0, sizeof(DevChannel));
+    if (e != cudaSuccess) {
+        vx_prover_destroy(p);
+        set_last_error(VX_ERR_CUDA, "initialising proof slot: %s", cudaGetErrorString(e));
+        return VX_ERR_CUDA;
+    }
+    *out = p;
+    return VX_OK;
+}
+
+extern "C" void vx_prover_destroy(vx_prover *p) {
+    if (!p) return;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(p->device);
+    if (p->s.block) cudaFree(p->s.block);
+    cudaSetDevice(cur);
+    if (p->s.tw) tables_release(p->s.tw);
+    delete p;
+}
+
+extern "C" size_t vx_prover_slot_bytes(const vx_prover *p) { return p ? p->s.block_bytes : 0; }
+extern "C" size_t vx_prover_table_bytes(const vx_prover *p) { return p && p->s.tw ? tables_bytes(p->s.tw) : 0; }
+
+// Stages of one proof, in order (prover.rs:264-619):
+//   0 trace, 1 interpolate, 2 LDE evaluate, 3 trace commitment,
+//   4 quotient commitment, 5 circle fold + FRI layer 0, 6 line folds,
+//   7 last layer + queries, 8 decommitment.
+static int enqueue_stage(vx_prover *p, uint32_t stage, uint32_t a, uint32_t b, cudaStream_t st, uint32_t *launches) {
+    ProofSlot &S = p->s;
+    const ProofLayout &L = S.L;
+    const SizeTables &T = *S.tw;
+    const uint32_t log_n = L.log_n, le = L.le;
+    const uint64_t n = 1ull << log_n, N = 1ull << le;
+    uint32_t *proof = S.proof;
+    LeafQuotient lq{S.eval, N - 1, S.alpha_q, {0, 0, 0, 0}};
+    auto tree_launches = [](const TreeLevels &lv) { return lv.n - 1; };
+    auto ntt_launches = [](uint32_t layers) { return (layers + 10u) / 11u; };
+    switch (stage) {
+    case 0:
+        VX_CUDA_TRY(cudaMemsetAsync(S.chan, 0, sizeof(DevChannel), st));
+        fib_trace_kernel<<<blocks_for((n + 31) / 32, 256), 256, 0, st>>>(a, b, S.coeffs, n, proof + L.magic + 3);
+        *launches += 1;
+        break;
+    case 1: {
+        NttTables it{T.itw_line, T.itw_circle, {}};
+        memcpy(it.off, T.itw_off, sizeof(it.off));
+        VX_CUDA_TRY(ntt_transform(S.coeffs, nullptr, 0, 1, log_n, it, false, nullptr, 0, st));
+        *launches += ntt_launches(log_n);
+        break;
+    }
+    case 2: {
+        NttTables ft{T.ftw_line, T.ftw_circle, {}};
+        memcpy(ft.off, T.ftw_off, sizeof(ft.off));
+        VX_CUDA_TRY(ntt_transform(S.eval, nullptr, 0, 1, le, ft, true, S.coeffs, log_n, st));
+        *launches += ntt_launches(log_n);
+        break;
+    }
+    case 3:
+        VX_CUDA_TRY(tree_build(LeafM31{S.eval}, S.trace_lv, st));
+        chan_commit_kernel<<<1, 32, 0, st>>>(S.chan, S.trace_lv.hashes[S.trace_lv.n - 1], proof + L.troot, S.alpha_q);
+        *launches += tree_launches(S.trace_lv) + 1;
+        break;
+    case 4:
+        VX_CUDA_TRY(tree_build(lq, S.quot_lv, st));
+        chan_commit_kernel<<<1, 32, 0, st>>>(S.chan, S.quot_lv.hashes[S.quot_lv.n - 1], proof + L.qroot, S.alpha_f);
+        *launches += tree_launches(S.quot_lv) + 1;
+        break;
+    case 5: {
+        LeafCircleFold cf{lq, T.fold_circle, S.alpha_f, S.fri[0][0], S.fri[0][1], S.fri[0][2], S.fri[0][3], {}};
+        VX_CUDA_TRY(tree_build(cf, S.fri_lv[0], st));
+        chan_commit_kernel<<<1, 32, 0, st>>>(S.chan, S.fri_lv[0].hashes[S.fri_lv[0].n - 1], proof + L.froots,
+                                             L.nfri > 1 ? S.alpha_f + 4 : nullptr);
+        *launches += tree_launches(S.fri_lv[0]) + 1;
+        break;
+    }
+    case 6:
+        for (uint32_t k = 1; k < L.nfri; k++) {
+            uint32_t lsrc = le - k;  // log size of the layer being folded
+            LeafLineFold lf{S.fri[k - 1][0], S.fri[k - 1][1], S.fri[k - 1][2], S.fri[k - 1][3],
+                            T.fold_line + T.fold_line_off[lsrc], S.alpha_f + 4 * k,
+                            S.fri[k][0], S.fri[k][1], S.fri[k][2], S.fri[k][3], {}};
+            VX_CUDA_TRY(tree_build(lf, S.fri_lv[k], st));
+            chan_commit_kernel<<<1, 32, 0, st>>>(S.chan, S.fri_lv[k].hashes[S.fri_lv[k].n - 1],
+                                                 proof + L.froots + 8 * k,
+                                                 k + 1 < L.nfri ? S.alpha_f + 4 * (k + 1) : nullptr);
+            *launches += tree_launches(S.fri_lv[k]) + 1;
+        }
+        break;
+    case 7: {
+        uint32_t kl = L.nfri - 1;
+        chan_queries_kernel<<<1, 128, 0, st>>>(S.chan, S.fri[kl][0], S.fri[kl][1], S.fri[kl][2], S.fri[kl][3],
+                                               proof + L.last, N, L.nq, S.qidx, proof + L.qidx);
+        *launches += 1;
+        break;
+    }
+    case 8: {
+        ValuesArgs va;
+        memset(&va, 0, sizeof(va));
+        va.eval = S.eval; va.mask = N - 1; va.alpha_q = S.alpha_q; va.nfri = L.nfri;
+        va.vals[0] = L.trace.vals; va.svals[0] = L.trace.svals;
+        va.vals[1] = L.quot.vals; va.svals[1] = L.quot.svals;
+        for (uint32_t k = 0; k < L.nfri; k++) {
+            for (int c = 0; c < 4; c++) va.fri[k][c] = S.fri[k][c];
+            va.vals[2 + k] = L.fri[k].vals; va.svals[2 + k] = L.fri[k].svals;
+        }
+        decommit_values_kernel<<<blocks_for((uint64_t)(2 + L.nfri) * L.nq, 128), 128, 0, st>>>(va, S.qidx, L.nq, proof);
+        *launches += 1;
+        auto paths = [&](auto src, const TreeLevels &lv, uint32_t shift, const DecomLayout &d) {
+            uint32_t nt = L.nq * (lv.n - 1);
+            decommit_paths_kernel<<<blocks_for(nt, 64), 64, 0, st>>>(src, lv, S.qidx, shift, L.nq, proof + d.paths,
+                                                                     proof + d.spaths);
+            *launches += 1;
+        };
+        paths(LeafM31{S.eval}, S.trace_lv, 0, L.trace);
+        paths(lq, S.quot_lv, 0, L.quot);
+        for (uint32_t k = 0; k < L.nfri; k++)
+            paths(LeafSoA4{S.fri[k][0], S.fri[k][1], S.fri[k][2], S.fri[k][3]}, S.fri_lv[k], k + 1, L.fri[k]);
+        break;
+    }
+    default:
+        set_last_error(VX_ERR_ARG, "unknown proof stage %u", stage);
+        return VX_ERR_ARG;
+    }
+    VX_CUDA_TRY(cudaGetLastError());
+    return VX_OK;
+}
+
+extern "C" int vx_prover_stage_async(vx_prover *p, uint32_t stage, uint32_t a, uint32_t b, void *stream_v) {
+    VX_CHECK_ARG(p != nullptr, "vx_prover_stage_async: null prover");
+    VX_CHECK_ARG(a < VX_P && b < VX_P, "vx_prover_stage_async: public inputs must be canonical M31 (< 2^31-1)");
+    uint32_t launches = 0;
+    return enqueue_stage(p, stage, a, b, (cudaStream_t)stream_v, &launches);
+}
+
+extern "C" int vx_prover_prove_async(vx_prover *p, uint32_t a, uint32_t b, void *stream_v) {
+    VX_CHECK_ARG(p != nullptr, "vx_prover_prove_async: null prover");
+    VX_CHECK_ARG(a < VX_P && b < VX_P, "vx_prover_prove_async: public inputs must be canonical M31 (< 2^31-1)");
+    uint32_t launches = 0;
+    for (uint32_t stage = 0; stage < VX_N_STAGES; stage++) {
+        int rc = enqueue_stage(p, stage, a, b, (cudaStream_t)stream_v, &launches);
+        if (rc) return rc;
+    }
+    p->launches = launches;
+    return VX_OK;
+}
+
+extern "C" uint32_t vx_prover_launches(const vx_prover *p) { return p ? p->launches : 0u; }
+
+extern "C" int vx_prover_fetch_async(vx_prover *p, void *dst, void *stream_v) {
+    VX_CHECK_ARG(p != nullptr && dst != nullptr, "vx_prover_fetch_async: null argument");
+    VX_CUDA_TRY(cudaMemcpyAsync(dst, p->s.proof, p->s.L.words * 4, cudaMemcpyDeviceToHost, (cudaStream_t)stream_v));
+    return VX_OK;
+}
+
+extern "C" int vx_prover_proof_device(vx_prover *p, const void **dptr, size_t *bytes) {
+    VX_CHECK_ARG(p != nullptr && dptr != nullptr && bytes != nullptr, "vx_prover_proof_device: null argument");
+    *dptr = p->s.proof;
+    *bytes = (size_t)(p->s.L.words * 4);
+    return VX_OK;
+}
+
+extern "C" int vx_prover_check(vx_prover *p) {
+    VX_CHECK_ARG(p != nullptr, "vx_prover_check: null prover");
+    uint32_t err = 0;
+    VX_CUDA_TRY(cudaMemcpy(&err, &p->s.chan->err, 4, cudaMemcpyDeviceToHost));
+    if (err) {
+        set_last_error(VX_ERR_DEVICE, "transcript rejection sampling exceeded its bound");
+        return VX_ERR_DEVICE;
+    }
+    return VX_OK;
+}
+
+// ---- synchronous convenience with a per-size slot cache ----
+namespace {
+std::mutex g_slot_mu;
+std::map<std::tuple<int, uint32_t, uint32_t, uint32_t>, vx_prover *> g_slots;
+}  // namespace
+
+extern "C" int vx_prove_fib(uint32_t a, uint32_t b, uint32_t log_n, uint32_t blowup_bits, uint32_t n_queries,
+                            uint8_t *out, size_t cap, size_t *out_len) {
+    VX_CHECK_ARG(out != nullptr && out_len != nullptr, "vx_prove_fib: null output");
+    size_t need = vx_proof_size(log_n, blowup_bits, n_queries);
+    VX_CHECK_ARG(need != 0, "vx_prove_fib: unsupported size log_n=%u blowup_bits=%u", log_n, blowup_bits);
+    VX_CHECK_ARG(cap >= need, "vx_prove_fib: output capacity %zu < proof size %zu", cap, need);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(g_slot_mu);
+    auto key = std::make_tuple(dev, log_n, blowup_bits, n_queries);
+    vx_prover *p = nullptr;
+    auto it = g_slots.find(key);
+    if (it != g_slots.end()) {
+        p = it->second;
+    } else {
+        int rc = vx_prover_create(log_n, blowup_bits, n_queries, &p);
+        if (rc) return rc;
+        g_slots[key] = p;
+    }
+    int rc = vx_prover_prove_async(p, a, b, nullptr);
+    if (rc) return rc;
+    rc = vx_prover_fetch_async(p, out, nullptr);
+    if (rc) return rc;
+    VX_CUDA_TRY(cudaStreamSynchronize(nullptr));
+    rc = vx_prover_check(p);
+    if (rc) return rc;
+    *out_len = need;
+    return VX_OK;
+}
+
+extern "C" void vx_release_all(void) {
+    {
+        std::lock_guard<std::mutex> lk(g_slot_mu);
+        for (auto &kv : g_slots) vx_prover_destroy(kv.second);
+        g_slots.clear();
+    }
+    std::lock_guard<std::mutex> lk(g_tab_mu);
+    for (auto &kv : g_tables) tables_destroy(kv.second.first);
+    g_tables.clear();
+}

@@ -1,0 +1,131 @@
+// Twiddle table construction (see vx_twiddles.cuh).
+#include <mutex>
+#include <vector>
+
+#include "vx_common.cuh"
+#include "vx_twiddles.cuh"
+
+namespace vx {
+
+namespace {
+
+std::mutex g_gen_mu;
+cpoint *g_gen_dev[64] = {nullptr};
+
+__global__ void line_layer_kernel(GenTables g, uint32_t e0, uint32_t k, uint32_t l, uint32_t *out, uint64_t size) {
+    uint64_t h = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= size) return;
+    uint64_t e = ((uint64_t)e0 + (h << (l + 1u + 31u - k))) << l;
+    out[h] = gpow(g, (uint32_t)(e & 0x7FFFFFFFull)).x;
+}
+
+__global__ void circle_layer_kernel(GenTables g, uint32_t e0, uint32_t k, uint32_t *out, uint64_t size) {
+    uint64_t h = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= size) return;
+    uint64_t e = (uint64_t)e0 + (h << (31u - k));
+    out[h] = gpow(g, (uint32_t)(e & 0x7FFFFFFFull)).y;
+}
+
+__global__ void fold_sources_kernel(GenTables g, uint32_t e0, uint32_t k, int extract_y, uint32_t *out, uint64_t half) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= half) return;
+    uint64_t idx = brev_bits((uint32_t)(i << 1), k);
+    uint64_t e = (uint64_t)e0 + (idx << (31u - k));
+    cpoint p = gpow(g, (uint32_t)(e & 0x7FFFFFFFull));
+    out[i] = extract_y ? p.y : p.x;
+}
+
+// One thread per aligned chunk of 64, mirroring batch_inverse.cu:8-41
+// exactly, including the zero-first-slot behaviour.  Safe in place.
+__global__ void batch_inverse_kernel(const uint32_t *in, uint32_t *out, uint64_t n) {
+    uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t s = c * 64ull;
+    if (s >= n) return;
+    uint32_t cnt = (uint32_t)((n - s) < 64ull ? (n - s) : 64ull);
+    uint32_t pre[64];
+    uint32_t acc = in[s];
+    pre[0] = acc;
+    for (uint32_t i = 1; i < cnt; i++) {
+        uint32_t v = in[s + i];
+        acc = v ? mmul(acc, v) : acc;
+        pre[i] = acc;
+    }
+    uint32_t first = in[s];
+    uint32_t inv = minv(acc);
+    for (uint32_t i = cnt - 1; i > 0; i--) {
+        uint32_t v = in[s + i];
+        if (!v) { out[s + i] = 0u; continue; }
+        out[s + i] = mmul(inv, pre[i - 1]);
+        inv = mmul(inv, v);
+    }
+    out[s] = first ? inv : 0u;
+}
+
+}  // namespace
+
+cudaError_t gen_tables_get(GenTables *out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_gen_mu);
+    if (!g_gen_dev[dev]) {
+        std::vector<hpoint> h((1u << 16) + (1u << 15));
+        hpoint p{1u, 0u};
+        for (uint32_t i = 0; i < (1u << 16); i++) { h[i] = p; p = h_pmul(p, kGen); }
+        hpoint g16 = h_ppow(kGen, 1ull << 16);
+        p = {1u, 0u};
+        for (uint32_t i = 0; i < (1u << 15); i++) { h[(1u << 16) + i] = p; p = h_pmul(p, g16); }
+        cpoint *d = nullptr;
+        e = cudaMalloc(&d, h.size() * sizeof(cpoint));
+        if (e != cudaSuccess) return e;
+        e = cudaMemcpy(d, h.data(), h.size() * sizeof(cpoint), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) { cudaFree(d); return e; }
+        g_gen_dev[dev] = d;
+    }
+    out->lo = g_gen_dev[dev];
+    out->hi = g_gen_dev[dev] + (1u << 16);
+    return cudaSuccess;
+}
+
+cudaError_t batch_inverse(const uint32_t *in, uint32_t *out, uint64_t n, cudaStream_t stream) {
+    if (!n) return cudaSuccess;
+    uint64_t chunks = (n + 63) / 64;
+    batch_inverse_kernel<<<blocks_for(chunks, 128), 128, 0, stream>>>(in, out, n);
+    return cudaGetLastError();
+}
+
+cudaError_t build_ntt_tables(ecoset c, bool inverse, uint32_t *line, uint32_t *circle, cudaStream_t stream) {
+    GenTables g;
+    cudaError_t e = gen_tables_get(&g);
+    if (e != cudaSuccess) return e;
+    uint64_t m = 1ull << c.k;
+    uint64_t off = 0;
+    for (uint32_t l = 0; l + 1 < c.k; l++) {
+        uint64_t size = m >> (l + 1);
+        line_layer_kernel<<<blocks_for(size, 256), 256, 0, stream>>>(g, c.e0, c.k, l, line + off, size);
+        off += size;
+    }
+    if (m / 2) circle_layer_kernel<<<blocks_for(m / 2, 256), 256, 0, stream>>>(g, c.e0, c.k, circle, m / 2);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (inverse) {
+        if (off) { e = batch_inverse(line, line, off, stream); if (e != cudaSuccess) return e; }
+        if (m / 2) { e = batch_inverse(circle, circle, m / 2, stream); if (e != cudaSuccess) return e; }
+    }
+    return cudaSuccess;
+}
+
+cudaError_t build_fold_twiddles(ecoset c, bool extract_y, uint32_t *out, cudaStream_t stream) {
+    GenTables g;
+    cudaError_t e = gen_tables_get(&g);
+    if (e != cudaSuccess) return e;
+    uint64_t half = (1ull << c.k) / 2;
+    if (!half) return cudaSuccess;
+    fold_sources_kernel<<<blocks_for(half, 256), 256, 0, stream>>>(g, c.e0, c.k, extract_y ? 1 : 0, out, half);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return batch_inverse(out, out, half, stream);
+}
+
+}  // namespace vx
