@@ -269,3 +269,46 @@ def qm31_mul(a, b) -> np.ndarray:
     out = np.zeros(4, np.uint32)
     lib().vxo_qm31_mul(_p(a), _p(b), _p(out))
     return out
+
+
+# ---- the reference's own CUDA kernels (oracle/_ref/libvxref.so) ----
+_REF_PATH = os.path.join(_HERE, "_ref", "libvxref.so")
+_ref = None
+
+
+def ref_available() -> bool:
+    return os.path.exists(_REF_PATH)
+
+
+def ref_lib():
+    """libvxref.so: the reference's hot-path .cu files compiled for sm_100a plus
+    ref_driver.cu (built by oracle/build_ref.sh).  Needs a GPU to run."""
+    global _ref
+    if _ref is None:
+        R = C.CDLL(_REF_PATH)
+        R.vxref_prove.argtypes = [C.c_uint32] * 5 + [C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]
+        R.vxref_prove.restype = C.c_int
+        R.vxref_ntt_time.argtypes = [C.c_uint32, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        R.vxref_ntt_time.restype = C.c_int
+        _ref = R
+    return _ref
+
+
+def ref_prove(a: int, b: int, log_n: int, blowup_bits: int = 2, n_queries: int = 80) -> bytes:
+    """Proof produced by the reference's CUDA kernels (prove_lean_inner order)."""
+    size = proof_size(log_n, blowup_bits, n_queries)
+    buf = (C.c_uint8 * size)()
+    n = C.c_size_t()
+    rc = ref_lib().vxref_prove(a, b, log_n, blowup_bits, n_queries, C.addressof(buf), size, C.byref(n))
+    if rc:
+        raise RuntimeError(f"reference-kernel prover failed (rc={rc})")
+    return bytes(buf[: n.value])
+
+
+def ref_ntt_time(log_n: int, reps: int = 5):
+    """(evaluate ms, interpolate ms) of the reference's circle NTT on this GPU."""
+    e, i = C.c_float(), C.c_float()
+    rc = ref_lib().vxref_ntt_time(log_n, reps, C.byref(e), C.byref(i))
+    if rc:
+        raise RuntimeError("reference NTT timing failed")
+    return e.value, i.value
