@@ -296,6 +296,19 @@ def main():
     probe_rate = 148 * 8 * 256 * iters / (pa.elapsed_time(pb) / 1e3)
     merkle_rate = compressions / tcommit_t
 
+    # per-stage device time of one proof (vx_prover_stage_async, stages in order)
+    stage_names = ["trace", "interpolate", "lde_evaluate", "trace_commit", "quotient_commit",
+                   "circle_fold_commit", "line_folds_commit", "queries", "decommit"]
+    st_ev = [[torch.cuda.Event(enable_timing=True) for _ in range(len(stage_names) + 1)] for _ in range(reps)]
+    for r in range(reps):
+        for k in range(len(stage_names)):
+            st_ev[r][k].record(stream)
+            _lib.check(L.vx_prover_stage_async(cache._p, k, a, b, s))
+        st_ev[r][-1].record(stream)
+    stream.synchronize()
+    stages_ms = {name: statistics.median([st_ev[r][k].elapsed_time(st_ev[r][k + 1]) for r in range(reps)])
+                 for k, name in enumerate(stage_names)}
+
     # max over ranks
     if dist is not None:
         t = torch.tensor([dev_ms, t_all], device="cuda")
@@ -327,6 +340,7 @@ def main():
             "roofline_alu": {"bound": "int-alu (Blake2s)", "kernel": "trace commitment (2^26 leaves)",
                              "achieved": merkle_rate, "peak": probe_rate, "unit": "compressions/s",
                              "frac": merkle_rate / probe_rate, "time_ms": tcommit_t * 1e3},
+            "stages_ms": stages_ms,
             "gpu_launches": launches_per_proof * steps,
             "launches_per_proof": launches_per_proof,
             "clocks": clocks,

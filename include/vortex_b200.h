@@ -210,6 +210,36 @@ int vx_prover_check(vx_prover *p);
 int vx_prove_fib(uint32_t a, uint32_t b, uint32_t log_n, uint32_t blowup_bits, uint32_t n_queries, uint8_t *out,
                  size_t cap, size_t *out_len);
 
+/* ---- serving: continuous batching of mixed-size proof requests (new) ----
+ * A dispatcher thread admits queued requests as proof slots of their size
+ * free up or can be created inside the device-memory budget, up to
+ * max_inflight proofs on the GPU at once, each on its own stream as one CUDA
+ * graph (use_graphs != 0) or as plain launches.  A request's proof bytes do
+ * not depend on what else is in flight. */
+typedef struct vx_server vx_server;
+typedef struct {
+    uint64_t tag;         /* as submitted */
+    int32_t status;       /* VX_OK or an error code */
+    uint32_t log_n;
+    uint64_t submit_ns;   /* host steady-clock times */
+    uint64_t start_ns;
+    uint64_t done_ns;
+    uint64_t proof_bytes;
+} vx_completion;
+int vx_server_create(size_t budget_bytes, uint32_t max_inflight, uint32_t blowup_bits, uint32_t n_queries,
+                     int use_graphs, vx_server **out);
+/* Queue one request (non-blocking). */
+int vx_server_submit(vx_server *s, uint64_t tag, uint32_t log_n, uint32_t a, uint32_t b);
+/* Create up to `count` slots of this size ahead of time (counts against the budget). */
+int vx_server_prewarm(vx_server *s, uint32_t log_n, uint32_t count);
+/* Take up to `max` completions, waiting up to wait_ms for the first one. */
+int vx_server_poll(vx_server *s, vx_completion *out, uint32_t max, uint32_t *n_out, int wait_ms);
+/* Copy (out != NULL) and release the proof bytes of a completed request. */
+int vx_server_result(vx_server *s, uint64_t tag, uint8_t *out, size_t cap, size_t *len);
+int vx_server_stats(vx_server *s, uint32_t *n_slots, uint32_t *inflight, uint32_t *pending, size_t *bytes_used);
+/* Waits for in-flight proofs, then frees every slot. */
+void vx_server_destroy(vx_server *s);
+
 /* Blake2s throughput probe: `blocks` x `threads` threads each run `iters`
  * chained compressions on registers only (no memory traffic) and write one
  * word to out[thread].  Gives the achievable compressions/s, the ALU

@@ -34,3 +34,32 @@ def test_reference_kernels_blowup_one(ref):
     want = ref.ref_prove(a, b, 10, 1)
     assert ref.prove(a, b, 10, 1) == want
     assert prover.prove_bytes(a, b, 10, 1) == want
+
+
+@pytest.mark.parametrize("log_n", [20, 24])
+def test_ntt_faster_than_reference_kernels(ref, log_n):
+    """Same transform, same B200: this library's evaluate / interpolate against
+    the reference's (one Forge layer kernel per layer), timed with CUDA events."""
+    import torch
+    from vortexstark_b200 import ntt
+    from vortexstark_b200.circle import Coset
+    from vortexstark_b200.workload import m31_array
+    from gpu_util import to_dev
+
+    ref_e, ref_i = ref.ref_ntt_time(log_n, 5)
+    cache = ntt.TwiddleCache(Coset.half_coset(log_n))
+    d = to_dev(m31_array(log_n, 1 << log_n))
+    ntt.evaluate(d, cache)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev[0].record()
+    for _ in range(5):
+        ntt.evaluate(d, cache)
+    ev[1].record()
+    for _ in range(5):
+        ntt.interpolate(d, cache)
+    ev[2].record()
+    torch.cuda.synchronize()
+    my_e, my_i = ev[0].elapsed_time(ev[1]) / 5, ev[1].elapsed_time(ev[2]) / 5
+    print(f"\nNTT 2^{log_n}: evaluate {my_e:.3f} ms (reference kernels {ref_e:.3f} ms), "
+          f"interpolate {my_i:.3f} ms (reference kernels {ref_i:.3f} ms)")
+    assert my_e < ref_e and my_i < ref_i

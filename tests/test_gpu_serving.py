@@ -1,0 +1,52 @@
+"""Serving engine: continuous batching must not change any proof byte.
+
+Every request's proof, computed while other requests of other sizes are in
+flight on the same GPU, must equal the proof of the same request computed
+alone (and the oracle's).  A tight memory budget forces queueing and slot
+reuse; that must not change any byte either.
+"""
+import pytest
+
+from vortexstark_b200 import prover
+from vortexstark_b200.serving import ProofServer, poisson_arrivals, run_stream
+from vortexstark_b200.workload import SplitMix64
+
+pytestmark = pytest.mark.gpu
+
+
+def _stream(seed, n, sizes):
+    g = SplitMix64(seed)
+    return [(sizes[g.next() % len(sizes)], g.m31(), g.m31()) for _ in range(n)]
+
+
+def test_mixed_stream_equals_alone(oracle):
+    reqs = _stream(7, 40, [8, 10, 12, 14, 16])
+    with ProofServer(budget_bytes=8 << 30, max_inflight=8) as srv:
+        for s in (8, 10, 12, 14, 16):
+            srv.prewarm(s, 2)
+        summary, results = run_stream(srv, reqs, poisson_arrivals(len(reqs), 2000.0, 1), keep_results=True)
+    assert summary["n"] == len(reqs)
+    for i, (log_n, a, b) in enumerate(reqs):
+        alone = prover.prove_bytes(a, b, log_n)
+        assert results[i] == alone, (i, log_n)
+        if log_n <= 12:
+            assert alone == oracle.prove(a, b, log_n)
+
+
+def test_tight_budget_queues_and_stays_exact():
+    reqs = _stream(11, 16, [10, 12])
+    budget = 3 << 20  # room for about two slots of these sizes
+    with ProofServer(budget_bytes=budget, max_inflight=4) as srv:
+        summary, results = run_stream(srv, reqs, [0.0] * len(reqs), keep_results=True)
+        st = srv.stats()
+    assert st["bytes_used"] <= budget and st["slots"] <= 3
+    for i, (log_n, a, b) in enumerate(reqs):
+        assert results[i] == prover.prove_bytes(a, b, log_n)
+
+
+def test_plain_launches_without_graphs():
+    reqs = _stream(13, 8, [10, 11])
+    with ProofServer(budget_bytes=1 << 30, max_inflight=4, use_graphs=False) as srv:
+        summary, results = run_stream(srv, reqs, [0.0] * len(reqs), keep_results=True)
+    for i, (log_n, a, b) in enumerate(reqs):
+        assert results[i] == prover.prove_bytes(a, b, log_n)

@@ -83,6 +83,184 @@ __global__ void ntt_layer_kernel(uint32_t *d, const uint32_t *__restrict__ tw, u
     }
 }
 
+// ---------------------------------------------------------------------
+// Register-radix pass: a tile of 2^(R+WL) elements (2^R rows of 2^WL
+// columns), 16 elements per thread.  The pass's R layers run in stages of up
+// to 4 layers; in a stage each thread holds the 16 elements that differ in
+// one contiguous block of 4 tile bits [A, A+4) covering the stage's layer
+// bits, and does all the stage's butterflies in registers.  Between stages
+// the tile goes through shared memory (padded by one word per 32 to spread
+// the strided accesses over the banks).  The tile's twiddles (2^R - 1 words,
+// one contiguous run of the reference table per layer) are staged in shared
+// memory once per tile.
+// ---------------------------------------------------------------------
+struct Pass2Args {
+    uint32_t *data;
+    uint32_t *const *dev_cols;
+    uint64_t col_stride;
+    const uint32_t *src;
+    uint64_t src_mask, src_stride;
+    const uint32_t *line, *circle;
+    PassOff off;
+    uint32_t s;       // lowest layer of the pass
+    uint32_t scale;   // 1 = none
+};
+
+__device__ __forceinline__ uint32_t pad32(uint32_t e) { return e + (e >> 5); }
+
+template <bool FWD, int R, int WL, int LO, int HI, int A>
+__device__ __forceinline__ void ntt_stage(uint32_t *sm, const uint32_t *smtw, uint32_t tid) {
+    constexpr int TB = R + WL;
+    const uint32_t base = (tid & ((1u << A) - 1u)) | ((tid >> A) << (A + 4));
+    uint32_t v[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) v[i] = sm[pad32(base | ((uint32_t)i << A))];
+#pragma unroll
+    for (int jj = 0; jj < HI - LO; jj++) {
+        const int j = FWD ? (HI - 1 - jj) : (LO + jj);
+        const int rb = j + WL - A;            // register bit of layer j
+        const int S = j + 1 + WL;             // tile-index shift giving the twiddle index
+        const uint32_t *tw = smtw + ((1u << (R - 1 - j)) - 1u) + (base >> S);
+#pragma unroll
+        for (int i0 = 0; i0 < 16; i0++) {
+            if (i0 & (1 << rb)) continue;
+            const int i1 = i0 | (1 << rb);
+            const uint32_t t = tw[i0 >> (rb + 1)];
+            if (FWD) {
+                uint32_t x = mmul(v[i1], t);
+                v[i1] = msub(v[i0], x);
+                v[i0] = madd(v[i0], x);
+            } else {
+                uint32_t a = v[i0], b = v[i1];
+                v[i0] = madd(a, b);
+                v[i1] = mmul(msub(a, b), t);
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 16; i++) sm[pad32(base | ((uint32_t)i << A))] = v[i];
+    (void)TB;
+}
+
+// Compile-time stage list: stage k covers pass layers [lo, hi), at most 4,
+// from the top for forward and from the bottom for inverse; the register
+// block A is the contiguous 4-bit block of the tile index covering them.
+template <bool FWD, int R, int WL, int K>
+struct StageIdx {
+    static constexpr int NST = (R + 3) / 4;
+    static constexpr int HI = FWD ? R - 4 * K : ((4 * K + 4) < R ? (4 * K + 4) : R);
+    static constexpr int LO = FWD ? ((R - 4 * K - 4) > 0 ? (R - 4 * K - 4) : 0) : 4 * K;
+    static constexpr int TB = R + WL;
+    static constexpr int A0 = (LO + WL) < (TB - 4) ? (LO + WL) : (TB - 4);
+    static constexpr int A = (HI + WL - A0) <= 4 ? A0 : (HI + WL - 4);
+};
+
+template <bool FWD, int R, int WL, int K>
+__device__ __forceinline__ void run_stages(uint32_t *sm, const uint32_t *smtw, uint32_t tid) {
+    if constexpr (K < StageIdx<FWD, R, WL, K>::NST) {
+        using St = StageIdx<FWD, R, WL, K>;
+        ntt_stage<FWD, R, WL, St::LO, St::HI, St::A>(sm, smtw, tid);
+        __syncthreads();
+        run_stages<FWD, R, WL, K + 1>(sm, smtw, tid);
+    }
+}
+
+template <bool FWD, int R, int WL>
+__global__ void __launch_bounds__((1 << (R + WL)) / 16) ntt_pass2_kernel(Pass2Args p) {
+    constexpr int TB = R + WL, TS = 1 << TB, NT = TS / 16, W = 1 << WL;
+    extern __shared__ uint32_t dsm[];
+    uint32_t *sm = dsm;                          // TS + TS/32 words
+    uint32_t *smtw = dsm + TS + TS / 32;         // 2^R - 1 twiddles
+    const uint32_t tid = threadIdx.x;
+    const uint32_t s = p.s;
+    const uint32_t cshift = s - WL;
+    const uint64_t tile = blockIdx.x;
+    const uint64_t cb = tile & ((1ull << cshift) - 1ull);
+    const uint64_t hb = tile >> cshift;
+    uint32_t *col = p.dev_cols ? p.dev_cols[blockIdx.y] : p.data + (uint64_t)blockIdx.y * p.col_stride;
+    const uint32_t *in = p.src ? p.src + (uint64_t)blockIdx.y * p.src_stride : col;
+    const uint64_t gbase = (hb << (s + R)) | (cb << WL);
+
+    // twiddles of layer j (pass-relative) are h in [hb 2^(R-1-j), (hb+1) 2^(R-1-j));
+    // every load is issued before any shared-memory store so they overlap
+    constexpr int TWN = (1 << R) - 1;
+    constexpr int TWPT = (TWN + NT - 1) / NT;   // twiddle loads per thread
+    constexpr int DPT = TS / NT;                // 16 data loads per thread
+    uint32_t tv[TWPT];
+#pragma unroll
+    for (int k = 0; k < TWPT; k++) {
+        uint32_t f = tid + (uint32_t)k * NT;
+        if (f < (uint32_t)TWN) {
+            uint32_t lg = 31u - __clz(f + 1u);   // floor(log2(f + 1))
+            uint32_t j = R - 1 - lg;
+            uint32_t t = f + 1u - (1u << lg);
+            uint32_t L = s + j;
+            const uint32_t *tab = L ? p.line + p.off.v[L - 1] : p.circle;
+            tv[k] = __ldg(tab + ((hb << lg) | t));
+        }
+    }
+    uint32_t dv[DPT];
+#pragma unroll
+    for (int k = 0; k < DPT; k++) {
+        uint32_t e = tid + (uint32_t)k * NT;
+        uint64_t g = gbase | ((uint64_t)(e >> WL) << s) | (e & (W - 1u));
+        dv[k] = in[p.src ? (g & p.src_mask) : g];
+    }
+#pragma unroll
+    for (int k = 0; k < TWPT; k++) {
+        uint32_t f = tid + (uint32_t)k * NT;
+        if (f < (uint32_t)TWN) smtw[f] = tv[k];
+    }
+#pragma unroll
+    for (int k = 0; k < DPT; k++) sm[pad32(tid + (uint32_t)k * NT)] = dv[k];
+    __syncthreads();
+    run_stages<FWD, R, WL, 0>(sm, smtw, tid);
+#pragma unroll
+    for (int k = 0; k < DPT; k++) {
+        uint32_t e = tid + (uint32_t)k * NT;
+        uint64_t g = gbase | ((uint64_t)(e >> WL) << s) | (e & (W - 1u));
+        uint32_t v = sm[pad32(e)];
+        col[g] = p.scale != 1u ? mmul(v, p.scale) : v;
+    }
+}
+
+template <bool FWD, int R, int WL>
+cudaError_t launch_pass2(const Pass2Args &a, uint64_t tiles, uint32_t n_cols, cudaStream_t st) {
+    constexpr int TS = 1 << (R + WL);
+    size_t smem = (TS + TS / 32 + (1 << R)) * 4;
+    ntt_pass2_kernel<FWD, R, WL><<<dim3((unsigned)tiles, n_cols), TS / 16, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <bool FWD>
+cudaError_t dispatch_pass2(uint32_t r, uint32_t wl, const Pass2Args &a, uint64_t tiles, uint32_t n_cols,
+                           cudaStream_t st) {
+    if (wl == 0) {
+        switch (r) {
+        case 4: return launch_pass2<FWD, 4, 0>(a, tiles, n_cols, st);
+        case 5: return launch_pass2<FWD, 5, 0>(a, tiles, n_cols, st);
+        case 6: return launch_pass2<FWD, 6, 0>(a, tiles, n_cols, st);
+        case 7: return launch_pass2<FWD, 7, 0>(a, tiles, n_cols, st);
+        case 8: return launch_pass2<FWD, 8, 0>(a, tiles, n_cols, st);
+        case 9: return launch_pass2<FWD, 9, 0>(a, tiles, n_cols, st);
+        case 10: return launch_pass2<FWD, 10, 0>(a, tiles, n_cols, st);
+        case 11: return launch_pass2<FWD, 11, 0>(a, tiles, n_cols, st);
+        case 12: return launch_pass2<FWD, 12, 0>(a, tiles, n_cols, st);
+        }
+    } else if (wl + r == 12) {
+        switch (r) {
+        case 3: return launch_pass2<FWD, 3, 9>(a, tiles, n_cols, st);
+        case 4: return launch_pass2<FWD, 4, 8>(a, tiles, n_cols, st);
+        case 5: return launch_pass2<FWD, 5, 7>(a, tiles, n_cols, st);
+        case 6: return launch_pass2<FWD, 6, 6>(a, tiles, n_cols, st);
+        case 7: return launch_pass2<FWD, 7, 5>(a, tiles, n_cols, st);
+        case 8: return launch_pass2<FWD, 8, 4>(a, tiles, n_cols, st);
+        case 9: return launch_pass2<FWD, 9, 3>(a, tiles, n_cols, st);
+        }
+    }
+    return cudaErrorInvalidValue;
+}
+
 bool g_attr_done = false;
 
 cudaError_t ensure_attrs() {
@@ -103,48 +281,70 @@ void ntt_table_offsets(uint32_t log_n, uint32_t off[32]) {
     for (uint32_t l = 0; l < 32; l++) off[l] = (l + 1 < log_n) ? (uint32_t)(m - (m >> l)) : 0u;
 }
 
+// Pass plan for `total` layers (0 .. total-1): a bottom pass of up to 12
+// layers on contiguous tiles (WL = 0), then passes of 3..9 layers, sizes
+// balanced, on tiles of 2^(12-R) contiguous columns (every tile 4096
+// elements; rows of at least 8 words = one 32-byte sector).  Transforms of
+// fewer than 4 layers use the one-tile shared-memory kernel.
+static uint32_t plan_passes(uint32_t total, uint32_t ps[32], uint32_t pr[32], uint32_t pw[32]) {
+    uint32_t np = 0;
+    uint32_t bottom = total < 12u ? total : 12u;
+    if (total > 12u && total < 15u) bottom = total - 3u;  // leave at least 3 layers above
+    ps[np] = 0; pr[np] = bottom; pw[np] = 0; np++;
+    uint32_t rest = total - bottom;
+    if (rest) {
+        uint32_t nu = (rest + 8u) / 9u;
+        if (rest < 3u * nu) nu = rest / 3u;  // every upper pass has 3..9 layers
+        uint32_t lo = bottom;
+        for (uint32_t i = 0; i < nu; i++) {
+            uint32_t r = rest / nu + (i < rest % nu ? 1u : 0u);
+            ps[np] = lo; pr[np] = r; pw[np] = 12u - r; np++;
+            lo += r;
+        }
+    }
+    return np;
+}
+
 cudaError_t ntt_transform(uint32_t *data, uint32_t *const *dev_cols, uint64_t col_stride, uint32_t n_cols,
                           uint32_t log_n, const NttTables &tw, bool forward, const uint32_t *src,
                           uint32_t src_log, cudaStream_t stream) {
     if (log_n == 0 || n_cols == 0) return cudaSuccess;
+    if (src && !forward) return cudaErrorInvalidValue;
     cudaError_t e = ensure_attrs();
     if (e != cudaSuccess) return e;
-    const uint32_t top = (src ? src_log : log_n) - 1u;  // highest layer applied
-    const uint32_t total = top + 1u;
-    const uint32_t np = (total + kMaxPassLayers - 1u) / kMaxPassLayers;
-    // pass ranges from the top down: sizes as even as possible
-    uint32_t ps[32], pr[32];
-    uint32_t hi = total;
-    for (uint32_t i = 0; i < np; i++) {
-        uint32_t r = total / np + (i < total % np ? 1u : 0u);
-        pr[i] = r;
-        ps[i] = hi - r;
-        hi -= r;
-    }
+    const uint32_t total = src ? src_log : log_n;  // layers applied: total-1 .. 0
     PassOff off;
     for (int i = 0; i < 32; i++) off.v[i] = tw.off[i];
     uint32_t e2 = (30u * log_n) % 31u;
     uint32_t inv_n = e2 == 0 ? 1u : (1u << e2);
-    for (uint32_t q = 0; q < np; q++) {
-        uint32_t i = forward ? q : np - 1u - q;
-        uint32_t s = ps[i], r = pr[i];
-        uint32_t wlog = s < 3u ? s : 3u;
-        uint32_t tsz = (1u << r) << wlog;
-        uint32_t threads = tsz / 2 < 32u ? 32u : (tsz / 2 > 512u ? 512u : tsz / 2);
+    const uint64_t mask = src ? ((1ull << src_log) - 1ull) : ~0ull;
+    const uint64_t src_stride = src ? (1ull << src_log) : 0ull;
+    if (total < 4) {
+        // tiny transform: one tile of 2^total rows, single-layer smem kernel
+        uint32_t r = total, wlog = 0, tsz = 1u << r;
         uint64_t tiles = (1ull << log_n) / tsz;
-        dim3 grid((unsigned)tiles, n_cols);
-        const uint32_t *in = (q == 0 && src) ? src : nullptr;
-        uint64_t mask = src ? ((1ull << src_log) - 1ull) : ~0ull;
-        uint64_t src_stride = src ? (1ull << src_log) : 0ull;
-        bool last_inv = !forward && q == np - 1u;
         if (forward)
-            ntt_pass_kernel<true><<<grid, threads, tsz * 4, stream>>>(data, dev_cols, col_stride, in, mask, src_stride,
-                                                                     tw.line, tw.circle, off, s, r, wlog, 1u);
+            ntt_pass_kernel<true><<<dim3((unsigned)tiles, n_cols), 32, tsz * 4, stream>>>(
+                data, dev_cols, col_stride, src, mask, src_stride, tw.line, tw.circle, off, 0, r, wlog, 1u);
         else
-            ntt_pass_kernel<false><<<grid, threads, tsz * 4, stream>>>(data, dev_cols, col_stride, in, mask, src_stride,
-                                                                      tw.line, tw.circle, off, s, r, wlog,
-                                                                      last_inv ? inv_n : 1u);
-        e = cudaGetLastError();
+            ntt_pass_kernel<false><<<dim3((unsigned)tiles, n_cols), 32, tsz * 4, stream>>>(
+                data, dev_cols, col_stride, nullptr, mask, 0, tw.line, tw.circle, off, 0, r, wlog, inv_n);
+        return cudaGetLastError();
+    }
+    uint32_t ps[32], pr[32], pw[32];
+    const uint32_t np = plan_passes(total, ps, pr, pw);
+    for (uint32_t q = 0; q < np; q++) {
+        uint32_t i = forward ? np - 1u - q : q;   // forward: top pass first
+        Pass2Args a;
+        a.data = data; a.dev_cols = dev_cols; a.col_stride = col_stride;
+        a.src = (q == 0 && src) ? src : nullptr;
+        a.src_mask = mask; a.src_stride = src_stride;
+        a.line = tw.line; a.circle = tw.circle; a.off = off;
+        a.s = ps[i];
+        a.scale = (!forward && q == np - 1u) ? inv_n : 1u;
+        uint64_t tiles = (1ull << log_n) >> (pr[i] + pw[i]);
+        e = forward ? dispatch_pass2<true>(pr[i], pw[i], a, tiles, n_cols, stream)
+                    : dispatch_pass2<false>(pr[i], pw[i], a, tiles, n_cols, stream);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;

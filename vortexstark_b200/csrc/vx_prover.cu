@@ -103,10 +103,12 @@ __device__ void fib_at(uint32_t a, uint32_t b, uint64_t k, uint32_t &fk, uint32_
 // Fibonacci trace t0 = a, t1 = b, t_{i+2} = t_i + t_{i+1} (air.rs:16-25),
 // chunks of 32 rows per thread seeded by fib_at.  Also stamps (a, b) into
 // the proof header.
-__global__ void fib_trace_kernel(uint32_t a, uint32_t b, uint32_t *out, uint64_t n, uint32_t *proof_ab) {
+__global__ void fib_trace_kernel(uint32_t a, uint32_t b, const uint32_t *ab_dev, uint32_t *out, uint64_t n,
+                                 uint32_t *proof_ab) {
     uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t C = 32;
     uint64_t s = t * C;
+    if (ab_dev) { a = ab_dev[0]; b = ab_dev[1]; }
     if (t == 0) { proof_ab[0] = a; proof_ab[1] = b; }
     if (s >= n) return;
     uint32_t f0, f1;
@@ -272,6 +274,80 @@ __global__ void decommit_values_kernel(ValuesArgs a, const uint32_t *qidx, uint3
     }
 }
 
+// All authentication paths of a proof in one launch: blockIdx.y selects the
+// tree (0 trace, 1 quotient, 2 + k FRI layer k), threads cover
+// (query, stored-level group) pairs of that tree.
+struct PathTree {
+    TreeLevels lv;
+    uint32_t kind;    // 0: M31 eval column, 1: quotient from eval, 2: SoA4 layer
+    uint32_t shift;   // query index >> shift is the leaf index
+    const uint32_t *c[4];
+    uint64_t paths, spaths;
+};
+struct PathsArgs {
+    PathTree t[34];
+    const uint32_t *eval;
+    uint64_t mask;
+    const uint32_t *alpha_q;
+};
+__global__ void __launch_bounds__(64) decommit_all_kernel(const __grid_constant__ PathsArgs a, const uint32_t *qidx,
+                                                          uint32_t nq, uint32_t *proof) {
+    const PathTree &T = a.t[blockIdx.y];
+    uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t ng = T.lv.n - 1;
+    if (tid >= nq * ng) return;
+    uint32_t q = tid / ng, g = tid % ng;
+    uint32_t depth = T.lv.height[T.lv.n - 1];
+    uint64_t idx = (uint64_t)qidx[q] >> T.shift;
+    uint32_t lo = T.lv.height[g], k = T.lv.height[g + 1] - lo;
+    uint64_t node = idx >> lo;
+    uint64_t blk = node >> k;
+    const uint32_t K = 1u << k;
+    uint32_t nh[31][8];
+    if (g == 0) {
+        LeafQuotient lq{a.eval, a.mask, a.alpha_q, {0, 0, 0, 0}};
+        if (T.kind == 1) lq.init();
+        for (uint32_t j = 0; j < K; j++) {
+            uint32_t m[16];
+#pragma unroll
+            for (int w = 0; w < 16; w++) m[w] = 0u;
+            uint64_t i = (blk << k) + j;
+            uint32_t nb;
+            if (T.kind == 0) { m[0] = T.c[0][i]; nb = 4u; }
+            else if (T.kind == 1) { nb = lq.load(i, m); }
+            else { m[0] = T.c[0][i]; m[1] = T.c[1][i]; m[2] = T.c[2][i]; m[3] = T.c[3][i]; nb = 16u; }
+            blake2s_block(nh[j], m, nb);
+        }
+    } else {
+        const uint32_t *h = T.lv.hashes[g] + 8ull * (blk << k);
+        for (uint32_t j = 0; j < K; j++)
+#pragma unroll
+            for (int w = 0; w < 8; w++) nh[j][w] = h[8 * j + w];
+    }
+    uint32_t lvl_off = 0, cnt = K;
+    for (uint32_t d = 0; d < k; d++) {
+        uint32_t nxt = lvl_off + cnt;
+        for (uint32_t j = 0; j < cnt / 2; j++) blake2s_node(nh[nxt + j], nh[lvl_off + 2 * j], nh[lvl_off + 2 * j + 1]);
+        lvl_off = nxt;
+        cnt /= 2;
+    }
+    uint32_t *p = proof + T.paths + (uint64_t)q * (1u + 8u * depth);
+    uint32_t *sp = proof + T.spaths + (uint64_t)q * (1u + 8u * depth);
+    lvl_off = 0; cnt = K;
+    uint64_t local = node & (K - 1u);
+    for (uint32_t d = 0; d < k; d++) {
+        uint32_t hgt = lo + d;
+        const uint32_t *sib = nh[lvl_off + (uint32_t)(local ^ 1u)];
+        const uint32_t *self = nh[lvl_off + (uint32_t)local];
+#pragma unroll
+        for (int w = 0; w < 8; w++) {
+            p[1 + 8 * hgt + w] = sib[w];
+            sp[1 + 8 * hgt + w] = (hgt == 0) ? self[w] : sib[w];
+        }
+        lvl_off += cnt; cnt /= 2; local >>= 1;
+    }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------
@@ -335,7 +411,9 @@ static void tables_destroy(SizeTables *t) {
 
 static size_t tables_bytes(const SizeTables *t) {
     uint64_t n = 1ull << t->log_n, N = 1ull << t->le;
-    return (size_t)(4 * ((n - 1) + n / 2 + (N - 1) + N / 2 + N / 2 + N / 2));
+    uint64_t w = align_words(n - 1) + align_words(n / 2) + align_words(N - 1) + align_words(N / 2) + align_words(N / 2);
+    for (uint32_t l = t->le - 1; l >= 4; l--) w += align_words(1ull << (l - 1));
+    return (size_t)(w * 4);
 }
 
 // Per-(device, log_n, blowup) shared tables.
@@ -484,7 +562,8 @@ static int enqueue_stage(vx_prover *p, uint32_t stage, uint32_t a, uint32_t b, c
     switch (stage) {
     case 0:
         VX_CUDA_TRY(cudaMemsetAsync(S.chan, 0, sizeof(DevChannel), st));
-        fib_trace_kernel<<<blocks_for((n + 31) / 32, 256), 256, 0, st>>>(a, b, S.coeffs, n, proof + L.magic + 3);
+        fib_trace_kernel<<<blocks_for((n + 31) / 32, 256), 256, 0, st>>>(a, b, S.inputs, S.coeffs, n,
+                                                                         proof + L.magic + 3);
         *launches += 1;
         break;
     case 1: {
@@ -550,17 +629,24 @@ static int enqueue_stage(vx_prover *p, uint32_t stage, uint32_t a, uint32_t b, c
             va.vals[2 + k] = L.fri[k].vals; va.svals[2 + k] = L.fri[k].svals;
         }
         decommit_values_kernel<<<blocks_for((uint64_t)(2 + L.nfri) * L.nq, 128), 128, 0, st>>>(va, S.qidx, L.nq, proof);
-        *launches += 1;
-        auto paths = [&](auto src, const TreeLevels &lv, uint32_t shift, const DecomLayout &d) {
-            uint32_t nt = L.nq * (lv.n - 1);
-            decommit_paths_kernel<<<blocks_for(nt, 64), 64, 0, st>>>(src, lv, S.qidx, shift, L.nq, proof + d.paths,
-                                                                     proof + d.spaths);
-            *launches += 1;
+        PathsArgs pa;
+        memset(&pa, 0, sizeof(pa));
+        pa.eval = S.eval; pa.mask = N - 1; pa.alpha_q = S.alpha_q;
+        uint32_t max_groups = 0;
+        auto add = [&](uint32_t i, const TreeLevels &lv, uint32_t kind, uint32_t shift, const uint32_t *const *c,
+                       const DecomLayout &d) {
+            pa.t[i].lv = lv; pa.t[i].kind = kind; pa.t[i].shift = shift;
+            for (int q = 0; q < 4; q++) pa.t[i].c[q] = c ? c[q] : nullptr;
+            pa.t[i].paths = d.paths; pa.t[i].spaths = d.spaths;
+            if (lv.n - 1 > max_groups) max_groups = lv.n - 1;
         };
-        paths(LeafM31{S.eval}, S.trace_lv, 0, L.trace);
-        paths(lq, S.quot_lv, 0, L.quot);
-        for (uint32_t k = 0; k < L.nfri; k++)
-            paths(LeafSoA4{S.fri[k][0], S.fri[k][1], S.fri[k][2], S.fri[k][3]}, S.fri_lv[k], k + 1, L.fri[k]);
+        const uint32_t *ev4[4] = {S.eval, nullptr, nullptr, nullptr};
+        add(0, S.trace_lv, 0, 0, ev4, L.trace);
+        add(1, S.quot_lv, 1, 0, nullptr, L.quot);
+        for (uint32_t k = 0; k < L.nfri; k++) add(2 + k, S.fri_lv[k], 2, k + 1, S.fri[k], L.fri[k]);
+        dim3 grid(blocks_for((uint64_t)L.nq * max_groups, 64), 2 + L.nfri);
+        decommit_all_kernel<<<grid, 64, 0, st>>>(pa, S.qidx, L.nq, proof);
+        *launches += 2;
         break;
     }
     default:
@@ -662,3 +748,61 @@ extern "C" void vx_release_all(void) {
     for (auto &kv : g_tables) tables_destroy(kv.second.first);
     g_tables.clear();
 }
+
+
+namespace vx {
+// Capture one whole proof of slot `p` as a CUDA graph whose public inputs
+// come from `pinned_ab` (two words of pinned host memory, copied to the
+// device by the graph's first node) and whose proof bytes land in
+// `pinned_out`.  Used by the serving engine, one graph per slot.
+int prover_capture_graph(vx_prover *p, cudaStream_t st, uint32_t *dev_ab, const uint32_t *pinned_ab,
+                         void *pinned_out, cudaGraphExec_t *exec) {
+    ProofSlot &S = p->s;
+    // one plain proof first so every lazily set kernel attribute exists
+    uint32_t launches = 0;
+    for (uint32_t stage = 0; stage < VX_N_STAGES; stage++) {
+        int rc = enqueue_stage(p, stage, 1u, 1u, st, &launches);
+        if (rc) return rc;
+    }
+    VX_CUDA_TRY(cudaStreamSynchronize(st));
+    S.inputs = dev_ab;
+    cudaGraph_t g = nullptr;
+    VX_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int rc = VX_OK;
+    if (cudaMemcpyAsync(dev_ab, pinned_ab, 8, cudaMemcpyHostToDevice, st) != cudaSuccess) rc = VX_ERR_CUDA;
+    launches = 0;
+    for (uint32_t stage = 0; stage < VX_N_STAGES && rc == VX_OK; stage++) rc = enqueue_stage(p, stage, 0u, 0u, st, &launches);
+    if (rc == VX_OK && cudaMemcpyAsync(pinned_out, S.proof, S.L.words * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        rc = VX_ERR_CUDA;
+    cudaError_t e = cudaStreamEndCapture(st, &g);
+    S.inputs = nullptr;
+    if (rc != VX_OK) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) { set_last_error(VX_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e)); return VX_ERR_CUDA; }
+    e = cudaGraphInstantiate(exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { set_last_error(VX_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e)); return VX_ERR_CUDA; }
+    p->launches = launches;
+    return VX_OK;
+}
+// Device bytes vx_prover_create takes for one slot of this size, and the
+// shared tables of the size (same arithmetic as the carving above).
+void prover_footprint(uint32_t log_n, uint32_t blowup, uint32_t nq, size_t *slot_b, size_t *tab_b) {
+    ProofLayout L;
+    proof_layout(log_n, blowup, nq, &L);
+    uint32_t le = L.le;
+    uint64_t n = 1ull << log_n, N = 1ull << le;
+    uint64_t w = align_words(n) + align_words(N);
+    for (uint32_t k = 0; k < L.nfri; k++) w += 4 * align_words(1ull << (le - 1 - k));
+    w += 2 * align_words(tree_pool_words(le));
+    for (uint32_t k = 0; k < L.nfri; k++) w += align_words(tree_pool_words(le - 1 - k));
+    w += align_words(sizeof(DevChannel) / 4 + 1) + align_words(4) + align_words(4ull * (L.nfri + 1)) +
+         align_words(nq) + align_words(L.words);
+    *slot_b = (size_t)(w * 4);
+    uint64_t t = align_words(n - 1) + align_words(n / 2) + align_words(N - 1) + align_words(N / 2) + align_words(N / 2);
+    for (uint32_t l = le - 1; l >= 4; l--) t += align_words(1ull << (l - 1));
+    *tab_b = (size_t)(t * 4);
+}
+uint32_t prover_log_n(const vx_prover *p) { return p->s.L.log_n; }
+size_t prover_proof_bytes(const vx_prover *p) { return (size_t)(p->s.L.words * 4); }
+const uint32_t *prover_chan_err(const vx_prover *p) { return &p->s.chan->err; }
+}  // namespace vx

@@ -56,8 +56,19 @@ struct ProofSlot {
     uint32_t *alpha_f;             // 4 words per FRI fold
     uint32_t *qidx;                // n_queries words
     uint32_t *proof;               // device proof, L.words words
+    const uint32_t *inputs;        // device (a, b) for captured graphs; null = kernel arguments
     void *block;                   // single allocation backing the above
     size_t block_bytes;
 };
 
+}  // namespace vx
+
+struct vx_prover;
+namespace vx {
+int prover_capture_graph(vx_prover *p, cudaStream_t st, uint32_t *dev_ab, const uint32_t *pinned_ab,
+                         void *pinned_out, cudaGraphExec_t *exec);
+uint32_t prover_log_n(const vx_prover *p);
+void prover_footprint(uint32_t log_n, uint32_t blowup, uint32_t nq, size_t *slot_b, size_t *tab_b);
+size_t prover_proof_bytes(const vx_prover *p);
+const uint32_t *prover_chan_err(const vx_prover *p);
 }  // namespace vx

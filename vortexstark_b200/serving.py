@@ -1,0 +1,159 @@
+"""Serving: continuous batching of mixed-size Fibonacci proof requests.
+
+``ProofServer`` wraps the native serving engine (vx_server_* in
+libvortex_b200): requests queue on the host, a dispatcher thread admits them
+as proof slots of their size free up or fit in the device-memory budget, and
+up to ``max_inflight`` proofs overlap on the GPU, each as one CUDA graph on
+its own stream.  ``run_stream`` replays a request stream with Poisson
+arrivals and reports throughput and latency; ``run_sequential`` is the plain
+one-proof-at-a-time path on the same arrivals, for comparison.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import random
+import statistics
+import threading
+import time
+
+from . import _lib
+
+
+class Completion(C.Structure):
+    _fields_ = [("tag", C.c_uint64), ("status", C.c_int32), ("log_n", C.c_uint32), ("submit_ns", C.c_uint64),
+                ("start_ns", C.c_uint64), ("done_ns", C.c_uint64), ("proof_bytes", C.c_uint64)]
+
+
+class ProofServer:
+    def __init__(self, budget_bytes: int, max_inflight: int = 16, blowup_bits: int = 2, n_queries: int = 80,
+                 use_graphs: bool = True):
+        self._s = C.c_void_p()
+        _lib.check(_lib.lib().vx_server_create(int(budget_bytes), max_inflight, blowup_bits, n_queries,
+                                               1 if use_graphs else 0, C.byref(self._s)))
+
+    def prewarm(self, log_n: int, count: int) -> None:
+        _lib.check(_lib.lib().vx_server_prewarm(self._s, log_n, count))
+
+    def submit(self, tag: int, log_n: int, a: int, b: int) -> None:
+        _lib.check(_lib.lib().vx_server_submit(self._s, tag, log_n, a, b))
+
+    def poll(self, max_items: int = 256, wait_ms: int = 0):
+        buf = (Completion * max_items)()
+        n = C.c_uint32()
+        _lib.check(_lib.lib().vx_server_poll(self._s, buf, max_items, C.byref(n), wait_ms))
+        return [buf[i] for i in range(n.value)]
+
+    def result(self, tag: int, keep: bool = True):
+        """Proof bytes of a finished request (and release them)."""
+        L = _lib.lib()
+        n = C.c_size_t()
+        if not keep:
+            _lib.check(L.vx_server_result(self._s, tag, None, 0, C.byref(n)))
+            return None
+        # size first is not available separately; proofs are at most a few MB
+        cap = 1 << 25
+        buf = (C.c_uint8 * cap)()
+        _lib.check(L.vx_server_result(self._s, tag, C.addressof(buf), cap, C.byref(n)))
+        return bytes(buf[: n.value])
+
+    def stats(self) -> dict:
+        ns, inf, pend = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        used = C.c_size_t()
+        _lib.check(_lib.lib().vx_server_stats(self._s, C.byref(ns), C.byref(inf), C.byref(pend), C.byref(used)))
+        return {"slots": ns.value, "inflight": inf.value, "pending": pend.value, "bytes_used": used.value}
+
+    def close(self) -> None:
+        if self._s:
+            _lib.lib().vx_server_destroy(self._s)
+            self._s = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def poisson_arrivals(n: int, rate: float, seed: int):
+    """Arrival offsets (seconds) of a Poisson process with the given rate."""
+    rng = random.Random(seed)
+    t, out = 0.0, []
+    for _ in range(n):
+        t += rng.expovariate(rate)
+        out.append(t)
+    return out
+
+
+def _summary(lat_ms, makespan_s, n):
+    lat = sorted(lat_ms)
+    p99 = lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))]
+    return {"proofs_per_s": n / makespan_s, "p50_ms": statistics.median(lat), "p99_ms": p99,
+            "mean_ms": statistics.fmean(lat), "makespan_s": makespan_s, "n": n}
+
+
+def run_stream(server: ProofServer, requests, arrivals, keep_results: bool = False):
+    """Submit requests (log_n, a, b) at the given arrival offsets; return the
+    summary and, if asked, the proof bytes per request index."""
+    n = len(requests)
+    lat = [0.0] * n
+    results = {}
+    done = threading.Event()
+    t0 = time.perf_counter_ns()
+    submit_ns = [0] * n
+
+    def submitter():
+        for i, ((log_n, a, b), at) in enumerate(zip(requests, arrivals)):
+            target = t0 + int(at * 1e9)
+            while True:
+                d = target - time.perf_counter_ns()
+                if d <= 0:
+                    break
+                time.sleep(min(d / 1e9, 0.001) if d > 200_000 else 0)
+            submit_ns[i] = time.perf_counter_ns()
+            server.submit(i, log_n, a, b)
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    got = 0
+    last_done = t0
+    while got < n:
+        for c in server.poll(256, wait_ms=50):
+            if c.status != 0:
+                raise RuntimeError(f"request {c.tag} failed with status {c.status}: {_lib.last_error()}")
+            i = int(c.tag)
+            lat[i] = (c.done_ns - c.submit_ns) / 1e6
+            last_done = max(last_done, time.perf_counter_ns())
+            if keep_results:
+                results[i] = server.result(i)
+            else:
+                server.result(i, keep=False)
+            got += 1
+    th.join()
+    done.set()
+    s = _summary(lat, (last_done - t0) / 1e9, n)
+    return s, results
+
+
+def run_sequential(requests, arrivals, blowup_bits: int = 2, n_queries: int = 80, caches=None):
+    """The plain one-proof-at-a-time GPU path on the same arrivals: requests in
+    arrival order, each started when it has arrived and the previous proof has
+    finished (vx_prove_fib through one cached slot per size)."""
+    from . import prover
+
+    n = len(requests)
+    lat = []
+    t0 = time.perf_counter()
+    for (log_n, a, b), at in zip(requests, arrivals):
+        now = time.perf_counter() - t0
+        if now < at:
+            time.sleep(at - now)
+        start_wait = t0 + at
+        prover.prove_bytes(a, b, log_n, blowup_bits, n_queries)
+        lat.append((time.perf_counter() - start_wait) * 1e3)
+    return _summary(lat, time.perf_counter() - t0, n)
