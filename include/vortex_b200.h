@@ -246,6 +246,22 @@ void vx_server_destroy(vx_server *s);
  * roofline of the Merkle kernels. */
 int vx_probe_blake2s(uint32_t blocks, uint32_t threads, uint32_t iters, uint32_t *out, void *stream);
 
+/* Whole proof without any device allocation — no counterpart in the
+ * reference.  For callers that may not allocate device memory: code inside a
+ * stream capture or CUDA-graph construction, hosts whose device memory is
+ * owned by another allocator (a Rust arena, a framework's caching pool), or
+ * sandboxes that forbid cudaMalloc after start-up.  Same result as
+ * vx_prove_fib, with every byte of device scratch in one fixed 8 MiB static
+ * device array of this library (held on every GPU that loads it until the
+ * process exits), so the size is limited to log_n + blowup_bits <= 14 and
+ * n_queries <= 80; larger sizes are rejected with VX_ERR_ARG.  The first call
+ * on a device looks up the array's device address and uploads constant
+ * tables, so make it before any stream capture.  Runs on the legacy default
+ * stream and returns when the proof is in `out`.  All calls share the array:
+ * calls that overlap on the GPU (other host threads, other streams) race. */
+int vx_prove_fib_noalloc(uint32_t a, uint32_t b, uint32_t log_n, uint32_t blowup_bits, uint32_t n_queries,
+                         uint8_t *out, size_t cap, size_t *out_len);
+
 /* Free every cached slot and table on every device. */
 void vx_release_all(void);
 

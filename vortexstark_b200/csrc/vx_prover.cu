@@ -749,6 +749,156 @@ extern "C" void vx_release_all(void) {
     g_tables.clear();
 }
 
+// ---------------------------------------------------------------------
+// vx_prove_fib_noalloc: the whole proof without any device allocation.
+//
+// For callers that may not allocate device memory: code running inside a
+// stream capture or a CUDA graph being built, hosts whose device memory is
+// owned by another allocator (a Rust arena, a framework's caching pool) and
+// sandboxes that forbid cudaMalloc after start-up.  Every byte of device
+// scratch — generator tables, twiddle tables, the LDE, FRI layers, stored
+// tree levels, transcript state and the proof — lives in one file-scope
+// static __device__ array of kNoAllocWords words (8 MiB), which every GPU
+// that loads this library keeps until the process exits.
+// ---------------------------------------------------------------------
+namespace {
+constexpr uint64_t kNoAllocWords = 1ull << 21;   // 8 MiB of device scratch
+constexpr uint32_t kNoAllocMaxLogEval = 14;       // log_n + blowup_bits <= 14
+constexpr uint32_t kNoAllocMaxQueries = 80;
+static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocWords];
+
+struct NoAllocDevice {
+    bool ready;
+    uint32_t *base;                 // device address of g_noalloc_scratch
+    uint32_t tab_log_n, tab_blowup; // size whose tables are resident (0 = none)
+};
+std::mutex g_na_mu;
+NoAllocDevice g_na[64];
+uint32_t g_na_host[kGenTableWords];       // staging for the generator tables
+uint32_t g_na_proof_tmpl[1u << 18];       // staging for the proof template
+}  // namespace
+
+extern "C" int vx_prove_fib_noalloc(uint32_t a, uint32_t b, uint32_t log_n, uint32_t blowup_bits,
+                                    uint32_t n_queries, uint8_t *out, size_t cap, size_t *out_len) {
+    VX_CHECK_ARG(out != nullptr && out_len != nullptr, "vx_prove_fib_noalloc: null output");
+    VX_CHECK_ARG(a < VX_P && b < VX_P, "vx_prove_fib_noalloc: public inputs must be canonical M31 (< 2^31-1)");
+    VX_CHECK_ARG(log_n >= 4 && blowup_bits >= 1 && log_n + blowup_bits <= kNoAllocMaxLogEval,
+                 "vx_prove_fib_noalloc: needs 4 <= log_n, blowup_bits >= 1 and log_n + blowup_bits <= %u "
+                 "(got %u, %u); larger proofs need vx_prove_fib",
+                 kNoAllocMaxLogEval, log_n, blowup_bits);
+    VX_CHECK_ARG(n_queries >= 1 && n_queries <= kNoAllocMaxQueries,
+                 "vx_prove_fib_noalloc: n_queries must be in [1, %u]", kNoAllocMaxQueries);
+    ProofLayout L;
+    proof_layout(log_n, blowup_bits, n_queries, &L);
+    size_t need = (size_t)(L.words * 4);
+    VX_CHECK_ARG(cap >= need, "vx_prove_fib_noalloc: output capacity %zu < proof size %zu", cap, need);
+    VX_CHECK_ARG(L.words <= (sizeof(g_na_proof_tmpl) / 4), "vx_prove_fib_noalloc: proof layout too large");
+    int dev = 0;
+    VX_CUDA_TRY(cudaGetDevice(&dev));
+    VX_CHECK_ARG(dev >= 0 && dev < 64, "vx_prove_fib_noalloc: device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lk(g_na_mu);
+    NoAllocDevice &D = g_na[dev];
+    if (!D.ready) {
+        // once per device: the array's device address (the host symbol is
+        // only a stand-in) and the generator tables
+        void *p = nullptr;
+        VX_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        gen_tables_host(g_na_host);
+        VX_CUDA_TRY(cudaMemcpy(p, g_na_host, sizeof(g_na_host), cudaMemcpyHostToDevice));
+        D.base = (uint32_t *)p;
+        D.tab_log_n = D.tab_blowup = 0;
+        D.ready = true;
+    }
+    uint32_t *base = D.base;
+    GenTables g{(const cpoint *)base, (const cpoint *)base + (1u << 16)};
+    const uint32_t le = L.le;
+    const uint64_t n = 1ull << log_n, N = 1ull << le;
+    uint64_t w = align_words(kGenTableWords);
+    // tables, laid out as tables_create does
+    SizeTables T;
+    memset(&T, 0, sizeof(T));
+    T.device = dev; T.log_n = log_n; T.blowup = blowup_bits; T.le = le;
+    T.itw_line = base + w; w += align_words(n - 1);
+    T.itw_circle = base + w; w += align_words(n / 2);
+    T.ftw_line = base + w; w += align_words(N - 1);
+    T.ftw_circle = base + w; w += align_words(N / 2);
+    T.fold_circle = base + w; w += align_words(N / 2);
+    T.fold_line = base + w;
+    uint64_t fl = 0;
+    for (uint32_t l = le - 1; l >= 4; l--) { T.fold_line_off[l] = fl; fl += align_words(1ull << (l - 1)); }
+    w += fl;
+    ntt_table_offsets(log_n, T.itw_off);
+    ntt_table_offsets(le, T.ftw_off);
+    // slot, laid out as vx_prover_create does
+    vx_prover P;
+    memset(&P.s, 0, sizeof(P.s));
+    P.device = dev;
+    P.launches = 0;
+    ProofSlot &S = P.s;
+    S.tw = &T;
+    S.L = L;
+    S.coeffs = base + w; w += align_words(n);
+    S.eval = base + w; w += align_words(N);
+    for (uint32_t k = 0; k < L.nfri; k++) {
+        uint64_t sz = align_words(1ull << (le - 1 - k));
+        for (int c = 0; c < 4; c++) S.fri[k][c] = base + w + c * sz;
+        w += 4 * sz;
+    }
+    w += align_words(tree_plan(le, base + w, &S.trace_lv));
+    w += align_words(tree_plan(le, base + w, &S.quot_lv));
+    for (uint32_t k = 0; k < L.nfri; k++) w += align_words(tree_plan(le - 1 - k, base + w, &S.fri_lv[k]));
+    S.chan = (DevChannel *)(base + w); w += align_words(sizeof(DevChannel) / 4 + 1);
+    S.alpha_q = base + w; w += align_words(4);
+    S.alpha_f = base + w; w += align_words(4ull * (L.nfri + 1));
+    S.qidx = base + w; w += align_words(n_queries);
+    S.proof = base + w; w += align_words(L.words);
+    VX_CHECK_ARG(w <= kNoAllocWords, "vx_prove_fib_noalloc: layout of %llu words exceeds the static scratch of %llu",
+                 (unsigned long long)w, (unsigned long long)kNoAllocWords);
+    cudaStream_t st = nullptr;  // legacy default stream
+    if (D.tab_log_n != log_n || D.tab_blowup != blowup_bits) {
+        D.tab_log_n = D.tab_blowup = 0;
+        VX_CUDA_TRY(build_ntt_tables_with(g, ecoset_half_coset(log_n), true, T.itw_line, T.itw_circle, st));
+        VX_CUDA_TRY(build_ntt_tables_with(g, ecoset_eval_domain(le), false, T.ftw_line, T.ftw_circle, st));
+        VX_CUDA_TRY(build_fold_twiddles_with(g, ecoset_eval_domain(le), true, T.fold_circle, st));
+        for (uint32_t l = le - 1; l >= 4; l--)
+            VX_CUDA_TRY(build_fold_twiddles_with(g, ecoset_half_odds(l), false, T.fold_line + T.fold_line_off[l], st));
+        D.tab_log_n = log_n;
+        D.tab_blowup = blowup_bits;
+    }
+    // the proof's constant words; everything else is overwritten by the stages
+    memset(g_na_proof_tmpl, 0, L.words * 4);
+    {
+        g_na_proof_tmpl[L.magic] = 0x4B52414Bu; g_na_proof_tmpl[L.magic + 1] = 1u; g_na_proof_tmpl[L.magic + 2] = log_n;
+        g_na_proof_tmpl[L.nfri_w] = L.nfri;
+        g_na_proof_tmpl[L.nlast] = 8u;
+        g_na_proof_tmpl[L.nq_w] = L.nq;
+        auto dec = [&](const DecomLayout &d) {
+            g_na_proof_tmpl[d.n] = L.nq;
+            for (uint32_t q = 0; q < L.nq; q++) {
+                g_na_proof_tmpl[d.paths + (uint64_t)q * (1 + 8ull * d.depth)] = d.depth;
+                g_na_proof_tmpl[d.spaths + (uint64_t)q * (1 + 8ull * d.depth)] = d.depth;
+            }
+        };
+        dec(L.trace); dec(L.quot);
+        g_na_proof_tmpl[L.nfd] = L.nfri;
+        for (uint32_t k = 0; k < L.nfri; k++) dec(L.fri[k]);
+    }
+    VX_CUDA_TRY(cudaMemcpy(S.proof, g_na_proof_tmpl, L.words * 4, cudaMemcpyHostToDevice));
+    uint32_t launches = 0;
+    for (uint32_t stage = 0; stage < VX_N_STAGES; stage++) {
+        int rc = enqueue_stage(&P, stage, a, b, st, &launches);
+        if (rc) return rc;
+    }
+    VX_CUDA_TRY(cudaMemcpy(out, S.proof, need, cudaMemcpyDeviceToHost));
+    uint32_t err = 0;
+    VX_CUDA_TRY(cudaMemcpy(&err, &S.chan->err, 4, cudaMemcpyDeviceToHost));
+    if (err) {
+        set_last_error(VX_ERR_DEVICE, "transcript rejection sampling exceeded its bound");
+        return VX_ERR_DEVICE;
+    }
+    *out_len = need;
+    return VX_OK;
+}
 
 namespace vx {
 // Capture one whole proof of slot `p` as a CUDA graph whose public inputs

@@ -128,4 +128,42 @@ cudaError_t build_fold_twiddles(ecoset c, bool extract_y, uint32_t *out, cudaStr
     return batch_inverse(out, out, half, stream);
 }
 
+cudaError_t build_ntt_tables_with(const GenTables &g, ecoset c, bool inverse, uint32_t *line, uint32_t *circle,
+                                  cudaStream_t stream) {
+    uint64_t m = 1ull << c.k;
+    uint64_t off = 0;
+    for (uint32_t l = 0; l + 1 < c.k; l++) {
+        uint64_t size = m >> (l + 1);
+        line_layer_kernel<<<blocks_for(size, 256), 256, 0, stream>>>(g, c.e0, c.k, l, line + off, size);
+        off += size;
+    }
+    if (m / 2) circle_layer_kernel<<<blocks_for(m / 2, 256), 256, 0, stream>>>(g, c.e0, c.k, circle, m / 2);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (inverse) {
+        if (off) { e = batch_inverse(line, line, off, stream); if (e != cudaSuccess) return e; }
+        if (m / 2) { e = batch_inverse(circle, circle, m / 2, stream); if (e != cudaSuccess) return e; }
+    }
+    return cudaSuccess;
+}
+
+cudaError_t build_fold_twiddles_with(const GenTables &g, ecoset c, bool extract_y, uint32_t *out,
+                                     cudaStream_t stream) {
+    uint64_t half = (1ull << c.k) / 2;
+    if (!half) return cudaSuccess;
+    fold_sources_kernel<<<blocks_for(half, 256), 256, 0, stream>>>(g, c.e0, c.k, extract_y ? 1 : 0, out, half);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return batch_inverse(out, out, half, stream);
+}
+
+void gen_tables_host(uint32_t *w) {
+    hpoint p{1u, 0u};
+    for (uint32_t i = 0; i < (1u << 16); i++) { w[2 * i] = p.x; w[2 * i + 1] = p.y; p = h_pmul(p, kGen); }
+    hpoint g16 = h_ppow(kGen, 1ull << 16);
+    p = {1u, 0u};
+    uint32_t *hi = w + 2 * (1u << 16);
+    for (uint32_t i = 0; i < (1u << 15); i++) { hi[2 * i] = p.x; hi[2 * i + 1] = p.y; p = h_pmul(p, g16); }
+}
+
 }  // namespace vx

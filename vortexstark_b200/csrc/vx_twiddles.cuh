@@ -45,6 +45,17 @@ cudaError_t build_ntt_tables(ecoset c, bool inverse, uint32_t *line, uint32_t *c
 // FRI fold twiddles of a domain of 2^k points: 2^(k-1) words.
 cudaError_t build_fold_twiddles(ecoset c, bool extract_y, uint32_t *out, cudaStream_t stream);
 
+// Same as build_ntt_tables / build_fold_twiddles with caller-provided
+// generator tables (no lazy allocation inside).
+cudaError_t build_ntt_tables_with(const GenTables &g, ecoset c, bool inverse, uint32_t *line, uint32_t *circle,
+                                  cudaStream_t stream);
+cudaError_t build_fold_twiddles_with(const GenTables &g, ecoset c, bool extract_y, uint32_t *out,
+                                     cudaStream_t stream);
+// Host computation of the generator tables: lo[i] = G^i (i < 2^16) followed
+// by hi[i] = G^(i << 16) (i < 2^15), as (x, y) word pairs: 196608 words.
+constexpr uint32_t kGenTableWords = 2u * ((1u << 16) + (1u << 15));
+void gen_tables_host(uint32_t *words);
+
 // Reference batch inverse: aligned chunks of 64, 0 -> 0, and a zero in a
 // chunk's first slot zeroes that whole chunk (batch_inverse.cu:8-41).
 cudaError_t batch_inverse(const uint32_t *in, uint32_t *out, uint64_t n, cudaStream_t stream);
