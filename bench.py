@@ -126,6 +126,62 @@ def cpu_baseline(log_n: int):
             "seconds": dt}
 
 
+def served_benchmark(seed: int, n_requests: int = 512):
+    """Mixed-size served stream (log_n in {16,...,24}, weights {.4,.25,.2,.1,.05},
+    Poisson arrivals): the continuous-batching engine against the plain
+    one-proof-at-a-time path on the same arrivals."""
+    import statistics as st
+
+    from vortexstark_b200 import prover
+    from vortexstark_b200.serving import ProofServer, plain_caches, poisson_arrivals, run_sequential, run_stream
+    from vortexstark_b200.workload import served_stream
+
+    reqs = served_stream(seed, n_requests)
+    sizes = sorted({r[0] for r in reqs})
+    # one-at-a-time service time per size (plain path: cached slot and pinned
+    # host buffer per size)
+    caches = plain_caches(sizes)
+    svc = {}
+    for ln in sizes:
+        prover.prove_cached_bytes(1, 2, caches[ln])
+        t = []
+        for i in range(5):
+            t0 = time.perf_counter()
+            prover.prove_cached_bytes(3 + i, 5, caches[ln])
+            t.append(time.perf_counter() - t0)
+        svc[ln] = st.median(t)
+    mean_svc = st.fmean(svc[r[0]] for r in reqs)
+    cap = 1.0 / mean_svc
+    plain_rate = 0.8 * cap
+    plain = run_sequential(reqs, poisson_arrivals(n_requests, plain_rate, seed + 1), caches=caches)
+    plain["rate"] = plain_rate
+    for c in caches.values():
+        c.close()
+    with ProofServer(budget_bytes=64 << 30, max_inflight=24) as srv:
+        counts = {16: 12, 18: 8, 20: 6, 22: 3, 24: 2}
+        for ln in sizes:
+            srv.prewarm(ln, counts.get(ln, 2))
+        run_stream(srv, reqs[:64], [0.0] * 64)  # warm-up
+        sweep = []
+        for mult in (0.8, 1.5, 2.0, 2.5, 3.0, 4.0, 6.0):
+            r, _ = run_stream(srv, reqs, poisson_arrivals(n_requests, mult * cap, seed + 2))
+            r["rate"] = mult * cap
+            sweep.append(r)
+        stats = srv.stats()
+    ok = [r for r in sweep if r["p99_ms"] <= plain["p99_ms"]]
+    best = max(ok, key=lambda r: r["proofs_per_s"]) if ok else None
+    return {
+        "requests": n_requests, "log_n_weights": {"16": 0.4, "18": 0.25, "20": 0.2, "22": 0.1, "24": 0.05},
+        "plain_service_ms": {str(k): 1e3 * v for k, v in svc.items()},
+        "plain_capacity_per_s": cap,
+        "plain": plain,
+        "served_sweep": sweep,
+        "served_best_at_plain_p99": best,
+        "speedup_at_equal_p99": (best["proofs_per_s"] / plain["proofs_per_s"]) if best else None,
+        "engine": {"max_inflight": 24, "slots": stats["slots"], "device_bytes": stats["bytes_used"]},
+    }
+
+
 def run_reference(args, rank: int):
     """CPU oracle arm: each step one proof of the workload (or a bounded
     sample of it), all host threads."""
@@ -179,6 +235,7 @@ def main():
     ap.add_argument("--impl", default="vortex", choices=["vortex", "reference"])
     ap.add_argument("--log-n", type=int, default=24)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-served", action="store_true", help="skip the mixed-size served stream")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -345,6 +402,9 @@ def main():
             "launches_per_proof": launches_per_proof,
             "clocks": clocks,
         }
+        if world == 1 and not args.no_served:
+            cache.close()
+            line["served"] = served_benchmark(SEED)
         if world == 1 and not args.no_cpu_baseline:
             cb = cpu_baseline(log_n)
             cb.pop("seconds", None)

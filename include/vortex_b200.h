@@ -262,7 +262,8 @@ int vx_probe_blake2s(uint32_t blocks, uint32_t threads, uint32_t iters, uint32_t
 int vx_prove_fib_noalloc(uint32_t a, uint32_t b, uint32_t log_n, uint32_t blowup_bits, uint32_t n_queries,
                          uint8_t *out, size_t cap, size_t *out_len);
 
-/* Free every cached slot and table on every device. */
+/* Free the slots cached by vx_prove_fib on every device; a size's shared
+ * tables are freed with the last slot (of any owner) that uses them. */
 void vx_release_all(void);
 
 #ifdef __cplusplus

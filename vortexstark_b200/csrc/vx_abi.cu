@@ -177,7 +177,7 @@ __global__ void tile_root_kernel(Src src, uint32_t *roots, uint32_t tile_log) {
 
 // Whole small tree of n <= 2048 leaves in one block (blake2s.cu:92-189).
 template <class Src>
-__global__ void small_tree_kernel(Src src, uint32_t *root, uint32_t n) {
+__global__ void abi_small_tree_kernel(Src src, uint32_t *root, uint32_t n) {
     extern __shared__ uint32_t sh[];
     src.init();
     uint32_t t = threadIdx.x;
@@ -489,7 +489,7 @@ void cuda_merkle_commit_small_soa4(const uint32_t *c0, const uint32_t *c1, const
                                    uint32_t *root, uint32_t n_leaves) {
     if (n_leaves < 2 || n_leaves > 2048) { set_last_error(VX_ERR_ARG, "cuda_merkle_commit_small_soa4: n_leaves must be in [2, 2048]"); return; }
     uint32_t thr = n_leaves / 2 < 32 ? 32 : n_leaves / 2;
-    small_tree_kernel<<<1, thr, 16 * n_leaves>>>(LeafSoA4{c0, c1, c2, c3}, root, n_leaves);
+    abi_small_tree_kernel<<<1, thr, 16 * n_leaves>>>(LeafSoA4{c0, c1, c2, c3}, root, n_leaves);
     VX_LAUNCH_CHECK();
 }
 

@@ -17,21 +17,43 @@ uint64_t tree_plan(uint32_t depth, uint32_t *pool, TreeLevels *lv) {
     lv->height[0] = 0;
     lv->hashes[0] = nullptr;
     uint64_t used = 0;
-    uint32_t h = 0;
-    while (h < depth) {
-        uint32_t k = depth - h < 4u ? depth - h : 4u;
-        h += k;
+    auto add = [&](uint32_t h) {
         lv->height[lv->n] = h;
         lv->hashes[lv->n] = pool ? pool + used : nullptr;
         used += 8ull << (depth - h);
         lv->n++;
+    };
+    uint32_t h = 0;
+    if (depth > kTopLog) {
+        // leaf kernel: 2^k leaves per thread, k = 1..4, at least 2^17 threads when possible
+        int k = (int)depth - 17;
+        k = k < 1 ? 1 : (k > 4 ? 4 : k);
+        h = (uint32_t)k;
+        add(h);
+        while (depth - h > kTopLog) { h += 4; add(h); }  // node kernels, 16 -> 1
     }
+    lv->top = lv->n;                                      // the single-block kernel from here on
+    while (h < depth) { h = h + 4 < depth ? h + 4 : depth; add(h); }
     return used;
 }
 
 uint64_t tree_pool_words(uint32_t depth) {
     TreeLevels lv;
     return tree_plan(depth, nullptr, &lv);
+}
+
+__global__ void __launch_bounds__(1024) top_tree_kernel(const uint32_t *in, uint32_t log_m, TreeLevels lv,
+                                                        ChanStep cs) {
+    extern __shared__ uint32_t sh[];
+    const uint32_t m = 1u << log_m;
+    for (uint32_t i = threadIdx.x; i < 8 * m; i += blockDim.x) sh[i] = in[i];
+    __syncthreads();
+    block_tree_up(sh, log_m, lv.height[lv.top - 1], lv, lv.top);
+    if (threadIdx.x == 0 && cs.ch) chan_commit(cs, sh);
+}
+
+cudaError_t small_tree_attr(const void *fn) {
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(32u << kTopLog));
 }
 
 }  // namespace vx

@@ -7,10 +7,11 @@
 // Work split: one thread hashes 2^kl consecutive leaves and folds them into
 // their subtree root with a small stack, so every lane stays busy and no data
 // moves between threads (kl = 4: 16 leaf + 15 node compressions per thread).
-// Upper levels are reduced the same way, 2^k hashes per thread.  The
-// resulting hash arrays at levels kl, kl + 4, ... are kept: they are the
-// tree's stored levels, from which any authentication path is rebuilt by
-// re-hashing one 16-node block per stored level.
+// Middle levels are reduced the same way, 16 hashes per thread; the last
+// <= 4096 hashes by one block in shared memory (see TreeLevels).  The hash
+// arrays at the planned heights are kept: they are the tree's stored levels,
+// from which any authentication path is rebuilt by re-hashing one block of
+// at most 16 nodes per stored level.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -141,92 +142,184 @@ __global__ void __launch_bounds__(256) leaf_subtree_kernel(Src src, uint32_t *ou
 
 __global__ void node_subtree_kernel(const uint32_t *in, uint32_t *out, uint64_t n_threads, uint32_t k);
 
+// Device transcript state (channel.rs:15-185), advanced by the kernel that
+// finishes a commitment.
+struct DevChannel {
+    uint32_t state[8];
+    uint32_t n_draws;
+    uint32_t err;  // nonzero if a bounded loop gave up
+};
+
+// squeeze = Blake2s(state || n_draws_le32 || 0x00), 37 bytes (channel.rs:174-182)
+__device__ __forceinline__ void chan_squeeze(const uint32_t state[8], uint32_t n_draws, uint32_t out[8]) {
+    uint32_t m[16];
+#pragma unroll
+    for (int i = 0; i < 8; i++) m[i] = state[i];
+    m[8] = n_draws;
+#pragma unroll
+    for (int i = 9; i < 16; i++) m[i] = 0u;
+    blake2s_block(out, m, 37u);
+}
+
+// draw_felt (channel.rs:65-84): squeeze until all 8 words < 2P, take words
+// 0..3 mod P.  Bounded: after 64 rejections (probability ~2^-1700) the
+// status word is set and zeros are returned.
+__device__ __forceinline__ void chan_draw_felt(DevChannel *ch, uint32_t out[4]) {
+    for (int it = 0; it < 64; it++) {
+        uint32_t w[8];
+        chan_squeeze(ch->state, ch->n_draws, w);
+        ch->n_draws++;
+        bool ok = true;
+#pragma unroll
+        for (int i = 0; i < 8; i++) ok &= w[i] < 2u * VX_P;
+        if (ok) {
+#pragma unroll
+            for (int i = 0; i < 4; i++) out[i] = w[i] % VX_P;
+            return;
+        }
+    }
+    ch->err = 1u;
+    out[0] = out[1] = out[2] = out[3] = 0u;
+}
+
+// After a commitment: mix_digest(root) (channel.rs:31-40), copy the root into
+// the proof, optionally draw the next challenge.
+struct ChanStep {
+    DevChannel *ch;       // null: no transcript step
+    uint32_t *proof_root; // 8 words in the proof
+    uint32_t *alpha_out;  // null: no draw
+};
+__device__ __forceinline__ void chan_commit(const ChanStep &c, const uint32_t root[8]) {
+    uint32_t m[16];
+#pragma unroll
+    for (int i = 0; i < 8; i++) { m[i] = c.ch->state[i]; m[8 + i] = root[i]; c.proof_root[i] = root[i]; }
+    uint32_t h[8];
+    blake2s_block(h, m, 64u);
+#pragma unroll
+    for (int i = 0; i < 8; i++) c.ch->state[i] = h[i];
+    c.ch->n_draws = 0;
+    if (c.alpha_out) chan_draw_felt(c.ch, c.alpha_out);
+}
+
 // Stored levels of one tree: level[0] is the leaf data (via its source),
-// level[i] (i >= 1) an array of hashes at tree height h[i]; h[n-1] = depth
-// holds the root.
+// level[i] (i >= 1) an array of hashes at tree height height[i];
+// height[n-1] = depth holds the root.
+//
+// Trees of depth <= 12 are built by one single-block kernel (leaves and all
+// levels in shared memory).  Deeper trees: one thread per 2^k-leaf subtree
+// (k = 1..4, chosen so at least 2^17 threads run), then 16 -> 1 node
+// kernels while a level has more than 4096 hashes, then one single-block
+// kernel reduces the last <= 4096 hashes to the root.  Every kernel that
+// finishes a tree also performs the transcript step of its commitment.
 struct TreeLevels {
     uint32_t n;            // number of stored levels including the leaf level
-    uint32_t height[12];   // height of each stored level (height[0] = 0)
+    uint32_t top;          // first level written by the single-block kernel
+    uint32_t height[12];
     uint32_t *hashes[12];  // hashes[0] unused
 };
 
-// Plan the stored levels of a tree of 2^depth leaves inside `pool`
-// (words); returns words used.
+constexpr uint32_t kTopLog = 12;  // single-block kernels handle <= 2^12 hashes
+
 uint64_t tree_plan(uint32_t depth, uint32_t *pool, TreeLevels *lv);
 uint64_t tree_pool_words(uint32_t depth);
 
-// Build all stored levels: leaf kernel then node kernels (no host sync).
+__global__ void node_subtree_kernel(const uint32_t *in, uint32_t *out, uint64_t n_threads, uint32_t k);
+
+// Reduce 2^log_m hashes held in shared memory (8 words each, at sh) up to the
+// root, storing the planned levels from lv.hashes[next]; height of the input
+// level is h0.  All threads of the block call it.
+__device__ __forceinline__ void block_tree_up(uint32_t *sh, uint32_t log_m, uint32_t h0, const TreeLevels &lv,
+                                              uint32_t next) {
+    uint32_t cnt = 1u << log_m, h = h0;
+    while (cnt > 1) {
+        uint32_t half = cnt >> 1;
+        for (uint32_t base = 0; base < half; base += blockDim.x) {
+            uint32_t t = base + threadIdx.x;
+            uint32_t hv[8];
+            bool act = t < half;
+            if (act) blake2s_node(hv, sh + 16 * t, sh + 16 * t + 8);
+            __syncthreads();
+            if (act)
+#pragma unroll
+                for (int w = 0; w < 8; w++) sh[8 * t + w] = hv[w];
+            __syncthreads();
+        }
+        cnt = half;
+        h++;
+        if (next < lv.n && lv.height[next] == h) {
+            uint32_t *dst = lv.hashes[next];
+            for (uint32_t i = threadIdx.x; i < 8 * cnt; i += blockDim.x) dst[i] = sh[i];
+            next++;
+        }
+    }
+    __syncthreads();
+}
+
+// Single-block kernel: the whole tree of a source with 2^depth <= 4096 leaves.
 template <class Src>
-cudaError_t tree_build(const Src &src, const TreeLevels &lv, cudaStream_t stream) {
-    if (lv.n < 2) return cudaSuccess;
+__global__ void __launch_bounds__(1024) small_tree_kernel(Src src, uint32_t depth, TreeLevels lv, ChanStep cs) {
+    extern __shared__ uint32_t sh[];
+    src.init();
+    const uint32_t m = 1u << depth;
+    for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+        uint32_t msg[16];
+#pragma unroll
+        for (int w = 0; w < 16; w++) msg[w] = 0u;
+        uint32_t nb = src.load(i, msg);
+        uint32_t h[8];
+        blake2s_block(h, msg, nb);
+#pragma unroll
+        for (int w = 0; w < 8; w++) sh[8 * i + w] = h[w];
+    }
+    __syncthreads();
+    block_tree_up(sh, depth, 0, lv, 1);
+    if (threadIdx.x == 0 && cs.ch) chan_commit(cs, sh);
+}
+
+// Single-block kernel: the last 2^log_m <= 4096 hashes of a tree to its root.
+__global__ void __launch_bounds__(1024) top_tree_kernel(const uint32_t *in, uint32_t log_m, TreeLevels lv,
+                                                        ChanStep cs);
+
+cudaError_t small_tree_attr(const void *fn);
+
+// Build all stored levels and the transcript step (no host sync).
+template <class Src>
+cudaError_t tree_build(const Src &src, const TreeLevels &lv, const ChanStep &cs, cudaStream_t stream) {
+    const uint32_t depth = lv.height[lv.n - 1];
+    if (depth <= kTopLog) {
+        static bool attr_done = false;  // one attribute call per template instance
+        if (!attr_done) {
+            cudaError_t e = small_tree_attr((const void *)small_tree_kernel<Src>);
+            if (e != cudaSuccess) return e;
+            attr_done = true;
+        }
+        uint32_t thr = (1u << depth) < 1024u ? ((1u << depth) < 32u ? 32u : (1u << depth)) : 1024u;
+        small_tree_kernel<Src><<<1, thr, (size_t)32 << depth, stream>>>(src, depth, lv, cs);
+        return cudaGetLastError();
+    }
     uint32_t kl = lv.height[1];
-    uint64_t n1 = 1ull << (lv.height[lv.n - 1] - kl);
+    uint64_t n1 = 1ull << (depth - kl);
     leaf_subtree_kernel<Src><<<(unsigned)((n1 + 255) / 256), 256, 0, stream>>>(src, lv.hashes[1], n1, kl);
-    for (uint32_t i = 2; i < lv.n; i++) {
+    for (uint32_t i = 2; i < lv.top; i++) {
         uint32_t k = lv.height[i] - lv.height[i - 1];
-        uint64_t nt = 1ull << (lv.height[lv.n - 1] - lv.height[i]);
+        uint64_t nt = 1ull << (depth - lv.height[i]);
         node_subtree_kernel<<<(unsigned)((nt + 255) / 256), 256, 0, stream>>>(lv.hashes[i - 1], lv.hashes[i], nt, k);
     }
+    static bool top_attr_done = false;
+    if (!top_attr_done) {
+        cudaError_t e = small_tree_attr((const void *)top_tree_kernel);
+        if (e != cudaSuccess) return e;
+        top_attr_done = true;
+    }
+    uint32_t log_m = depth - lv.height[lv.top - 1];
+    uint32_t thr = (1u << log_m) < 1024u ? ((1u << log_m) < 32u ? 32u : (1u << log_m)) : 1024u;
+    top_tree_kernel<<<1, thr, (size_t)32 << log_m, stream>>>(lv.hashes[lv.top - 1], log_m, lv, cs);
     return cudaGetLastError();
 }
 
-// Authentication paths, written straight into a proof in the reference's
-// byte layout (stark_cli.rs:1060-1090): for each query q, the path of
-// index[q] at paths + q*(1+8*depth) (depth word then siblings leaf->root)
-// and the path of index[q]^1 at spaths + q*(1+8*depth).
-template <class Src>
-__global__ void decommit_paths_kernel(Src src, TreeLevels lv, const uint32_t *qidx, uint32_t shift, uint32_t nq,
-                                      uint32_t *paths, uint32_t *spaths) {
-    uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t ng = lv.n - 1;
-    if (tid >= nq * ng) return;
-    uint32_t q = tid / ng, g = tid % ng;
-    uint32_t depth = lv.height[lv.n - 1];
-    uint64_t idx = (uint64_t)qidx[q] >> shift;
-    uint32_t lo = lv.height[g], k = lv.height[g + 1] - lo;
-    uint64_t node = idx >> lo;              // node index at height lo
-    uint64_t blk = node >> k;               // block of 2^k nodes
-    // all hashes of the block, level by level (16 + 8 + 4 + 2 + 1 max)
-    uint32_t nh[31][8];
-    const uint32_t K = 1u << k;
-    if (g == 0) {
-        src.init();
-        for (uint32_t j = 0; j < K; j++) {
-            uint32_t m[16];
-#pragma unroll
-            for (int w = 0; w < 16; w++) m[w] = 0u;
-            uint32_t nb = src.load((blk << k) + j, m);
-            blake2s_block(nh[j], m, nb);
-        }
-    } else {
-        const uint32_t *h = lv.hashes[g] + 8ull * (blk << k);
-        for (uint32_t j = 0; j < K; j++)
-#pragma unroll
-            for (int w = 0; w < 8; w++) nh[j][w] = h[8 * j + w];
-    }
-    uint32_t lvl_off = 0, cnt = K;
-    for (uint32_t d = 0; d < k; d++) {
-        uint32_t nxt = lvl_off + cnt;
-        for (uint32_t j = 0; j < cnt / 2; j++) blake2s_node(nh[nxt + j], nh[lvl_off + 2 * j], nh[lvl_off + 2 * j + 1]);
-        lvl_off = nxt;
-        cnt /= 2;
-    }
-    uint32_t *p = paths + (uint64_t)q * (1u + 8u * depth);
-    uint32_t *sp = spaths + (uint64_t)q * (1u + 8u * depth);
-    lvl_off = 0; cnt = K;
-    uint64_t local = node & (K - 1u);
-    for (uint32_t d = 0; d < k; d++) {
-        uint32_t hgt = lo + d;
-        const uint32_t *sib = nh[lvl_off + (uint32_t)(local ^ 1u)];
-        const uint32_t *self = nh[lvl_off + (uint32_t)local];
-#pragma unroll
-        for (int w = 0; w < 8; w++) {
-            p[1 + 8 * hgt + w] = sib[w];
-            sp[1 + 8 * hgt + w] = (hgt == 0) ? self[w] : sib[w];
-        }
-        lvl_off += cnt; cnt /= 2; local >>= 1;
-    }
-    if (g == 0) { p[0] = depth; sp[0] = depth; }
+// Kernels launched by tree_build for this plan.
+inline uint32_t tree_launches(const TreeLevels &lv) {
+    return lv.height[lv.n - 1] <= kTopLog ? 1u : lv.top;
 }
 
 }  // namespace vx

@@ -123,53 +123,6 @@ __global__ void fib_trace_kernel(uint32_t a, uint32_t b, const uint32_t *ab_dev,
     }
 }
 
-// ---- device transcript: channel.rs:31-119 ----
-__device__ void chan_squeeze(const uint32_t state[8], uint32_t n_draws, uint32_t out[8]) {
-    uint32_t m[16];
-#pragma unroll
-    for (int i = 0; i < 8; i++) m[i] = state[i];
-    m[8] = n_draws;
-#pragma unroll
-    for (int i = 9; i < 16; i++) m[i] = 0u;  // byte 36 is the 0x00 domain byte
-    blake2s_block(out, m, 37u);
-}
-
-// draw_felt (channel.rs:65-84): squeeze until all 8 words < 2P, take words
-// 0..3 mod P.  Bounded: after 64 rejections (probability ~2^-1700) the
-// status word is set and zeros are returned.
-__device__ void chan_draw_felt(DevChannel *ch, uint32_t out[4]) {
-    for (int it = 0; it < 64; it++) {
-        uint32_t w[8];
-        chan_squeeze(ch->state, ch->n_draws, w);
-        ch->n_draws++;
-        bool ok = true;
-#pragma unroll
-        for (int i = 0; i < 8; i++) ok &= w[i] < 2u * VX_P;
-        if (ok) {
-#pragma unroll
-            for (int i = 0; i < 4; i++) out[i] = w[i] % VX_P;
-            return;
-        }
-    }
-    ch->err = 1u;
-    out[0] = out[1] = out[2] = out[3] = 0u;
-}
-
-// mix_digest(root) (channel.rs:31-40), copy the root into the proof, then
-// optionally draw the next challenge.
-__global__ void chan_commit_kernel(DevChannel *ch, const uint32_t *root, uint32_t *proof_root, uint32_t *alpha_out) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    uint32_t m[16];
-#pragma unroll
-    for (int i = 0; i < 8; i++) { m[i] = ch->state[i]; m[8 + i] = root[i]; proof_root[i] = root[i]; }
-    uint32_t h[8];
-    blake2s_block(h, m, 64u);
-#pragma unroll
-    for (int i = 0; i < 8; i++) ch->state[i] = h[i];
-    ch->n_draws = 0;
-    if (alpha_out) chan_draw_felt(ch, alpha_out);
-}
-
 // mix_felts(last layer) (channel.rs:46-59) then n_queries x draw_number(N)
 // (channel.rs:93-97, prover.rs:1056-1059).  Draw j squeezes with
 // n_draws = j, so the draws run in parallel.
@@ -557,7 +510,6 @@ static int enqueue_stage(vx_prover *p, uint32_t stage, uint32_t a, uint32_t b, c
     const uint64_t n = 1ull << log_n, N = 1ull << le;
     uint32_t *proof = S.proof;
     LeafQuotient lq{S.eval, N - 1, S.alpha_q, {0, 0, 0, 0}};
-    auto tree_launches = [](const TreeLevels &lv) { return lv.n - 1; };
     auto ntt_launches = [](uint32_t layers) { return (layers + 10u) / 11u; };
     switch (stage) {
     case 0:
@@ -581,21 +533,18 @@ static int enqueue_stage(vx_prover *p, uint32_t stage, uint32_t a, uint32_t b, c
         break;
     }
     case 3:
-        VX_CUDA_TRY(tree_build(LeafM31{S.eval}, S.trace_lv, st));
-        chan_commit_kernel<<<1, 32, 0, st>>>(S.chan, S.trace_lv.hashes[S.trace_lv.n - 1], proof + L.troot, S.alpha_q);
-        *launches += tree_launches(S.trace_lv) + 1;
+        VX_CUDA_TRY(tree_build(LeafM31{S.eval}, S.trace_lv, ChanStep{S.chan, proof + L.troot, S.alpha_q}, st));
+        *launches += tree_launches(S.trace_lv);
         break;
     case 4:
-        VX_CUDA_TRY(tree_build(lq, S.quot_lv, st));
-        chan_commit_kernel<<<1, 32, 0, st>>>(S.chan, S.quot_lv.hashes[S.quot_lv.n - 1], proof + L.qroot, S.alpha_f);
-        *launches += tree_launches(S.quot_lv) + 1;
+        VX_CUDA_TRY(tree_build(lq, S.quot_lv, ChanStep{S.chan, proof + L.qroot, S.alpha_f}, st));
+        *launches += tree_launches(S.quot_lv);
         break;
     case 5: {
         LeafCircleFold cf{lq, T.fold_circle, S.alpha_f, S.fri[0][0], S.fri[0][1], S.fri[0][2], S.fri[0][3], {}};
-        VX_CUDA_TRY(tree_build(cf, S.fri_lv[0], st));
-        chan_commit_kernel<<<1, 32, 0, st>>>(S.chan, S.fri_lv[0].hashes[S.fri_lv[0].n - 1], proof + L.froots,
-                                             L.nfri > 1 ? S.alpha_f + 4 : nullptr);
-        *launches += tree_launches(S.fri_lv[0]) + 1;
+        VX_CUDA_TRY(tree_build(cf, S.fri_lv[0], ChanStep{S.chan, proof + L.froots, L.nfri > 1 ? S.alpha_f + 4 : nullptr},
+                               st));
+        *launches += tree_launches(S.fri_lv[0]);
         break;
     }
     case 6:
@@ -604,11 +553,11 @@ static int enqueue_stage(vx_prover *p, uint32_t stage, uint32_t a, uint32_t b, c
             LeafLineFold lf{S.fri[k - 1][0], S.fri[k - 1][1], S.fri[k - 1][2], S.fri[k - 1][3],
                             T.fold_line + T.fold_line_off[lsrc], S.alpha_f + 4 * k,
                             S.fri[k][0], S.fri[k][1], S.fri[k][2], S.fri[k][3], {}};
-            VX_CUDA_TRY(tree_build(lf, S.fri_lv[k], st));
-            chan_commit_kernel<<<1, 32, 0, st>>>(S.chan, S.fri_lv[k].hashes[S.fri_lv[k].n - 1],
-                                                 proof + L.froots + 8 * k,
-                                                 k + 1 < L.nfri ? S.alpha_f + 4 * (k + 1) : nullptr);
-            *launches += tree_launches(S.fri_lv[k]) + 1;
+            VX_CUDA_TRY(tree_build(lf, S.fri_lv[k],
+                                   ChanStep{S.chan, proof + L.froots + 8 * k,
+                                            k + 1 < L.nfri ? S.alpha_f + 4 * (k + 1) : nullptr},
+                                   st));
+            *launches += tree_launches(S.fri_lv[k]);
         }
         break;
     case 7: {
@@ -739,14 +688,10 @@ extern "C" int vx_prove_fib(uint32_t a, uint32_t b, uint32_t log_n, uint32_t blo
 }
 
 extern "C" void vx_release_all(void) {
-    {
-        std::lock_guard<std::mutex> lk(g_slot_mu);
-        for (auto &kv : g_slots) vx_prover_destroy(kv.second);
-        g_slots.clear();
-    }
-    std::lock_guard<std::mutex> lk(g_tab_mu);
-    for (auto &kv : g_tables) tables_destroy(kv.second.first);
-    g_tables.clear();
+    // the cached slots of vx_prove_fib; each size's tables go with their last slot
+    std::lock_guard<std::mutex> lk(g_slot_mu);
+    for (auto &kv : g_slots) vx_prover_destroy(kv.second);
+    g_slots.clear();
 }
 
 // ---------------------------------------------------------------------

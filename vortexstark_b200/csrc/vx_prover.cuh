@@ -24,12 +24,6 @@ struct ProofLayout {
 };
 void proof_layout(uint32_t log_n, uint32_t blowup, uint32_t nq, ProofLayout *L);
 
-// Fiat-Shamir transcript state on the device (channel.rs:15-185).
-struct DevChannel {
-    uint32_t state[8];
-    uint32_t n_draws;
-    uint32_t err;  // nonzero if a bounded loop gave up
-};
 
 // Read-only tables for one (log_n, blowup) on one device.
 struct SizeTables {

@@ -35,10 +35,11 @@ def prove_bytes(a: int, b: int, log_n: int, blowup_bits: int = BLOWUP_BITS, n_qu
     _check_inputs(a, b, log_n, blowup_bits)
     L = _lib.lib()
     size = proof_size(log_n, blowup_bits, n_queries)
-    buf = (C.c_uint8 * size)()
+    buf = bytearray(size)
     n = C.c_size_t()
-    _lib.check(L.vx_prove_fib(a, b, log_n, blowup_bits, n_queries, C.addressof(buf), size, C.byref(n)))
-    return bytes(buf[: n.value])
+    _lib.check(L.vx_prove_fib(a, b, log_n, blowup_bits, n_queries, C.addressof((C.c_uint8 * size).from_buffer(buf)),
+                              size, C.byref(n)))
+    return bytes(memoryview(buf)[: n.value])
 
 
 def prove(a: int, b: int, log_n: int) -> StarkProof:

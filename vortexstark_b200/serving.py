@@ -28,6 +28,8 @@ class ProofServer:
     def __init__(self, budget_bytes: int, max_inflight: int = 16, blowup_bits: int = 2, n_queries: int = 80,
                  use_graphs: bool = True):
         self._s = C.c_void_p()
+        self._blowup_bits, self._n_queries = blowup_bits, n_queries
+        self._log_n = {}
         _lib.check(_lib.lib().vx_server_create(int(budget_bytes), max_inflight, blowup_bits, n_queries,
                                                1 if use_graphs else 0, C.byref(self._s)))
 
@@ -35,7 +37,12 @@ class ProofServer:
         _lib.check(_lib.lib().vx_server_prewarm(self._s, log_n, count))
 
     def submit(self, tag: int, log_n: int, a: int, b: int) -> None:
-        _lib.check(_lib.lib().vx_server_submit(self._s, tag, log_n, a, b))
+        self._log_n[tag] = log_n  # before the engine can complete it
+        try:
+            _lib.check(_lib.lib().vx_server_submit(self._s, tag, log_n, a, b))
+        except Exception:
+            self._log_n.pop(tag, None)
+            raise
 
     def poll(self, max_items: int = 256, wait_ms: int = 0):
         buf = (Completion * max_items)()
@@ -47,14 +54,17 @@ class ProofServer:
         """Proof bytes of a finished request (and release them)."""
         L = _lib.lib()
         n = C.c_size_t()
+        log_n = self._log_n.pop(tag, None)
         if not keep:
             _lib.check(L.vx_server_result(self._s, tag, None, 0, C.byref(n)))
             return None
-        # size first is not available separately; proofs are at most a few MB
-        cap = 1 << 25
-        buf = (C.c_uint8 * cap)()
-        _lib.check(L.vx_server_result(self._s, tag, C.addressof(buf), cap, C.byref(n)))
-        return bytes(buf[: n.value])
+        if log_n is None:
+            raise _lib.VortexError(f"vx_server_result: unknown tag {tag}")
+        cap = int(L.vx_proof_size(log_n, self._blowup_bits, self._n_queries))
+        buf = bytearray(cap)
+        _lib.check(L.vx_server_result(self._s, tag, C.addressof((C.c_uint8 * cap).from_buffer(buf)), cap,
+                                      C.byref(n)))
+        return bytes(memoryview(buf)[: n.value])
 
     def stats(self) -> dict:
         ns, inf, pend = C.c_uint32(), C.c_uint32(), C.c_uint32()
@@ -140,13 +150,24 @@ def run_stream(server: ProofServer, requests, arrivals, keep_results: bool = Fal
     return s, results
 
 
+def plain_caches(sizes, blowup_bits: int = 2, n_queries: int = 80):
+    """One device-resident ProverCache (slot + pinned host buffer) per size:
+    the fastest one-proof-at-a-time path."""
+    from . import prover
+
+    return {ln: prover.ProverCache(ln, blowup_bits, n_queries) for ln in sorted(set(sizes))}
+
+
 def run_sequential(requests, arrivals, blowup_bits: int = 2, n_queries: int = 80, caches=None):
     """The plain one-proof-at-a-time GPU path on the same arrivals: requests in
     arrival order, each started when it has arrived and the previous proof has
-    finished (vx_prove_fib through one cached slot per size)."""
+    finished, through one cached slot with a pinned host buffer per size
+    (``prove_cached_bytes``)."""
     from . import prover
 
     n = len(requests)
+    if caches is None:
+        caches = plain_caches([r[0] for r in requests], blowup_bits, n_queries)
     lat = []
     t0 = time.perf_counter()
     for (log_n, a, b), at in zip(requests, arrivals):
@@ -154,6 +175,6 @@ def run_sequential(requests, arrivals, blowup_bits: int = 2, n_queries: int = 80
         if now < at:
             time.sleep(at - now)
         start_wait = t0 + at
-        prover.prove_bytes(a, b, log_n, blowup_bits, n_queries)
+        prover.prove_cached_bytes(a, b, caches[log_n])
         lat.append((time.perf_counter() - start_wait) * 1e3)
     return _summary(lat, time.perf_counter() - t0, n)
