@@ -246,6 +246,15 @@ void vx_server_destroy(vx_server *s);
  * roofline of the Merkle kernels. */
 int vx_probe_blake2s(uint32_t blocks, uint32_t threads, uint32_t iters, uint32_t *out, void *stream);
 
+/* Host-only description of the Merkle build plan for a tree of 2^depth
+ * leaves (1 <= depth <= 31); no device work.  heights[0..*n_levels) are the
+ * stored levels' heights (heights[0] = 0 is the leaf level, the last is
+ * depth); the reduce kernel starts from stored level *top (0: the leaves);
+ * *n_counters group counters, *pool_words device words for the stored levels
+ * and counters. */
+int vx_tree_plan(uint32_t depth, uint32_t heights[12], uint32_t *n_levels, uint32_t *top, uint32_t *n_counters,
+                 uint64_t *pool_words);
+
 /* Whole proof without any device allocation — no counterpart in the
  * reference.  For callers that may not allocate device memory: code inside a
  * stream capture or CUDA-graph construction, hosts whose device memory is

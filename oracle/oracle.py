@@ -61,6 +61,20 @@ def lib():
         L.vxo_qm31_mul.argtypes = [U32P, U32P, U32P]
         L.vxo_hash_leaf.argtypes = [U32P, C.c_uint32, U32P]
         L.vxo_hash_pair.argtypes = [U32P, U32P, U32P]
+        L.vxo_stwo_twiddles.argtypes = [C.c_uint32, C.c_int, U32P]
+        L.vxo_stwo_ntt_evaluate.argtypes = [U32P, U32P, C.c_uint32]
+        L.vxo_stwo_ntt_interpolate.argtypes = [U32P, U32P, C.c_uint32]
+        L.vxo_bit_reverse_qm31.argtypes = [U32P, U32P, C.c_uint32]
+        L.vxo_accumulate_lift.argtypes = [U32P, U32P, C.c_uint64, C.c_uint32]
+        L.vxo_pack_leaves.argtypes = [C.POINTER(U32P), C.POINTER(U32P), C.c_uint64]
+        L.vxo_stwo_fold_circle_twiddles.argtypes = [C.c_uint32, U32P]
+        L.vxo_lifted_size.argtypes = [C.c_uint32, U32P, C.c_uint32, C.c_uint32]
+        L.vxo_lifted_size.restype = C.c_size_t
+        L.vxo_commit_lifted.argtypes = [C.POINTER(U32P), U32P, C.c_uint32, C.c_uint32, C.c_uint32,
+                                        C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(C.c_size_t)]
+        L.vxo_commit_lifted.restype = C.c_int
+        L.vxo_lifted_lde.argtypes = [C.POINTER(U32P), U32P, C.c_uint32, C.c_uint32, C.POINTER(U32P)]
+        L.vxo_lifted_lde.restype = C.c_int
         for name in ("subgroup", "half_coset", "half_odds"):
             f = getattr(L, f"vxo_coset_{name}")
             f.argtypes = [C.c_uint32]
@@ -269,6 +283,99 @@ def qm31_mul(a, b) -> np.ndarray:
     out = np.zeros(4, np.uint32)
     lib().vxo_qm31_mul(_p(a), _p(b), _p(out))
     return out
+
+
+# ---- stwo-format NTT and the batched lifted commitment ----
+def stwo_twiddles(log_n: int, inverse: bool = False) -> np.ndarray:
+    out = np.zeros(1 << (log_n - 1), np.uint32)
+    lib().vxo_stwo_twiddles(log_n, int(inverse), _p(out))
+    return out
+
+
+def stwo_ntt_evaluate(data: np.ndarray, tw: np.ndarray | None = None) -> np.ndarray:
+    d = np.ascontiguousarray(data, dtype=np.uint32).copy()
+    k = int(len(d)).bit_length() - 1
+    t = stwo_twiddles(k) if tw is None else np.ascontiguousarray(tw, dtype=np.uint32)
+    lib().vxo_stwo_ntt_evaluate(_p(d), _p(t), k)
+    return d
+
+
+def stwo_ntt_interpolate(data: np.ndarray, itw: np.ndarray | None = None) -> np.ndarray:
+    d = np.ascontiguousarray(data, dtype=np.uint32).copy()
+    k = int(len(d)).bit_length() - 1
+    t = stwo_twiddles(k, True) if itw is None else np.ascontiguousarray(itw, dtype=np.uint32)
+    lib().vxo_stwo_ntt_interpolate(_p(d), _p(t), k)
+    return d
+
+
+def bit_reverse_qm31(data: np.ndarray) -> np.ndarray:
+    s = np.ascontiguousarray(data, dtype=np.uint32).reshape(-1)
+    d = np.zeros_like(s)
+    lib().vxo_bit_reverse_qm31(_p(s), _p(d), int(len(s) // 4).bit_length() - 1)
+    return d
+
+
+def accumulate_lift(col: np.ndarray, curr: np.ndarray) -> np.ndarray:
+    c = np.ascontiguousarray(col, dtype=np.uint32).copy()
+    s = np.ascontiguousarray(curr, dtype=np.uint32)
+    ratio = (int(len(c)).bit_length() - 1) - (int(len(s)).bit_length() - 1)
+    lib().vxo_accumulate_lift(_p(c), _p(s), len(c), ratio)
+    return c
+
+
+def pack_leaves(cols) -> np.ndarray:
+    cols = [np.ascontiguousarray(c, dtype=np.uint32) for c in cols]
+    n = len(cols[0])
+    out = np.zeros((64, n // 16), np.uint32)
+    ins = (U32P * 4)(*[_p(c) for c in cols])
+    outs = (U32P * 64)(*[_p(out[i]) for i in range(64)])
+    lib().vxo_pack_leaves(ins, outs, n)
+    return out
+
+
+def stwo_fold_circle_twiddles(log: int) -> np.ndarray:
+    out = np.zeros(1 << (log - 1), np.uint32)
+    lib().vxo_stwo_fold_circle_twiddles(log, _p(out))
+    return out
+
+
+def lifted_size(log_sizes, blowup_bits: int = 2, n_queries: int = 80) -> int:
+    logs = np.array(log_sizes, np.uint32)
+    return int(lib().vxo_lifted_size(len(logs), _p(logs), blowup_bits, n_queries))
+
+
+def commit_lifted(cols, blowup_bits: int = 2, n_queries: int = 80) -> bytes:
+    """The "LIFT" v1 words of the batched lifted commitment of `cols`
+    (sorted by ascending size)."""
+    cols = [np.ascontiguousarray(c, dtype=np.uint32) for c in cols]
+    logs = np.array([int(len(c)).bit_length() - 1 for c in cols], np.uint32)
+    arr = (U32P * len(cols))(*[_p(c) for c in cols])
+    out = C.POINTER(C.c_uint8)()
+    n = C.c_size_t()
+    L = lib()
+    rc = L.vxo_commit_lifted(arr, _p(logs), len(cols), blowup_bits, n_queries, C.byref(out), C.byref(n))
+    if rc:
+        raise ValueError(f"oracle commit_lifted rejected its arguments (rc={rc})")
+    try:
+        return C.string_at(out, n.value)
+    finally:
+        L.vxo_free(out)
+
+
+def lifted_lde(cols, blowup_bits: int = 2):
+    cols = [np.ascontiguousarray(c, dtype=np.uint32) for c in cols]
+    logs = np.array([int(len(c)).bit_length() - 1 for c in cols], np.uint32)
+    arr = (U32P * len(cols))(*[_p(c) for c in cols])
+    outs = (U32P * len(cols))()
+    L = lib()
+    if L.vxo_lifted_lde(arr, _p(logs), len(cols), blowup_bits, outs):
+        raise ValueError("oracle lifted_lde rejected its arguments")
+    res = []
+    for c, lg in enumerate(logs):
+        m = 1 << (int(lg) + blowup_bits)
+        res.append(np.ctypeslib.as_array(outs[c], shape=(m,)).copy())
+        L.vxo_free(outs[c])
+    return res
 
 
 # ---- the reference's own CUDA kernels (oracle/_ref/libvxref.so) ----

@@ -813,3 +813,284 @@ done:
     free(froots); free(fal); free(qi); free(fi);
     return rc;
 }
+
+/* ------------------------------------------------------------------ */
+/* stwo-format NTT: ntt.rs:300-379, circle_ntt_stwo.cu:15-404          */
+/* ------------------------------------------------------------------ */
+void vxo_stwo_twiddles(uint32_t log_n, int inverse, uint32_t *out) {
+    /* StwoNttCache::new (ntt.rs:300-341): levels of half_odds(log_n - 1),
+     * x-coordinates of each level's first half in bit-reversed order, the
+     * coset doubled between levels, then a 1; 2^(log_n-1) words. */
+    uint64_t tc = 1ull << (log_n - 1), w = 0;
+    vxo_coset cur = vxo_coset_half_odds(log_n - 1);
+    uint32_t levels = cur.log_size;
+    for (uint32_t lv = 0; lv < levels; lv++) {
+        uint64_t half = (1ull << cur.log_size) / 2;
+        uint32_t ll = 0;
+        while ((1ull << ll) < half) ll++;
+        vxo_point pt = cur.initial;
+        for (uint64_t j = 0; j < half; j++) {
+            uint64_t bj = ll ? brev(j, ll) : 0;
+            out[w + bj] = pt.x;
+            pt = vxo_point_mul(pt, cur.step);
+        }
+        w += half;
+        cur.initial = vxo_point_mul(cur.initial, cur.initial);
+        cur.step = vxo_point_mul(cur.step, cur.step);
+        cur.log_size--;
+    }
+    if (w < tc) out[w++] = 1u;
+    while (w < tc) out[w++] = 0u;
+    if (inverse) vxo_batch_inverse(out, out, (size_t)tc);
+}
+
+/* one butterfly layer of the stwo kernels (circle_ntt_stwo.cu:31-57) */
+static void stwo_line_layer(uint32_t *d, const uint32_t *tw, uint32_t layer_idx, uint64_t half_n, int fwd) {
+    #pragma omp parallel for schedule(static)
+    for (int64_t tid = 0; tid < (int64_t)half_n; tid++) {
+        uint64_t stride = 1ull << layer_idx, h = (uint64_t)tid >> layer_idx;
+        uint64_t i0 = (h << (layer_idx + 1)) + ((uint64_t)tid & (stride - 1)), i1 = i0 + stride;
+        uint32_t v0 = d[i0], v1 = d[i1], t = tw[h];
+        if (fwd) { uint32_t x = m_mul(v1, t); d[i1] = m_sub(v0, x); d[i0] = m_add(v0, x); }
+        else { d[i0] = m_add(v0, v1); d[i1] = m_mul(m_sub(v0, v1), t); }
+    }
+}
+/* circle layer: twiddle [y, -y, -x, x][tid % 4] of the pair
+ * (x, y) = (tw[2 (tid / 4)], tw[2 (tid / 4) + 1]) (circle_ntt_stwo.cu:202-249) */
+static void stwo_circle_layer(uint32_t *d, const uint32_t *tw, uint64_t half_n, int fwd) {
+    #pragma omp parallel for schedule(static)
+    for (int64_t tid = 0; tid < (int64_t)half_n; tid++) {
+        uint64_t pr = (uint64_t)tid / 4;
+        uint32_t x = tw[2 * pr], y = tw[2 * pr + 1], t;
+        switch (tid % 4) { case 0: t = y; break; case 1: t = m_neg(y); break; case 2: t = m_neg(x); break; default: t = x; }
+        uint32_t v0 = d[2 * tid], v1 = d[2 * tid + 1];
+        if (fwd) { uint32_t x2 = m_mul(v1, t); d[2 * tid + 1] = m_sub(v0, x2); d[2 * tid] = m_add(v0, x2); }
+        else { d[2 * tid] = m_add(v0, v1); d[2 * tid + 1] = m_mul(m_sub(v0, v1), t); }
+    }
+}
+void vxo_stwo_ntt_evaluate(uint32_t *d, const uint32_t *tw, uint32_t log_n) {
+    uint64_t half_n = 1ull << (log_n - 1);
+    uint32_t nl = log_n - 1;
+    for (int k = (int)nl - 1; k >= 0; k--)
+        stwo_line_layer(d, tw + (half_n - (1ull << (nl - (uint32_t)k))), (uint32_t)k + 1, half_n, 1);
+    stwo_circle_layer(d, tw, half_n, 1);
+}
+void vxo_stwo_ntt_interpolate(uint32_t *d, const uint32_t *itw, uint32_t log_n) {
+    uint64_t half_n = 1ull << (log_n - 1), n = 1ull << log_n;
+    uint32_t nl = log_n - 1;
+    stwo_circle_layer(d, itw, half_n, 0);
+    for (uint32_t k = 0; k < nl; k++) stwo_line_layer(d, itw + (half_n - (1ull << (nl - k))), k + 1, half_n, 0);
+    uint32_t e = (30u * log_n) % 31u, s = e ? (1u << e) : 1u;
+    #pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)n; i++) d[i] = m_mul(d[i], s);
+}
+
+void vxo_bit_reverse_qm31(const uint32_t *in, uint32_t *out, uint32_t log_n) {
+    uint64_t n = 1ull << log_n;
+    #pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)n; i++) {
+        uint64_t j = brev((uint64_t)i, log_n);
+        for (int c = 0; c < 4; c++) out[4 * j + c] = in[4 * i + c];
+    }
+}
+void vxo_accumulate_lift(uint32_t *col, const uint32_t *curr, uint64_t col_n, uint32_t log_ratio) {
+    #pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)col_n; i++) {
+        uint64_t src = (((uint64_t)i >> (log_ratio + 1)) << 1) | ((uint64_t)i & 1);
+        col[i] = m_add(col[i], curr[src]);
+    }
+}
+void vxo_pack_leaves(const uint32_t *const in[4], uint32_t *const out[64], uint64_t n) {
+    for (uint32_t c = 0; c < 4; c++)
+        for (uint64_t i = 0; i < n; i++) out[c * 16 + (i % 16)][i / 16] = in[c][i];
+}
+
+/* CircleDomain(half_odds(log-1)).at(k): the half coset for k < n/2, its
+ * conjugate after (ntt.rs:539, 585) */
+static vxo_point stwo_domain_at(uint32_t log, uint64_t k) {
+    vxo_coset hc = vxo_coset_half_odds(log - 1);
+    uint64_t half = 1ull << (log - 1);
+    if (k < half) return vxo_coset_at(&hc, k);
+    vxo_point p = vxo_coset_at(&hc, k - half);
+    p.y = m_neg(p.y);
+    return p;
+}
+void vxo_stwo_fold_circle_twiddles(uint32_t log, uint32_t *out) {
+    /* fri_ops.rs:44-66: 1 / y(domain.at(bit_reverse_index(i << 1, log))) */
+    int64_t half = (int64_t)1 << (log - 1);
+    #pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < half; i++) out[i] = vxo_m31_inv(stwo_domain_at(log, brev((uint64_t)i << 1, log)).y);
+}
+
+/* ------------------------------------------------------------------ */
+/* Batched lifted commitment ("LIFT" v1): stwo-format LDE of every     */
+/* column, one lifted tree, a random QM31 combination of the lifted    */
+/* columns, FRI with stwo twiddles, queries by draw_query_indices.     */
+/* ------------------------------------------------------------------ */
+static int lifted_check(const uint32_t *logs, uint32_t n_cols, uint32_t B, uint32_t nq) {
+    if (n_cols < 1 || n_cols > 64 || B < 1 || B > 4 || nq < 1 || nq > 1024) return 0;
+    for (uint32_t c = 0; c < n_cols; c++) {
+        if (logs[c] < 2 || logs[c] + B > 28) return 0;
+        if (c && logs[c] < logs[c - 1]) return 0;
+    }
+    return logs[n_cols - 1] + B >= 4;
+}
+size_t vxo_lifted_size(uint32_t n_cols, const uint32_t *logs, uint32_t B, uint32_t nq) {
+    if (!lifted_check(logs, n_cols, B, nq)) return 0;
+    uint32_t S = logs[n_cols - 1] + B, nfri = S - 3;
+    size_t w = 5 + n_cols + 8 + 8 + 1 + 8 * (size_t)nfri + 1 + 32 + 1 + nq;
+    w += 1 + 2 * (size_t)nq * n_cols + 2 * (size_t)nq * (1 + 8 * (size_t)S);
+    w += 1 + 2 * (size_t)nq * 4 + 2 * (size_t)nq * (1 + 8 * (size_t)S);
+    w += 1;
+    for (uint32_t k = 0; k < nfri; k++) w += 1 + 2 * (size_t)nq * 4 + 2 * (size_t)nq * (1 + 8 * (size_t)(S - 1 - k));
+    return 4 * w;
+}
+static inline uint64_t lift_row(uint64_t idx, uint32_t S, uint32_t L) {
+    return L == S ? idx : (((idx >> (S - L + 1)) << 1) | (idx & 1));
+}
+static void tree_from_leaves(vxo_tree *t, uint32_t *leaves, uint32_t log_n) {
+    t->log_n = log_n;
+    t->levels = (uint32_t **)calloc(log_n + 1, sizeof(uint32_t *));
+    t->levels[0] = leaves;
+    for (uint32_t l = 1; l <= log_n; l++) {
+        uint64_t m = (1ull << log_n) >> l;
+        uint32_t *up = (uint32_t *)malloc(m * 32), *dn = t->levels[l - 1];
+        #pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < (int64_t)m; i++) vxo_hash_pair(dn + 16 * i, dn + 16 * i + 8, up + 8 * i);
+        t->levels[l] = up;
+    }
+}
+static int lifted_impl(const uint32_t *const *cols, const uint32_t *logs, uint32_t n_cols, uint32_t B,
+                       uint32_t nq, uint8_t **out, size_t *out_len, uint32_t **lde_out) {
+    if (!lifted_check(logs, n_cols, B, nq)) return 1;
+    const uint32_t S = logs[n_cols - 1] + B, nfri = S - 3;
+    const uint64_t NS = 1ull << S;
+    /* 1. LDE of every column: stwo interpolate at 2^L, zero pad, stwo evaluate at 2^(L+B) */
+    uint32_t **lde = (uint32_t **)calloc(n_cols, sizeof(uint32_t *));
+    uint32_t *lde_logs = (uint32_t *)malloc(n_cols * 4);
+    for (uint32_t c = 0; c < n_cols; c++) {
+        uint32_t L = logs[c], LE = L + B;
+        lde_logs[c] = LE;
+        lde[c] = (uint32_t *)calloc(1ull << LE, 4);
+        memcpy(lde[c], cols[c], (1ull << L) * 4);
+        uint32_t *itw = (uint32_t *)malloc((1ull << (L - 1)) * 4);
+        vxo_stwo_twiddles(L, 1, itw);
+        vxo_stwo_ntt_interpolate(lde[c], itw, L);
+        free(itw);
+        uint32_t *tw = (uint32_t *)malloc((1ull << (LE - 1)) * 4);
+        vxo_stwo_twiddles(LE, 0, tw);
+        vxo_stwo_ntt_evaluate(lde[c], tw, LE);
+        free(tw);
+    }
+    /* 2. lifted tree */
+    uint32_t *leaves = (uint32_t *)malloc(NS * 32);
+    vxo_lifted_leaves((const uint32_t *const *)lde, lde_logs, n_cols, S, leaves);
+    vxo_tree t0;
+    tree_from_leaves(&t0, leaves, S);
+    uint32_t r0[8]; vxo_tree_root(&t0, r0);
+    vxo_channel ch; vxo_channel_init(&ch);
+    vxo_channel_mix_digest(&ch, r0);
+    uint32_t alpha[4]; vxo_channel_draw_felt(&ch, alpha);
+    /* 3. C = sum_c alpha^c * lift(lde_c) */
+    qm pw[64];
+    pw[0].v[0] = 1; pw[0].v[1] = pw[0].v[2] = pw[0].v[3] = 0;
+    qm al; memcpy(al.v, alpha, 16);
+    for (uint32_t c = 1; c < n_cols; c++) pw[c] = q_mul(pw[c - 1], al);
+    uint32_t *C[4];
+    for (int k = 0; k < 4; k++) C[k] = (uint32_t *)malloc(NS * 4);
+    #pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)NS; i++) {
+        qm acc = {{0, 0, 0, 0}};
+        for (uint32_t c = 0; c < n_cols; c++) acc = q_add(acc, q_mulm(pw[c], lde[c][lift_row((uint64_t)i, S, lde_logs[c])]));
+        for (int k = 0; k < 4; k++) C[k][i] = acc.v[k];
+    }
+    vxo_tree t1;
+    vxo_tree_build(&t1, (const uint32_t *const *)C, 4, S);
+    uint32_t r1[8]; vxo_tree_root(&t1, r1);
+    vxo_channel_mix_digest(&ch, r1);
+    /* 4. FRI: circle fold with the stwo twiddles, then line folds (fri_ops.rs) */
+    uint32_t **lay = (uint32_t **)calloc((size_t)nfri * 4, sizeof(uint32_t *));
+    vxo_tree *ft = (vxo_tree *)calloc(nfri, sizeof(vxo_tree));
+    uint32_t *froots = (uint32_t *)malloc((size_t)nfri * 32);
+    uint32_t fa[4], fa2[4];
+    vxo_channel_draw_felt(&ch, fa);
+    vxo_qm31_mul(fa, fa, fa2);
+    uint32_t *tw = (uint32_t *)malloc((NS / 2) * 4);
+    vxo_stwo_fold_circle_twiddles(S, tw);
+    for (int k = 0; k < 4; k++) lay[k] = (uint32_t *)calloc(NS / 2, 4);
+    vxo_fold_circle_into_line(lay, (const uint32_t *const *)C, tw, fa, fa2, NS / 2);
+    uint32_t cur = S - 1;
+    vxo_tree_build(&ft[0], (const uint32_t *const *)lay, 4, cur);
+    vxo_tree_root(&ft[0], froots);
+    vxo_channel_mix_digest(&ch, froots);
+    for (uint32_t k = 1; k < nfri; k++) {
+        uint32_t a2[4]; vxo_channel_draw_felt(&ch, a2);
+        vxo_coset dom = vxo_coset_half_odds(cur);
+        uint64_t half = 1ull << (cur - 1);
+        vxo_fold_twiddles(&dom, 0, tw);
+        for (int c = 0; c < 4; c++) lay[4 * k + c] = (uint32_t *)malloc(half * 4);
+        vxo_fold_line((const uint32_t *const *)(lay + 4 * (k - 1)), tw, a2, lay + 4 * k, half);
+        cur--;
+        vxo_tree_build(&ft[k], (const uint32_t *const *)(lay + 4 * k), 4, cur);
+        vxo_tree_root(&ft[k], froots + 8 * k);
+        vxo_channel_mix_digest(&ch, froots + 8 * k);
+    }
+    free(tw);
+    uint32_t last[32];
+    for (int i = 0; i < 8; i++) for (int c = 0; c < 4; c++) last[4 * i + c] = lay[4 * (nfri - 1) + c][i];
+    vxo_channel_mix_felts(&ch, last, 8);
+    uint32_t *qi = (uint32_t *)malloc(4 * (size_t)nq);
+    vxo_channel_draw_query_indices(&ch, S, nq, qi);
+    /* 5. bytes */
+    if (out) {
+        wbuf w = {NULL, 0, 0};
+        w.cap = vxo_lifted_size(n_cols, logs, B, nq); w.p = (uint8_t *)malloc(w.cap);
+        wr(&w, 0x5446494Cu); wr(&w, 1); wr(&w, n_cols); wr(&w, B); wr(&w, S);
+        wrs(&w, logs, n_cols);
+        wrs(&w, r0, 8); wrs(&w, r1, 8);
+        wr(&w, nfri); wrs(&w, froots, 8 * (size_t)nfri);
+        wr(&w, 8); wrs(&w, last, 32);
+        wr(&w, nq); wrs(&w, qi, nq);
+        uint64_t *idx = (uint64_t *)malloc(8 * (size_t)nq);
+        for (uint32_t j = 0; j < nq; j++) idx[j] = qi[j];
+        /* lifted tree: the row of every column at q and at q ^ 1, then paths */
+        wr(&w, nq);
+        for (int s = 0; s < 2; s++)
+            for (uint32_t j = 0; j < nq; j++)
+                for (uint32_t c = 0; c < n_cols; c++) wr(&w, lde[c][lift_row(idx[j] ^ (uint64_t)s, S, lde_logs[c])]);
+        uint32_t *path = (uint32_t *)malloc(((size_t)S + 1) * 32);
+        for (int s = 0; s < 2; s++)
+            for (uint32_t j = 0; j < nq; j++) {
+                vxo_tree_path(&t0, idx[j] ^ (uint64_t)s, path);
+                wr(&w, S);
+                wrs(&w, path, 8 * (size_t)S);
+            }
+        free(path);
+        write_decom(&w, &t1, (const uint32_t *const *)C, 4, idx, nq);
+        wr(&w, nfri);
+        for (uint32_t j = 0; j < nq; j++) idx[j] >>= 1;
+        for (uint32_t k = 0; k < nfri; k++) {
+            write_decom(&w, &ft[k], (const uint32_t *const *)(lay + 4 * k), 4, idx, nq);
+            for (uint32_t j = 0; j < nq; j++) idx[j] >>= 1;
+        }
+        free(idx);
+        *out = w.p; *out_len = w.n;
+    }
+    free(qi);
+    for (uint32_t k = 0; k < nfri; k++) { vxo_tree_free(&ft[k]); for (int c = 0; c < 4; c++) free(lay[4 * k + c]); }
+    free(ft); free(lay); free(froots);
+    vxo_tree_free(&t1); for (int k = 0; k < 4; k++) free(C[k]);
+    vxo_tree_free(&t0);
+    if (lde_out) for (uint32_t c = 0; c < n_cols; c++) lde_out[c] = lde[c];
+    else for (uint32_t c = 0; c < n_cols; c++) free(lde[c]);
+    free(lde); free(lde_logs);
+    return 0;
+}
+int vxo_commit_lifted(const uint32_t *const *cols, const uint32_t *log_sizes, uint32_t n_cols, uint32_t blowup,
+                      uint32_t n_queries, uint8_t **out, size_t *out_len) {
+    return lifted_impl(cols, log_sizes, n_cols, blowup, n_queries, out, out_len, NULL);
+}
+int vxo_lifted_lde(const uint32_t *const *cols, const uint32_t *log_sizes, uint32_t n_cols, uint32_t blowup,
+                   uint32_t **lde_out) {
+    return lifted_impl(cols, log_sizes, n_cols, blowup, 1, NULL, NULL, lde_out);
+}

@@ -121,6 +121,47 @@ int vxo_verify(const uint8_t *proof, size_t len, uint32_t blowup_bits, uint32_t 
  * root, fri roots (count = log_eval-3). */
 int vxo_prove_roots(uint32_t a, uint32_t b, uint32_t log_n, uint32_t blowup_bits,
                     uint32_t *trace_root, uint32_t *quotient_root, uint32_t *fri_roots);
+/* ---- stwo-format circle NTT (ntt.rs:300-379, circle_ntt_stwo.cu:15-404) ----
+ * Twiddles of CanonicCoset(log_n).circle_domain() as StwoNttCache::new builds
+ * them (ntt.rs:300-341): 2^(log_n-1) words, level j = x-coordinates of the
+ * first half of half_odds(log_n-1) doubled j times in bit-reversed order,
+ * then a 1.  inverse != 0: elementwise inverses.  log_n >= 2. */
+void vxo_stwo_twiddles(uint32_t log_n, int inverse, uint32_t *out);
+/* line layers k = log_n-2 .. 0 (table at 2^(log_n-1) - 2^(log_n-1-k)), then
+ * the circle layer [y, -y, -x, x] from the pairs of level 0 */
+void vxo_stwo_ntt_evaluate(uint32_t *d, const uint32_t *tw, uint32_t log_n);
+/* circle layer, line layers 0 .. log_n-2, then x 2^((30 log_n) mod 31) */
+void vxo_stwo_ntt_interpolate(uint32_t *d, const uint32_t *itw, uint32_t log_n);
+void vxo_bit_reverse_qm31(const uint32_t *in, uint32_t *out, uint32_t log_n);          /* bit_reverse_wide.cu:21-52 */
+void vxo_accumulate_lift(uint32_t *col, const uint32_t *curr, uint64_t col_n, uint32_t log_ratio); /* accumulate_lift.cu:16-31 */
+void vxo_pack_leaves(const uint32_t *const in[4], uint32_t *const out[64], uint64_t n); /* pack_leaves.cu:22-38 */
+/* circle-fold twiddles of CanonicCoset(log).circle_domain(), 2^(log-1)
+ * words: 1 / y(domain.at(bit_reverse_index(i << 1, log))) (fri_ops.rs:44-66).
+ * Line folds use vxo_fold_twiddles(half_odds(l), 0) (fri_ops.rs:68-92). */
+void vxo_stwo_fold_circle_twiddles(uint32_t log, uint32_t *out);
+
+/* ---- batched lifted commitment ("LIFT" v1, a synthetic transcript) ----
+ * Columns sorted by ascending log size L_c (2 <= L_c, L_c + blowup <= 28,
+ * 1..64 columns), values in stwo's bit-reversed circle-domain order.
+ *  1. LDE_c = stwo evaluate at 2^(L_c+B) of the zero-padded stwo interpolation;
+ *  2. one lifted Blake2s tree over all LDE_c (S = max L_c + B), root R0;
+ *  3. channel: mix(R0), alpha = draw_felt;
+ *  4. C[i] = sum_c alpha^c * LDE_c[lift_row(i)] (accumulate_lift.cu:26-31), QM31[2^S];
+ *  5. SoA4 tree over C, mix(R1), alpha_0; circle fold with the stwo twiddles,
+ *     then line folds down to 8 values, each layer committed and mixed, a
+ *     fresh alpha before every fold (the Fibonacci FRI of prover.rs:860-926);
+ *  6. mix_felts(last 8), draw_query_indices(S, n_queries) (channel.rs:102-116).
+ * Words: "LIFT", 1, n_cols, B, S, log sizes; R0; R1; nfri, FRI roots; 8, last
+ * layer; nq, queries; decommitments (n, values at q, values at q^1, paths of
+ * q, paths of q^1) of the lifted tree (a row = n_cols words), of C and of
+ * every FRI layer (at q >> (k+1)), as the KRAK layout orders them. */
+size_t vxo_lifted_size(uint32_t n_cols, const uint32_t *log_sizes, uint32_t blowup, uint32_t n_queries);
+int vxo_commit_lifted(const uint32_t *const *cols, const uint32_t *log_sizes, uint32_t n_cols, uint32_t blowup,
+                      uint32_t n_queries, uint8_t **out, size_t *out_len);
+/* The LDE columns of step 1 (malloc'd, free each with vxo_free). */
+int vxo_lifted_lde(const uint32_t *const *cols, const uint32_t *log_sizes, uint32_t n_cols, uint32_t blowup,
+                   uint32_t **lde_out);
+
 void vxo_free(void *p);
 void vxo_set_threads(int n);
 int vxo_get_threads(void);

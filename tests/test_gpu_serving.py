@@ -35,13 +35,32 @@ def test_mixed_stream_equals_alone(oracle):
 
 def test_tight_budget_queues_and_stays_exact():
     reqs = _stream(11, 16, [10, 12])
-    budget = 3 << 20  # room for about two slots of these sizes
+    # room for one slot of each size (slot buffers + device input words +
+    # the size's tables) and half a slot more: every other request queues
+    slot, tab = {}, {}
+    for ln in (10, 12):
+        c = prover.ProverCache(ln)
+        slot[ln], tab[ln] = c.slot_bytes() + 256, c.table_bytes()
+        c.close()
+    budget = sum(slot.values()) + sum(tab.values()) + min(slot.values()) // 2
     with ProofServer(budget_bytes=budget, max_inflight=4) as srv:
         summary, results = run_stream(srv, reqs, [0.0] * len(reqs), keep_results=True)
         st = srv.stats()
-    assert st["bytes_used"] <= budget and st["slots"] <= 3
+    assert st["bytes_used"] <= budget and st["slots"] == 2
     for i, (log_n, a, b) in enumerate(reqs):
         assert results[i] == prover.prove_bytes(a, b, log_n)
+
+
+def test_burst_while_slots_are_created():
+    # no prewarm: the engine creates slots (lock released) while the
+    # submitter keeps appending requests
+    reqs = _stream(17, 96, [8, 9, 10, 11])
+    with ProofServer(budget_bytes=4 << 30, max_inflight=16) as srv:
+        summary, results = run_stream(srv, reqs, [0.0] * len(reqs), keep_results=True)
+        st = srv.stats()
+    assert summary["n"] == len(reqs) and st["pending"] == 0 and st["inflight"] == 0
+    for i, (log_n, a, b) in enumerate(reqs):
+        assert results[i] == prover.prove_bytes(a, b, log_n), (i, log_n)
 
 
 def test_plain_launches_without_graphs():

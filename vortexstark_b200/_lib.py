@@ -75,6 +75,8 @@ _SIGS = {
     "vx_prover_stage_async": ([vp, u32, u32, u32, vp], C.c_int),
     "vx_prover_launches": ([vp], C.c_uint32),
     "vx_probe_blake2s": ([u32, u32, u32, vp, vp], C.c_int),
+    "vx_tree_plan": ([u32, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32), C.POINTER(u32),
+                      C.POINTER(C.c_uint64)], C.c_int),
     "vx_prover_proof_device": ([vp, C.POINTER(vp), C.POINTER(C.c_size_t)], C.c_int),
     "vx_prover_check": ([vp], C.c_int),
     "vx_prove_fib": ([u32, u32, u32, u32, u32, vp, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),

@@ -24,16 +24,31 @@ uint64_t tree_plan(uint32_t depth, uint32_t *pool, TreeLevels *lv) {
         lv->n++;
     };
     uint32_t h = 0;
-    if (depth > kTopLog) {
-        // leaf kernel: 2^k leaves per thread, k = 1..4, at least 2^17 threads when possible
+    lv->top = 0;
+    if (depth > 16) {
+        // leaf kernel: 2^k leaves per thread, k = 1..4, at least 2^16 threads
         int k = (int)depth - 17;
         k = k < 1 ? 1 : (k > 4 ? 4 : k);
         h = (uint32_t)k;
         add(h);
-        while (depth - h > kTopLog) { h += 4; add(h); }  // node kernels, 16 -> 1
+        while (depth - h > 20) { h += 4; add(h); }  // node kernels, 16 -> 1
+        lv->top = lv->n - 1;
     }
-    lv->top = lv->n;                                      // the single-block kernel from here on
+    // reduce stages of 8 levels from h: every 4th height is stored, so the
+    // stage boundaries h + 8j are stored levels
     while (h < depth) { h = h + 4 < depth ? h + 4 : depth; add(h); }
+    // one counter per group of every stage after the first
+    uint32_t u = depth - lv->height[lv->top];
+    uint32_t x = u - (u < kStageLog ? u : kStageLog);  // log2 of the first stage's chunks
+    uint64_t nc = 0;
+    while (x > 0) {
+        uint32_t cn = x < kStageLog ? x : kStageLog;
+        nc += 1ull << (x - cn);
+        x -= cn;
+    }
+    lv->n_cnt = (uint32_t)nc;
+    lv->cnt = (pool && nc) ? pool + used : nullptr;
+    used += nc;
     return used;
 }
 
@@ -42,18 +57,9 @@ uint64_t tree_pool_words(uint32_t depth) {
     return tree_plan(depth, nullptr, &lv);
 }
 
-__global__ void __launch_bounds__(1024) top_tree_kernel(const uint32_t *in, uint32_t log_m, TreeLevels lv,
-                                                        ChanStep cs) {
-    extern __shared__ uint32_t sh[];
-    const uint32_t m = 1u << log_m;
-    for (uint32_t i = threadIdx.x; i < 8 * m; i += blockDim.x) sh[i] = in[i];
-    __syncthreads();
-    block_tree_up(sh, log_m, lv.height[lv.top - 1], lv, lv.top);
-    if (threadIdx.x == 0 && cs.ch) chan_commit(cs, sh);
-}
-
-cudaError_t small_tree_attr(const void *fn) {
-    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(32u << kTopLog));
+cudaError_t tree_reset(const TreeLevels &lv, cudaStream_t stream) {
+    if (!lv.cnt || !lv.n_cnt) return cudaSuccess;
+    return cudaMemsetAsync(lv.cnt, 0, 4ull * lv.n_cnt, stream);
 }
 
 }  // namespace vx
@@ -81,5 +87,19 @@ extern "C" int vx_probe_blake2s(uint32_t blocks, uint32_t threads, uint32_t iter
     VX_CHECK_ARG(out != nullptr && blocks > 0 && threads > 0 && threads <= 256, "vx_probe_blake2s: bad launch shape");
     vx::blake2s_probe_kernel<<<blocks, threads, 0, (cudaStream_t)stream>>>(iters, out);
     VX_CUDA_TRY(cudaGetLastError());
+    return VX_OK;
+}
+
+extern "C" int vx_tree_plan(uint32_t depth, uint32_t heights[12], uint32_t *n_levels, uint32_t *top,
+                            uint32_t *n_counters, uint64_t *pool_words) {
+    VX_CHECK_ARG(depth >= 1 && depth <= 31, "vx_tree_plan: depth %u outside 1..31", depth);
+    VX_CHECK_ARG(heights && n_levels && top && n_counters && pool_words, "vx_tree_plan: null output");
+    vx::TreeLevels lv;
+    uint64_t w = vx::tree_plan(depth, nullptr, &lv);
+    for (uint32_t i = 0; i < 12; i++) heights[i] = i < lv.n ? lv.height[i] : 0u;
+    *n_levels = lv.n;
+    *top = lv.top;
+    *n_counters = lv.n_cnt;
+    *pool_words = w;
     return VX_OK;
 }

@@ -7,11 +7,12 @@
 // Work split: one thread hashes 2^kl consecutive leaves and folds them into
 // their subtree root with a small stack, so every lane stays busy and no data
 // moves between threads (kl = 4: 16 leaf + 15 node compressions per thread).
-// Middle levels are reduced the same way, 16 hashes per thread; the last
-// <= 4096 hashes by one block in shared memory (see TreeLevels).  The hash
-// arrays at the planned heights are kept: they are the tree's stored levels,
-// from which any authentication path is rebuilt by re-hashing one block of
-// at most 16 nodes per stored level.
+// Big middle levels are reduced the same way, 16 hashes per thread; the
+// levels above, where one compression per thread per level is what keeps the
+// chain short, by blocks in shared memory (see TreeLevels).  The hash arrays
+// at the planned heights are kept: they are the tree's stored levels, from
+// which any authentication path is rebuilt by re-hashing one block of at most
+// 16 nodes per stored level.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -203,123 +204,139 @@ __device__ __forceinline__ void chan_commit(const ChanStep &c, const uint32_t ro
 
 // Stored levels of one tree: level[0] is the leaf data (via its source),
 // level[i] (i >= 1) an array of hashes at tree height height[i];
-// height[n-1] = depth holds the root.
+// height[n-1] = depth holds the root.  Consecutive heights differ by 1..4,
+// so an authentication path is rebuilt from at most 16 nodes per level.
 //
-// Trees of depth <= 12 are built by one single-block kernel (leaves and all
-// levels in shared memory).  Deeper trees: one thread per 2^k-leaf subtree
-// (k = 1..4, chosen so at least 2^17 threads run), then 16 -> 1 node
-// kernels while a level has more than 4096 hashes, then one single-block
-// kernel reduces the last <= 4096 hashes to the root.  Every kernel that
-// finishes a tree also performs the transcript step of its commitment.
+// Build: trees of depth <= 16 go to one multi-block reduce launch straight
+// from the leaves.  Deeper trees: one thread per 2^k-leaf subtree (k = 1..4,
+// chosen so that at least 2^16 threads run), then 16 -> 1 node kernels while
+// a level has more than 2^20 hashes, then the reduce launch for the rest.
+// The reduce kernel works in stages of up to 8 levels: each block reduces 256
+// hashes in shared memory, one compression per thread per level; the last
+// block of every group of 256 (found with a counter, no waiting) carries on
+// with the group's roots, and the block that reaches the root performs the
+// transcript step of the commitment.
 struct TreeLevels {
     uint32_t n;            // number of stored levels including the leaf level
-    uint32_t top;          // first level written by the single-block kernel
+    uint32_t top;          // stored level the reduce kernel starts from (0: leaves)
     uint32_t height[12];
     uint32_t *hashes[12];  // hashes[0] unused
+    uint32_t *cnt;         // group counters of the reduce kernel (zero between launches)
+    uint32_t n_cnt;
 };
 
-constexpr uint32_t kTopLog = 12;  // single-block kernels handle <= 2^12 hashes
+constexpr uint32_t kStageLog = 8;        // levels per reduce stage (256 hashes per block)
+constexpr uint32_t kReduceThreads = 128;
 
 uint64_t tree_plan(uint32_t depth, uint32_t *pool, TreeLevels *lv);
 uint64_t tree_pool_words(uint32_t depth);
+// Zero the group counters of a freshly carved tree.
+cudaError_t tree_reset(const TreeLevels &lv, cudaStream_t stream);
 
-__global__ void node_subtree_kernel(const uint32_t *in, uint32_t *out, uint64_t n_threads, uint32_t k);
-
-// Reduce 2^log_m hashes held in shared memory (8 words each, at sh) up to the
-// root, storing the planned levels from lv.hashes[next]; height of the input
-// level is h0.  All threads of the block call it.
-__device__ __forceinline__ void block_tree_up(uint32_t *sh, uint32_t log_m, uint32_t h0, const TreeLevels &lv,
-                                              uint32_t next) {
-    uint32_t cnt = 1u << log_m, h = h0;
-    while (cnt > 1) {
-        uint32_t half = cnt >> 1;
-        for (uint32_t base = 0; base < half; base += blockDim.x) {
-            uint32_t t = base + threadIdx.x;
-            uint32_t hv[8];
-            bool act = t < half;
-            if (act) blake2s_node(hv, sh + 16 * t, sh + 16 * t + 8);
-            __syncthreads();
-            if (act)
-#pragma unroll
-                for (int w = 0; w < 8; w++) sh[8 * t + w] = hv[w];
-            __syncthreads();
-        }
-        cnt = half;
-        h++;
-        if (next < lv.n && lv.height[next] == h) {
-            uint32_t *dst = lv.hashes[next];
-            for (uint32_t i = threadIdx.x; i < 8 * cnt; i += blockDim.x) dst[i] = sh[i];
-            next++;
-        }
+// Write this block's part of level `h` if it is a stored level: cnt hashes
+// held at sh, chunk index `part` of that level.
+__device__ __forceinline__ void store_level_part(const TreeLevels &lv, uint32_t h, const uint32_t *sh, uint32_t cnt,
+                                                 uint64_t part) {
+    for (uint32_t i = 1; i < lv.n; i++) {
+        if (lv.height[i] != h) continue;
+        uint4 *dst = (uint4 *)(lv.hashes[i] + 8ull * part * cnt);
+        const uint4 *s4 = (const uint4 *)sh;
+        for (uint32_t j = threadIdx.x; j < 2u * cnt; j += blockDim.x) dst[j] = s4[j];
     }
-    __syncthreads();
 }
 
-// Single-block kernel: the whole tree of a source with 2^depth <= 4096 leaves.
 template <class Src>
-__global__ void __launch_bounds__(1024) small_tree_kernel(Src src, uint32_t depth, TreeLevels lv, ChanStep cs) {
-    extern __shared__ uint32_t sh[];
-    src.init();
-    const uint32_t m = 1u << depth;
-    for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
-        uint32_t msg[16];
+__global__ void __launch_bounds__(kReduceThreads) tree_reduce_kernel(Src src, TreeLevels lv, ChanStep cs) {
+    __shared__ __align__(16) uint32_t sh[8u << kStageLog];
+    __shared__ uint32_t is_last;
+    const uint32_t depth = lv.height[lv.n - 1];
+    uint32_t h = lv.height[lv.top];
+    const uint32_t *in = lv.top ? lv.hashes[lv.top] : nullptr;
+    uint64_t part = blockIdx.x;     // this block's chunk of the current stage
+    uint64_t chunks = gridDim.x;    // chunks of the current stage
+    uint32_t cbase = 0;             // first counter of the current stage
+    while (true) {
+        const uint32_t c = depth - h < kStageLog ? depth - h : kStageLog;
+        const uint32_t m = 1u << c;
+        if (!in) {
+            src.init();
+            for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+                uint32_t msg[16];
 #pragma unroll
-        for (int w = 0; w < 16; w++) msg[w] = 0u;
-        uint32_t nb = src.load(i, msg);
-        uint32_t h[8];
-        blake2s_block(h, msg, nb);
-#pragma unroll
-        for (int w = 0; w < 8; w++) sh[8 * i + w] = h[w];
+                for (int w = 0; w < 16; w++) msg[w] = 0u;
+                uint32_t nb = src.load((part << c) + i, msg);
+                uint32_t hv[8];
+                blake2s_block(hv, msg, nb);
+                store_hash(sh + 8 * i, hv);
+            }
+        } else {
+            const uint4 *p = (const uint4 *)(in + 8ull * (part << c));
+            for (uint32_t j = threadIdx.x; j < 2u * m; j += blockDim.x) ((uint4 *)sh)[j] = __ldcg(p + j);
+        }
+        __syncthreads();
+        for (uint32_t d = 0; d < c; d++) {
+            const uint32_t half = m >> (d + 1);
+            for (uint32_t base = 0; base < half; base += blockDim.x) {
+                const uint32_t t = base + threadIdx.x;
+                uint32_t hv[8];
+                const bool act = t < half;
+                if (act) blake2s_node(hv, sh + 16 * t, sh + 16 * t + 8);
+                __syncthreads();
+                if (act) store_hash(sh + 8 * t, hv);
+                __syncthreads();
+            }
+            store_level_part(lv, h + d + 1, sh, half, part);
+        }
+        h += c;
+        if (h == depth) {
+            if (threadIdx.x == 0 && cs.ch) chan_commit(cs, sh);
+            return;
+        }
+        // this chunk's root is in the stored level at height h; the last
+        // block of each group of 2^cn chunks reduces the group next
+        const uint32_t cn = depth - h < kStageLog ? depth - h : kStageLog;
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t *ctr = lv.cnt + cbase + (part >> cn);
+            uint32_t old = atomicAdd(ctr, 1u);
+            is_last = old == (1u << cn) - 1u;
+            if (is_last) *ctr = 0u;  // every block of the group has arrived: ready for the next launch
+        }
+        __syncthreads();
+        if (!is_last) return;
+        __threadfence();
+        cbase += (uint32_t)(chunks >> cn);
+        chunks >>= cn;
+        part >>= cn;
+        in = nullptr;
+        for (uint32_t i = 1; i < lv.n; i++)
+            if (lv.height[i] == h) in = lv.hashes[i];
     }
-    __syncthreads();
-    block_tree_up(sh, depth, 0, lv, 1);
-    if (threadIdx.x == 0 && cs.ch) chan_commit(cs, sh);
 }
-
-// Single-block kernel: the last 2^log_m <= 4096 hashes of a tree to its root.
-__global__ void __launch_bounds__(1024) top_tree_kernel(const uint32_t *in, uint32_t log_m, TreeLevels lv,
-                                                        ChanStep cs);
-
-cudaError_t small_tree_attr(const void *fn);
 
 // Build all stored levels and the transcript step (no host sync).
 template <class Src>
 cudaError_t tree_build(const Src &src, const TreeLevels &lv, const ChanStep &cs, cudaStream_t stream) {
     const uint32_t depth = lv.height[lv.n - 1];
-    if (depth <= kTopLog) {
-        static bool attr_done = false;  // one attribute call per template instance
-        if (!attr_done) {
-            cudaError_t e = small_tree_attr((const void *)small_tree_kernel<Src>);
-            if (e != cudaSuccess) return e;
-            attr_done = true;
+    if (lv.top > 0) {
+        uint32_t kl = lv.height[1];
+        uint64_t n1 = 1ull << (depth - kl);
+        leaf_subtree_kernel<Src><<<(unsigned)((n1 + 255) / 256), 256, 0, stream>>>(src, lv.hashes[1], n1, kl);
+        for (uint32_t i = 2; i <= lv.top; i++) {
+            uint32_t k = lv.height[i] - lv.height[i - 1];
+            uint64_t nt = 1ull << (depth - lv.height[i]);
+            node_subtree_kernel<<<(unsigned)((nt + 255) / 256), 256, 0, stream>>>(lv.hashes[i - 1], lv.hashes[i], nt,
+                                                                                  k);
         }
-        uint32_t thr = (1u << depth) < 1024u ? ((1u << depth) < 32u ? 32u : (1u << depth)) : 1024u;
-        small_tree_kernel<Src><<<1, thr, (size_t)32 << depth, stream>>>(src, depth, lv, cs);
-        return cudaGetLastError();
     }
-    uint32_t kl = lv.height[1];
-    uint64_t n1 = 1ull << (depth - kl);
-    leaf_subtree_kernel<Src><<<(unsigned)((n1 + 255) / 256), 256, 0, stream>>>(src, lv.hashes[1], n1, kl);
-    for (uint32_t i = 2; i < lv.top; i++) {
-        uint32_t k = lv.height[i] - lv.height[i - 1];
-        uint64_t nt = 1ull << (depth - lv.height[i]);
-        node_subtree_kernel<<<(unsigned)((nt + 255) / 256), 256, 0, stream>>>(lv.hashes[i - 1], lv.hashes[i], nt, k);
-    }
-    static bool top_attr_done = false;
-    if (!top_attr_done) {
-        cudaError_t e = small_tree_attr((const void *)top_tree_kernel);
-        if (e != cudaSuccess) return e;
-        top_attr_done = true;
-    }
-    uint32_t log_m = depth - lv.height[lv.top - 1];
-    uint32_t thr = (1u << log_m) < 1024u ? ((1u << log_m) < 32u ? 32u : (1u << log_m)) : 1024u;
-    top_tree_kernel<<<1, thr, (size_t)32 << log_m, stream>>>(lv.hashes[lv.top - 1], log_m, lv, cs);
+    const uint32_t u = depth - lv.height[lv.top];
+    const uint32_t c0 = u < kStageLog ? u : kStageLog;
+    tree_reduce_kernel<Src><<<(unsigned)(1ull << (u - c0)), kReduceThreads, 0, stream>>>(src, lv, cs);
     return cudaGetLastError();
 }
 
 // Kernels launched by tree_build for this plan.
-inline uint32_t tree_launches(const TreeLevels &lv) {
-    return lv.height[lv.n - 1] <= kTopLog ? 1u : lv.top;
-}
+inline uint32_t tree_launches(const TreeLevels &lv) { return lv.top + 1u; }
 
 }  // namespace vx

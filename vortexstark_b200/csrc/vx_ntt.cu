@@ -12,11 +12,19 @@ constexpr uint32_t kMaxTileWords = (1u << kMaxPassLayers) * 8u;
 
 struct PassOff { uint32_t v[32]; };
 
+// Circle-layer twiddle of butterfly h (see NttTables::circle_mode).
+__device__ __forceinline__ uint32_t circle_tw(const uint32_t *__restrict__ circle, uint32_t mode, uint64_t h) {
+    if (!mode) return __ldg(circle + h);
+    const uint32_t sub = (uint32_t)h & 3u;
+    const uint32_t v = __ldg(circle + 2 * (h >> 2) + (sub < 2u ? 1u : 0u));
+    return (sub == 1u || sub == 2u) ? msub(0u, v) : v;
+}
+
 template <bool FWD>
 __global__ void __launch_bounds__(512) ntt_pass_kernel(
     uint32_t *data, uint32_t *const *dev_cols, uint64_t col_stride,
     const uint32_t *src, uint64_t src_mask, uint64_t src_stride,
-    const uint32_t *__restrict__ line, const uint32_t *__restrict__ circle, PassOff off,
+    const uint32_t *__restrict__ line, const uint32_t *__restrict__ circle, uint32_t cmode, PassOff off,
     uint32_t s, uint32_t r, uint32_t wlog, uint32_t scale) {
     extern __shared__ uint32_t sm[];
     const uint32_t W = 1u << wlog;
@@ -39,13 +47,12 @@ __global__ void __launch_bounds__(512) ntt_pass_kernel(
     for (uint32_t jj = 0; jj < r; jj++) {
         const uint32_t j = FWD ? r - 1u - jj : jj;
         const uint32_t L = s + j;
-        const uint32_t *tw = L ? line + off.v[L - 1] : circle;
         for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) {
             uint32_t c = b & (W - 1u), p = b >> wlog;
             uint32_t row0 = ((p >> j) << (j + 1)) | (p & ((1u << j) - 1u));
             uint32_t e0 = (row0 << wlog) | c, e1 = e0 + (1u << (j + wlog));
             uint64_t h = (hb << (r - 1u - j)) | (uint64_t)(row0 >> (j + 1));
-            uint32_t t = __ldg(tw + h);
+            uint32_t t = L ? __ldg(line + off.v[L - 1] + h) : circle_tw(circle, cmode, h);
             uint32_t v0 = sm[e0], v1 = sm[e1];
             if (FWD) {
                 uint32_t tmp = mmul(v1, t);
@@ -101,6 +108,7 @@ struct Pass2Args {
     const uint32_t *src;
     uint64_t src_mask, src_stride;
     const uint32_t *line, *circle;
+    uint32_t cmode;
     PassOff off;
     uint32_t s;       // lowest layer of the pass
     uint32_t scale;   // 1 = none
@@ -195,8 +203,8 @@ __global__ void __launch_bounds__((1 << (R + WL)) / 16) ntt_pass2_kernel(Pass2Ar
             uint32_t j = R - 1 - lg;
             uint32_t t = f + 1u - (1u << lg);
             uint32_t L = s + j;
-            const uint32_t *tab = L ? p.line + p.off.v[L - 1] : p.circle;
-            tv[k] = __ldg(tab + ((hb << lg) | t));
+            uint64_t h = (hb << lg) | t;
+            tv[k] = L ? __ldg(p.line + p.off.v[L - 1] + h) : circle_tw(p.circle, p.cmode, h);
         }
     }
     uint32_t dv[DPT];
@@ -276,6 +284,16 @@ cudaError_t ensure_attrs() {
 
 }  // namespace
 
+NttTables stwo_tables(const uint32_t *tw, uint32_t log_n) {
+    NttTables t;
+    t.line = tw;
+    t.circle = tw;
+    t.circle_mode = 1u;
+    for (uint32_t l = 0; l < 32; l++)
+        t.off[l] = (l + 1 < log_n) ? (uint32_t)((1ull << (log_n - 1)) - (1ull << (log_n - 1 - l))) : 0u;
+    return t;
+}
+
 void ntt_table_offsets(uint32_t log_n, uint32_t off[32]) {
     uint64_t m = 1ull << log_n;
     for (uint32_t l = 0; l < 32; l++) off[l] = (l + 1 < log_n) ? (uint32_t)(m - (m >> l)) : 0u;
@@ -309,10 +327,10 @@ cudaError_t ntt_transform(uint32_t *data, uint32_t *const *dev_cols, uint64_t co
                           uint32_t log_n, const NttTables &tw, bool forward, const uint32_t *src,
                           uint32_t src_log, cudaStream_t stream) {
     if (log_n == 0 || n_cols == 0) return cudaSuccess;
-    if (src && !forward) return cudaErrorInvalidValue;
+    if (src && !forward && src_log != log_n) return cudaErrorInvalidValue;
     cudaError_t e = ensure_attrs();
     if (e != cudaSuccess) return e;
-    const uint32_t total = src ? src_log : log_n;  // layers applied: total-1 .. 0
+    const uint32_t total = (src && forward) ? src_log : log_n;  // layers applied: total-1 .. 0
     PassOff off;
     for (int i = 0; i < 32; i++) off.v[i] = tw.off[i];
     uint32_t e2 = (30u * log_n) % 31u;
@@ -325,10 +343,12 @@ cudaError_t ntt_transform(uint32_t *data, uint32_t *const *dev_cols, uint64_t co
         uint64_t tiles = (1ull << log_n) / tsz;
         if (forward)
             ntt_pass_kernel<true><<<dim3((unsigned)tiles, n_cols), 32, tsz * 4, stream>>>(
-                data, dev_cols, col_stride, src, mask, src_stride, tw.line, tw.circle, off, 0, r, wlog, 1u);
+                data, dev_cols, col_stride, src, mask, src_stride, tw.line, tw.circle, tw.circle_mode, off, 0, r, wlog,
+                1u);
         else
             ntt_pass_kernel<false><<<dim3((unsigned)tiles, n_cols), 32, tsz * 4, stream>>>(
-                data, dev_cols, col_stride, nullptr, mask, 0, tw.line, tw.circle, off, 0, r, wlog, inv_n);
+                data, dev_cols, col_stride, src, mask, src_stride, tw.line, tw.circle, tw.circle_mode, off, 0, r,
+                wlog, inv_n);
         return cudaGetLastError();
     }
     uint32_t ps[32], pr[32], pw[32];
@@ -339,7 +359,7 @@ cudaError_t ntt_transform(uint32_t *data, uint32_t *const *dev_cols, uint64_t co
         a.data = data; a.dev_cols = dev_cols; a.col_stride = col_stride;
         a.src = (q == 0 && src) ? src : nullptr;
         a.src_mask = mask; a.src_stride = src_stride;
-        a.line = tw.line; a.circle = tw.circle; a.off = off;
+        a.line = tw.line; a.circle = tw.circle; a.cmode = tw.circle_mode; a.off = off;
         a.s = ps[i];
         a.scale = (!forward && q == np - 1u) ? inv_n : 1u;
         uint64_t tiles = (1ull << log_n) >> (pr[i] + pw[i]);

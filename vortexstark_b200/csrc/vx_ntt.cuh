@@ -19,8 +19,10 @@ namespace vx {
 
 struct NttTables {
     const uint32_t *line;     // flat line twiddles, layer l at line + off[l]
-    const uint32_t *circle;   // circle twiddles (n/2)
+    const uint32_t *circle;   // circle twiddles (n/2), or the stwo pair table
     uint32_t off[32];
+    uint32_t circle_mode;     // 0: circle[h]; 1: stwo, [y, -y, -x, x][h & 3] of the
+                              // pair (circle[2 (h >> 2)], circle[2 (h >> 2) + 1])
 };
 
 // Enqueue a full forward (evaluate) or inverse (interpolate, with 1/n scale)
@@ -29,7 +31,8 @@ struct NttTables {
 // For the LDE, `src` (coefficients, 2^src_log words) replaces the first pass's
 // input: element g reads src[g & (2^src_log - 1)], and the top
 // (log_n - src_log) layers, which only replicate zero-padded coefficients,
-// are skipped.  src == nullptr means in place.
+// are skipped.  An inverse transform may read `src` (src_log = log_n) to
+// run out of place.  src == nullptr means in place.
 cudaError_t ntt_transform(uint32_t *data, uint32_t *const *dev_cols, uint64_t col_stride, uint32_t n_cols,
                           uint32_t log_n, const NttTables &tw, bool forward, const uint32_t *src,
                           uint32_t src_log, cudaStream_t stream);
@@ -42,5 +45,10 @@ cudaError_t ntt_single_layer(uint32_t *data, const uint32_t *tw, uint32_t layer_
 // (2^log_n - 1 words) and circle twiddles (2^(log_n-1) words); offsets of
 // line layer l are  sum_{j<l} 2^(log_n-1-j).
 void ntt_table_offsets(uint32_t log_n, uint32_t off[32]);
+
+// stwo layout (ntt.rs:300-341, circle_ntt_stwo.cu:268-404): one table of
+// 2^(log_n-1) words, line layer l at 2^(log_n-1) - 2^(log_n-1-l), and the
+// circle layer derived from layer 0's pairs.  Tables for ntt_transform.
+NttTables stwo_tables(const uint32_t *tw, uint32_t log_n);
 
 }  // namespace vx

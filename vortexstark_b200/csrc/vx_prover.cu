@@ -475,6 +475,10 @@ extern "C" int vx_prover_create(uint32_t log_n, uint32_t blowup_bits, uint32_t n
     proof_template(L, tmpl);
     cudaError_t e = cudaMemcpy(S.proof, tmpl.data(), L.words * 4, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(S.chan, 0, sizeof(DevChannel));
+    if (e == cudaSuccess) e = tree_reset(S.trace_lv, nullptr);
+    if (e == cudaSuccess) e = tree_reset(S.quot_lv, nullptr);
+    for (uint32_t k = 0; k < L.nfri && e == cudaSuccess; k++) e = tree_reset(S.fri_lv[k], nullptr);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(nullptr);  // slot streams may be non-blocking
     if (e != cudaSuccess) {
         vx_prover_destroy(p);
         set_last_error(VX_ERR_CUDA, "initialising proof slot: %s", cudaGetErrorString(e));
@@ -800,6 +804,11 @@ extern "C" int vx_prove_fib_noalloc(uint32_t a, uint32_t b, uint32_t log_n, uint
     VX_CHECK_ARG(w <= kNoAllocWords, "vx_prove_fib_noalloc: layout of %llu words exceeds the static scratch of %llu",
                  (unsigned long long)w, (unsigned long long)kNoAllocWords);
     cudaStream_t st = nullptr;  // legacy default stream
+    // the counters of the tree reduce kernels sit where another size's
+    // layout may have left data
+    VX_CUDA_TRY(tree_reset(S.trace_lv, st));
+    VX_CUDA_TRY(tree_reset(S.quot_lv, st));
+    for (uint32_t k = 0; k < L.nfri; k++) VX_CUDA_TRY(tree_reset(S.fri_lv[k], st));
     if (D.tab_log_n != log_n || D.tab_blowup != blowup_bits) {
         D.tab_log_n = D.tab_blowup = 0;
         VX_CUDA_TRY(build_ntt_tables_with(g, ecoset_half_coset(log_n), true, T.itw_line, T.itw_circle, st));

@@ -186,18 +186,23 @@ void worker_loop(vx_server *s) {
             s->inflight--;
             progress = true;
         }
-        // admit queued requests, oldest first, skipping ones that cannot start yet
-        for (auto it = s->pending.begin(); it != s->pending.end() && s->inflight < s->max_inflight;) {
+        // admit queued requests, oldest first, skipping ones that cannot start
+        // yet.  Requests are addressed by index: submitters append to
+        // `pending` while the lock is released for a slot creation (which
+        // invalidates deque iterators), and only this thread removes entries,
+        // so an index keeps naming the same request.
+        for (size_t qi = 0; qi < s->pending.size() && s->inflight < s->max_inflight;) {
+            const uint32_t log_n = s->pending[qi].log_n;
             Slot *free_slot = nullptr;
             for (Slot *sl : s->slots)
-                if (!sl->busy && sl->log_n == it->log_n) { free_slot = sl; break; }
+                if (!sl->busy && sl->log_n == log_n) { free_slot = sl; break; }
             if (!free_slot) {
                 size_t sb, tb;
-                size_estimate(s, it->log_n, &sb, &tb);
-                if (s->used + slot_cost(s, it->log_n, sb, tb) <= s->budget) {
+                size_estimate(s, log_n, &sb, &tb);
+                if (s->used + slot_cost(s, log_n, sb, tb) <= s->budget) {
                     Slot *sl = nullptr;
                     lk.unlock();
-                    int rc = slot_create(s, it->log_n, &sl);
+                    int rc = slot_create(s, log_n, &sl);
                     lk.lock();
                     if (rc) {
                         s->fatal = rc;
@@ -205,15 +210,15 @@ void worker_loop(vx_server *s) {
                         s->stop = true;
                         break;
                     }
-                    s->used += sl->footprint + (s->table_bytes.count(it->log_n) ? 0 : vx_prover_table_bytes(sl->p));
-                    s->table_bytes[it->log_n] = vx_prover_table_bytes(sl->p);
+                    s->used += sl->footprint + (s->table_bytes.count(log_n) ? 0 : vx_prover_table_bytes(sl->p));
+                    s->table_bytes[log_n] = vx_prover_table_bytes(sl->p);
                     s->slots.push_back(sl);
                     free_slot = sl;
                 }
             }
             if (free_slot) {
-                Request r = *it;
-                it = s->pending.erase(it);
+                Request r = s->pending[qi];
+                s->pending.erase(s->pending.begin() + (std::ptrdiff_t)qi);
                 if (launch(s, free_slot, r) != VX_OK) {
                     s->fatal = VX_ERR_CUDA;
                     s->fatal_msg = vx_last_error();
@@ -222,7 +227,7 @@ void worker_loop(vx_server *s) {
                 }
                 progress = true;
             } else {
-                ++it;
+                ++qi;
             }
         }
         if (!progress) {

@@ -35,6 +35,30 @@ __global__ void fold_sources_kernel(GenTables g, uint32_t e0, uint32_t k, int ex
     out[i] = extract_y ? p.y : p.x;
 }
 
+__global__ void stwo_table_kernel(GenTables g, uint32_t log_n, uint32_t *out, uint64_t size) {
+    uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= size) return;
+    if (w == size - 1) { out[w] = 1u; return; }
+    // level j = number of leading ones of w as a (log_n - 1)-bit number
+    const uint32_t bits = log_n - 1;
+    const uint32_t j = __clz(~((uint32_t)w << (32u - bits)));
+    const uint64_t off = size - (size >> j);
+    const uint32_t L = bits - j;                 // log size of the level's coset
+    const uint64_t p = w - off;                  // < 2^(L-1)
+    const uint64_t idx = L > 1 ? brev_bits((uint32_t)p, L - 1) : 0u;
+    const uint32_t e0 = ecoset_half_odds_e0(L);
+    const uint64_t e = (uint64_t)e0 + (idx << (31u - L));
+    out[w] = gpow(g, (uint32_t)(e & 0x7FFFFFFFull)).x;
+}
+
+__global__ void stwo_fold_circle_kernel(GenTables g, uint32_t log, uint32_t *out, uint64_t half) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= half) return;
+    const uint64_t idx = brev_bits((uint32_t)(i << 1), log);
+    const uint64_t e = (uint64_t)ecoset_half_odds_e0(log - 1) + (idx << (31u - (log - 1)));
+    out[i] = gpow(g, (uint32_t)(e & 0x7FFFFFFFull)).y;
+}
+
 // One thread per aligned chunk of 64, mirroring batch_inverse.cu:8-41
 // exactly, including the zero-first-slot behaviour.  Safe in place.
 __global__ void batch_inverse_kernel(const uint32_t *in, uint32_t *out, uint64_t n) {
@@ -164,6 +188,25 @@ void gen_tables_host(uint32_t *w) {
     p = {1u, 0u};
     uint32_t *hi = w + 2 * (1u << 16);
     for (uint32_t i = 0; i < (1u << 15); i++) { hi[2 * i] = p.x; hi[2 * i + 1] = p.y; p = h_pmul(p, g16); }
+}
+
+cudaError_t build_stwo_table_with(const GenTables &g, uint32_t log_n, bool inverse, uint32_t *out,
+                                  cudaStream_t stream) {
+    if (log_n < 2 || log_n > 29) return cudaErrorInvalidValue;
+    const uint64_t size = 1ull << (log_n - 1);
+    stwo_table_kernel<<<blocks_for(size, 256), 256, 0, stream>>>(g, log_n, out, size);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && inverse) e = batch_inverse(out, out, size, stream);
+    return e;
+}
+
+cudaError_t build_stwo_fold_circle_with(const GenTables &g, uint32_t log, uint32_t *out, cudaStream_t stream) {
+    if (log < 2 || log > 30) return cudaErrorInvalidValue;
+    const uint64_t half = 1ull << (log - 1);
+    stwo_fold_circle_kernel<<<blocks_for(half, 256), 256, 0, stream>>>(g, log, out, half);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = batch_inverse(out, out, half, stream);
+    return e;
 }
 
 }  // namespace vx

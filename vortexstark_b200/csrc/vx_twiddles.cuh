@@ -35,7 +35,8 @@ __device__ __forceinline__ cpoint gpow(const GenTables &t, uint32_t e) {
 struct ecoset { uint32_t e0, k; };
 inline ecoset ecoset_half_coset(uint32_t k) { return {k <= 30 ? (1u << (30 - k)) : 0u, k}; }
 inline ecoset ecoset_subgroup(uint32_t k) { return {0u, k}; }
-inline ecoset ecoset_half_odds(uint32_t k) { return {k >= 29 ? 1u : (1u << (29 - k)), k}; }
+__host__ __device__ inline uint32_t ecoset_half_odds_e0(uint32_t k) { return k >= 29 ? 1u : (1u << (29 - k)); }
+inline ecoset ecoset_half_odds(uint32_t k) { return {ecoset_half_odds_e0(k), k}; }
 inline ecoset ecoset_eval_domain(uint32_t k) { return k <= 30 ? ecoset_half_coset(k) : ecoset_subgroup(k); }
 
 // NTT tables in the reference layout (line: 2^k - 1 words, circle: 2^(k-1)).
@@ -55,6 +56,19 @@ cudaError_t build_fold_twiddles_with(const GenTables &g, ecoset c, bool extract_
 // by hi[i] = G^(i << 16) (i < 2^15), as (x, y) word pairs: 196608 words.
 constexpr uint32_t kGenTableWords = 2u * ((1u << 16) + (1u << 15));
 void gen_tables_host(uint32_t *words);
+
+// stwo NTT table of CanonicCoset(log_n)'s circle domain (ntt.rs:300-341):
+// 2^(log_n-1) words; level j (j <= log_n-2) at 2^(log_n-1) - 2^(log_n-1-j)
+// holds x(half_odds(L).at(brev(p, L-1))) for p < 2^(L-1), L = log_n-1-j
+// (half_odds(L) doubled is half_odds(L-1)); the last word is 1.  inverse:
+// elementwise inverses.  log_n in [2, 29].
+cudaError_t build_stwo_table_with(const GenTables &g, uint32_t log_n, bool inverse, uint32_t *out,
+                                  cudaStream_t stream);
+// stwo circle-fold twiddles of CanonicCoset(log)'s circle domain
+// (fri_ops.rs:44-66): out[i] = 1 / y(half_odds(log-1).at(brev(2i, log))),
+// 2^(log-1) words (brev(2i, log) < 2^(log-1), so the conjugate half of the
+// domain is never reached).
+cudaError_t build_stwo_fold_circle_with(const GenTables &g, uint32_t log, uint32_t *out, cudaStream_t stream);
 
 // Reference batch inverse: aligned chunks of 64, 0 -> 0, and a zero in a
 // chunk's first slot zeroes that whole chunk (batch_inverse.cu:8-41).
