@@ -157,13 +157,45 @@ void cuda_fold_circle_into_line_soa_forge(uint32_t *dst0, uint32_t *dst1, uint32
 /* replaces cuda_device_sync, fields.cu:44 */
 void cuda_device_sync(void);
 
+/* -- stwo-format path (crates/cuda-backend; ffi.rs:1182-1194) -- */
+/* replaces cuda_stwo_ntt_evaluate, circle_ntt_stwo.cu:268-330: bit-reversed
+ * circle FFT of n = 2^k (k >= 2) words in place with the stwo twiddle table
+ * (2^(k-1) words, StwoNttCache / CpuBackend::precompute_twiddles layout);
+ * synchronises the device before returning.  n = 2 (which the reference
+ * serves by reading past its 1-word table) is rejected. */
+void cuda_stwo_ntt_evaluate(uint32_t *data, const uint32_t *twiddles, uint32_t n);
+/* replaces cuda_stwo_ntt_interpolate, circle_ntt_stwo.cu:333-402 (inverse
+ * table; scales by 2^((30 k) mod 31) = 1/n) */
+void cuda_stwo_ntt_interpolate(uint32_t *data, const uint32_t *itwiddles, uint32_t n);
+/* replaces cuda_stwo_ntt_batch_evaluate, circle_ntt_stwo_batch.cu:239-306:
+ * n_cols columns of n words; col_ptrs is a HOST array of device pointers */
+void cuda_stwo_ntt_batch_evaluate(uint32_t *const *col_ptrs, const uint32_t *twiddles, uint32_t n,
+                                  uint32_t n_cols);
+/* replaces cuda_stwo_ntt_batch_interpolate, circle_ntt_stwo_batch.cu:308-374 */
+void cuda_stwo_ntt_batch_interpolate(uint32_t *const *col_ptrs, const uint32_t *itwiddles, uint32_t n,
+                                     uint32_t n_cols);
+/* replaces cuda_bit_reverse_qm31, bit_reverse_wide.cu:41-50: out[brev(i)] =
+ * in[i] for n = 2^log_n QM31 elements of 4 words, out of place (n must be
+ * 2^log_n; the reference writes out of bounds otherwise) */
+void cuda_bit_reverse_qm31(const uint32_t *in, uint32_t *out, uint32_t n, uint32_t log_n);
+/* replaces cuda_accumulate_lift, accumulate_lift.cu:35-44: col[i] +=
+ * curr[((i >> (log_ratio + 1)) << 1) | (i & 1)] for i < col_n */
+void cuda_accumulate_lift(uint32_t *col, const uint32_t *curr, uint32_t col_n, uint32_t log_ratio);
+/* replaces cuda_pack_leaves, pack_leaves.cu:44-52: output[c*16 + p][i] =
+ * input[c][16 i + p]; both pointer arrays are DEVICE arrays (4 and 64
+ * entries), N a multiple of 16 */
+void cuda_pack_leaves(const uint32_t *const *input_col_ptrs, uint32_t *const *output_col_ptrs, uint32_t n);
+
 /* ======================================================================
  * 2. Device-resident whole-proof path (new; no counterpart symbol in the
  *    reference — it replaces the body of prover.rs:264-619 / 627-1167)
  * ====================================================================== */
 
-/* Message describing the last failure on the calling host thread. */
+/* Message describing the last failure on the calling host thread (empty
+ * if none since the last vx_clear_error). */
 const char *vx_last_error(void);
+/* Forget the calling thread's recorded failure (before a void launcher). */
+void vx_clear_error(void);
 /* Library version, major * 10000 + minor * 100 + patch. */
 int vx_version(void);
 
@@ -209,6 +241,74 @@ int vx_prover_check(vx_prover *p);
  * tables are cached per size and reused by later calls. */
 int vx_prove_fib(uint32_t a, uint32_t b, uint32_t log_n, uint32_t blowup_bits, uint32_t n_queries, uint8_t *out,
                  size_t cap, size_t *out_len);
+
+/* ---- stwo twiddles built on the device (new) ----
+ * Replaces the CPU loops of StwoNttCache::new (ntt.rs:300-362) and the
+ * host-built uploads of CudaBackend's twiddle cache (poly_ops.rs:102-127):
+ * the 2^(log_n-1)-word table of CanonicCoset(log_n)'s circle domain
+ * (inverse != 0: elementwise inverses), 2 <= log_n <= 29, into device
+ * memory `out`, enqueued on `stream`. */
+int vx_stwo_twiddles(uint32_t log_n, int inverse, uint32_t *out, void *stream);
+/* Replaces get_or_compute_circle_fold_twiddles (fri_ops.rs:44-66): 2^(log-1)
+ * words 1 / y(CanonicCoset(log).circle_domain().at(brev(2i, log))). */
+int vx_stwo_fold_circle_twiddles(uint32_t log, uint32_t *out, void *stream);
+
+/* ---- batched lifted commitment of uneven-size columns (new) ----
+ * The workload of a multi-column stwo commitment on B200: columns sorted by
+ * ascending log size L_c (1..64 columns, 2 <= L_c, L_c + blowup <= 28), each
+ * given as 2^L_c M31 values in stwo's bit-reversed circle-domain order.
+ *  1. LDE_c = stwo evaluate at 2^(L_c + blowup) of the zero-padded stwo
+ *     interpolation (PolyOps::evaluate_polynomials, poly_ops.rs:676-770);
+ *  2. one lifted Blake2s tree over all LDE rows, S = max L_c + blowup
+ *     (MerkleOpsLifted::build_leaves, merkle_ops.rs:47-160); mix its root,
+ *     draw alpha;
+ *  3. C[i] = sum_c alpha^c * LDE_c[lift_row(i)] (accumulate_lift.cu:26-31),
+ *     committed as a 4-word-leaf tree; mix, draw the first fold challenge;
+ *  4. FRI: circle fold with the stwo twiddles, line folds down to 8 values,
+ *     each layer committed and mixed, a fresh challenge per fold
+ *     (fri_ops.rs:143-255, the Fibonacci FRI of prover.rs:860-926);
+ *  5. mix_felts(last layer); draw_query_indices(S, n_queries)
+ *     (channel.rs:102-116); open every tree at the queries.
+ * The result is "LIFT" v1 words: "LIFT", 1, n_cols, blowup, S, log sizes;
+ * the lifted root; C's root; nfri = S - 3, the FRI roots; 8, the last layer;
+ * n_queries, the query indices; then for the lifted tree (a row = n_cols
+ * words), for C and for every FRI layer k (at q >> (k + 1)): n, values at q,
+ * values at q ^ 1, paths of q, paths of q ^ 1 (each path: depth, 8 words per
+ * height), as the KRAK layout orders them.  The transcript is this
+ * library's own (the reference has no such proof); tests check it against a
+ * CPU restatement. */
+typedef struct vx_lifted vx_lifted;
+/* Bytes of the commitment for this shape, 0 if unsupported. */
+size_t vx_lifted_size(uint32_t n_cols, const uint32_t *log_sizes, uint32_t blowup_bits, uint32_t n_queries);
+/* Device buffers and tables for one shape. */
+int vx_lifted_create(uint32_t n_cols, const uint32_t *log_sizes, uint32_t blowup_bits, uint32_t n_queries,
+                     vx_lifted **out);
+void vx_lifted_destroy(vx_lifted *h);
+/* Device address of input column c (2^L_c words); write the column there,
+ * or use vx_lifted_upload_async. */
+int vx_lifted_column(vx_lifted *h, uint32_t c, uint32_t **dev_ptr);
+/* Copy host columns (host_cols[c] of 2^L_c words) to the device on `stream`. */
+int vx_lifted_upload_async(vx_lifted *h, const uint32_t *const *host_cols, void *stream);
+/* Stages: 0 LDE, 1 lifted tree, 2 combination + its tree, 3 circle fold,
+ * 4 line folds, 5 last layer + queries, 6 openings.  For per-stage timing. */
+#define VX_LIFT_STAGES 7
+int vx_lifted_stage_async(vx_lifted *h, uint32_t stage, void *stream);
+/* All stages on the device-resident columns, no host synchronisation. */
+int vx_lifted_commit_async(vx_lifted *h, void *stream);
+/* The same schedule as one CUDA graph, captured on the first call. */
+int vx_lifted_commit_graph(vx_lifted *h, void *stream);
+/* Copy the commitment words to host memory `dst` (vx_lifted_size bytes). */
+int vx_lifted_fetch_async(vx_lifted *h, void *dst, void *stream);
+/* Device status word, after the stream has drained. */
+int vx_lifted_check(vx_lifted *h);
+/* Kernels of the last whole commitment; device bytes held. */
+uint32_t vx_lifted_launches(const vx_lifted *h);
+size_t vx_lifted_device_bytes(const vx_lifted *h);
+/* Synchronous convenience: host columns in, commitment words out; one
+ * instance per shape is cached (vx_lifted_release_all frees them). */
+int vx_commit_lifted(const uint32_t *const *host_cols, const uint32_t *log_sizes, uint32_t n_cols,
+                     uint32_t blowup_bits, uint32_t n_queries, uint8_t *out, size_t cap, size_t *out_len);
+void vx_lifted_release_all(void);
 
 /* ---- serving: continuous batching of mixed-size proof requests (new) ----
  * A dispatcher thread admits queued requests as proof slots of their size

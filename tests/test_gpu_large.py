@@ -37,3 +37,15 @@ def test_max_size_proof_verifies(oracle, log_n, blowup):
     again = prover.prove_bytes(a, b, log_n, blowup)
     assert hashlib.sha256(again).digest() == hashlib.sha256(blob).digest()
     _free()
+
+
+def test_lifted_commitment_full_shape_matches_oracle(oracle):
+    """The batched workload at its full size: 34 columns (8 x 2^16,
+    16 x 2^18, 10 x 2^20), blowup 4, 80 queries, S = 22."""
+    import bench
+    from vortexstark_b200.lifted import commit_lifted, verify_lifted
+
+    cols = bench.lifted_workload(bench.SEED)
+    got = commit_lifted(cols, 2, 80)
+    assert got == oracle.commit_lifted(cols, 2, 80)
+    verify_lifted(got, 80)

@@ -62,6 +62,14 @@ _SIGS = {
     "cuda_fold_line_soa_forge": [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, u32],
     "cuda_fold_circle_into_line_soa_forge": [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, u32],
     "cuda_device_sync": [],
+    # stwo-format path
+    "cuda_stwo_ntt_evaluate": [vp, vp, u32],
+    "cuda_stwo_ntt_interpolate": [vp, vp, u32],
+    "cuda_stwo_ntt_batch_evaluate": [vp, vp, u32, u32],
+    "cuda_stwo_ntt_batch_interpolate": [vp, vp, u32, u32],
+    "cuda_bit_reverse_qm31": [vp, vp, u32, u32],
+    "cuda_accumulate_lift": [vp, vp, u32, u32],
+    "cuda_pack_leaves": [vp, vp, u32],
     # vx_ API
     "vx_last_error": ([], C.c_char_p),
     "vx_version": ([], C.c_int),
@@ -89,6 +97,23 @@ _SIGS = {
     "vx_server_stats": ([vp, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32), C.POINTER(C.c_size_t)], C.c_int),
     "vx_server_destroy": [vp],
     "vx_release_all": [],
+    "vx_clear_error": [],
+    "vx_stwo_twiddles": ([u32, C.c_int, vp, vp], C.c_int),
+    "vx_stwo_fold_circle_twiddles": ([u32, vp, vp], C.c_int),
+    "vx_lifted_size": ([u32, vp, u32, u32], C.c_size_t),
+    "vx_lifted_create": ([u32, vp, u32, u32, C.POINTER(vp)], C.c_int),
+    "vx_lifted_destroy": [vp],
+    "vx_lifted_column": ([vp, u32, C.POINTER(vp)], C.c_int),
+    "vx_lifted_upload_async": ([vp, vp, vp], C.c_int),
+    "vx_lifted_stage_async": ([vp, u32, vp], C.c_int),
+    "vx_lifted_commit_async": ([vp, vp], C.c_int),
+    "vx_lifted_commit_graph": ([vp, vp], C.c_int),
+    "vx_lifted_fetch_async": ([vp, vp, vp], C.c_int),
+    "vx_lifted_check": ([vp], C.c_int),
+    "vx_lifted_launches": ([vp], C.c_uint32),
+    "vx_lifted_device_bytes": ([vp], C.c_size_t),
+    "vx_commit_lifted": ([vp, vp, u32, u32, u32, vp, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
+    "vx_lifted_release_all": [],
 }
 
 _lib = None
@@ -130,6 +155,18 @@ def lib() -> C.CDLL:
                 f.argtypes, f.restype = sig, None
         _lib = L
     return _lib
+
+
+def clear_error() -> None:
+    lib().vx_clear_error()
+
+
+def raise_if_error() -> None:
+    """After a void (reference-style) launcher: raise what it recorded."""
+    msg = (lib().vx_last_error() or b"").decode()
+    if msg:
+        lib().vx_clear_error()
+        raise VortexError(VX_ERR_CUDA, msg)
 
 
 def check(rc: int) -> None:

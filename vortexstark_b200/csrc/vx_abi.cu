@@ -314,6 +314,7 @@ using namespace vx;
 extern "C" {
 
 const char *vx_last_error(void) { return t_err.c_str(); }
+void vx_clear_error(void) { t_err.clear(); }
 int vx_version(void) { return 100; }
 
 // ---------------- NTT ----------------

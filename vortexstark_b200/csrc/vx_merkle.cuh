@@ -15,6 +15,7 @@
 // 16 nodes per stored level.
 #pragma once
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 #include "vx_blake2s.cuh"
@@ -72,6 +73,59 @@ struct LeafQuotient {
     }
 };
 
+// A leaf source either fills one message block (load: m[] pre-zeroed, returns
+// the byte length) or, when its message spans several blocks, hashes the
+// leaf itself (digest).
+template <class Src, class = void>
+struct is_wide_leaf : std::false_type {};
+template <class Src>
+struct is_wide_leaf<Src, std::void_t<decltype(&Src::digest)>> : std::true_type {};
+
+template <class Src>
+__device__ __forceinline__ void leaf_digest(const Src &src, uint64_t i, uint32_t h[8]) {
+    if constexpr (is_wide_leaf<Src>::value) {
+        src.digest(i, h);
+    } else {
+        uint32_t m[16];
+#pragma unroll
+        for (int w = 0; w < 16; w++) m[w] = 0u;
+        uint32_t nb = src.load(i, m);
+        blake2s_block(h, m, nb);
+    }
+}
+
+// Lifted multi-size leaf (merkle_leaves_lifted.cu:25-98): the row of every
+// column, columns in ascending size, column c of 2^L rows read at
+// ((idx >> (S - L + 1)) << 1) | (idx & 1) (idx itself when L = S); one
+// Blake2s over all n_cols words, every full block but the last compressed
+// as non-final.
+constexpr uint32_t kMaxLiftCols = 64;
+struct LeafLifted {
+    const uint32_t *col[kMaxLiftCols];
+    uint32_t shift[kMaxLiftCols];  // S - L + 1, or 0 when L = S
+    uint32_t n_cols;
+    __device__ __forceinline__ void init() {}
+    __device__ __forceinline__ uint32_t word(uint32_t c, uint64_t idx) const {
+        const uint32_t sh = shift[c];
+        const uint64_t row = sh ? (((idx >> sh) << 1) | (idx & 1ull)) : idx;
+        return __ldg(col[c] + row);
+    }
+    __device__ __forceinline__ void digest(uint64_t idx, uint32_t h[8]) const {
+        blake2s_init(h);
+        const uint32_t nblk = n_cols ? (n_cols + 15u) / 16u : 1u;
+        for (uint32_t b = 0; b < nblk; b++) {
+            uint32_t m[16];
+#pragma unroll
+            for (uint32_t w = 0; w < 16; w++) {
+                const uint32_t c = 16u * b + w;
+                m[w] = c < n_cols ? word(c, idx) : 0u;
+            }
+            const bool last = b + 1 == nblk;
+            blake2s_compress(h, m, last ? 4u * n_cols : 64u * (b + 1), last);
+        }
+    }
+};
+
 // Fold a subtree of 2^kl leaves starting at `base` into its root.
 template <class Src>
 __device__ __forceinline__ void subtree_root(const Src &src, uint64_t base, uint32_t kl, uint32_t root[8]) {
@@ -79,12 +133,8 @@ __device__ __forceinline__ void subtree_root(const Src &src, uint64_t base, uint
     uint32_t sp = 0;
     const uint32_t K = 1u << kl;
     for (uint32_t j = 0; j < K; j++) {
-        uint32_t m[16];
-#pragma unroll
-        for (int w = 0; w < 16; w++) m[w] = 0u;
-        uint32_t nb = src.load(base + j, m);
         uint32_t h[8];
-        blake2s_block(h, m, nb);
+        leaf_digest(src, base + j, h);
         for (uint32_t jj = j; jj & 1u; jj >>= 1) {
             --sp;
             uint32_t mm[16];
@@ -261,12 +311,8 @@ __global__ void __launch_bounds__(kReduceThreads) tree_reduce_kernel(Src src, Tr
         if (!in) {
             src.init();
             for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
-                uint32_t msg[16];
-#pragma unroll
-                for (int w = 0; w < 16; w++) msg[w] = 0u;
-                uint32_t nb = src.load((part << c) + i, msg);
                 uint32_t hv[8];
-                blake2s_block(hv, msg, nb);
+                leaf_digest(src, (part << c) + i, hv);
                 store_hash(sh + 8 * i, hv);
             }
         } else {

@@ -323,6 +323,13 @@ static uint32_t plan_passes(uint32_t total, uint32_t ps[32], uint32_t pr[32], ui
     return np;
 }
 
+uint32_t ntt_pass_count(uint32_t layers) {
+    if (layers == 0) return 0;
+    if (layers < 4) return 1;
+    uint32_t ps[32], pr[32], pw[32];
+    return plan_passes(layers, ps, pr, pw);
+}
+
 cudaError_t ntt_transform(uint32_t *data, uint32_t *const *dev_cols, uint64_t col_stride, uint32_t n_cols,
                           uint32_t log_n, const NttTables &tw, bool forward, const uint32_t *src,
                           uint32_t src_log, cudaStream_t stream) {

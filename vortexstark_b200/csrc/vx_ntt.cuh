@@ -37,6 +37,9 @@ cudaError_t ntt_transform(uint32_t *data, uint32_t *const *dev_cols, uint64_t co
                           uint32_t log_n, const NttTables &tw, bool forward, const uint32_t *src,
                           uint32_t src_log, cudaStream_t stream);
 
+// Kernel launches of a transform that applies `layers` layers.
+uint32_t ntt_pass_count(uint32_t layers);
+
 // One butterfly layer over the whole array (reference cuda_circle_ntt_layer).
 cudaError_t ntt_single_layer(uint32_t *data, const uint32_t *tw, uint32_t layer_idx, uint32_t log_n, bool forward,
                              cudaStream_t stream);

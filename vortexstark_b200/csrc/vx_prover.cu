@@ -18,6 +18,7 @@
 
 #include "vx_common.cuh"
 #include "vx_field.cuh"
+#include "vx_fri.cuh"
 #include "vx_merkle.cuh"
 #include "vx_ntt.cuh"
 #include "vx_prover.cuh"
@@ -173,24 +174,9 @@ struct LeafCircleFold {
         return 16u;
     }
 };
+
 // Line fold of FRI layer k-1 into layer k.
-struct LeafLineFold {
-    const uint32_t *i0, *i1, *i2, *i3;
-    const uint32_t *tw;
-    const uint32_t *alpha_ptr;
-    uint32_t *o0, *o1, *o2, *o3;
-    qm31 al;
-    __device__ __forceinline__ void init() { al = {{alpha_ptr[0], alpha_ptr[1], alpha_ptr[2], alpha_ptr[3]}}; }
-    __device__ __forceinline__ uint32_t load(uint64_t j, uint32_t m[16]) const {
-        uint2 a0 = __ldg((const uint2 *)i0 + j), a1 = __ldg((const uint2 *)i1 + j);
-        uint2 a2 = __ldg((const uint2 *)i2 + j), a3 = __ldg((const uint2 *)i3 + j);
-        qm31 f0{{a0.x, a1.x, a2.x, a3.x}}, f1{{a0.y, a1.y, a2.y, a3.y}};
-        qm31 r = qadd(qadd(f0, f1), qmul(al, qmulm(qsub(f0, f1), __ldg(tw + j))));
-        o0[j] = r.v[0]; o1[j] = r.v[1]; o2[j] = r.v[2]; o3[j] = r.v[3];
-        m[0] = r.v[0]; m[1] = r.v[1]; m[2] = r.v[2]; m[3] = r.v[3];
-        return 16u;
-    }
-};
+using LeafLineFold = LeafFold;
 
 // Query values and sibling values of every committed column, written
 // into the proof.  Thread (tree, q): tree 0 = trace, 1 = quotient, 2 + k
@@ -514,7 +500,7 @@ static int enqueue_stage(vx_prover *p, uint32_t stage, uint32_t a, uint32_t b, c
     const uint64_t n = 1ull << log_n, N = 1ull << le;
     uint32_t *proof = S.proof;
     LeafQuotient lq{S.eval, N - 1, S.alpha_q, {0, 0, 0, 0}};
-    auto ntt_launches = [](uint32_t layers) { return (layers + 10u) / 11u; };
+    auto ntt_launches = [](uint32_t layers) { return ntt_pass_count(layers); };
     switch (stage) {
     case 0:
         VX_CUDA_TRY(cudaMemsetAsync(S.chan, 0, sizeof(DevChannel), st));

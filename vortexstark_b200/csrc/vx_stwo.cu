@@ -1,0 +1,244 @@
+// stwo-format launchers (the crates/cuda-backend symbols of src/cuda/ffi.rs):
+// the bit-reversed-order circle NTT of circle_ntt_stwo.cu and its batched
+// form, the QM31 bit reverse of bit_reverse_wide.cu, lift-and-accumulate
+// (accumulate_lift.cu) and the leaf packing of pack_leaves.cu.  Same
+// signatures, arguments and synchronisation as the reference; the kernels
+// are this library's own: the NTT runs on the register-radix passes of
+// vx_ntt.cu with the stwo table layout, the permutations go through
+// shared-memory tiles so both their reads and their writes are coalesced.
+#include <mutex>
+
+#include "vx_common.cuh"
+#include "vx_field.cuh"
+#include "vx_ntt.cuh"
+#include "vx_twiddles.cuh"
+
+namespace vx {
+namespace {
+
+inline uint32_t log2_of(uint64_t n) {
+    uint32_t l = 0;
+    while ((1ull << l) < n) l++;
+    return l;
+}
+
+// ---- host pointer lists of the batched NTT, uploaded once per call into a
+// per-device buffer that only grows (the reference mallocs one per call) ----
+std::mutex g_ptr_mu;
+uint32_t **g_ptr_buf[64] = {nullptr};
+uint32_t g_ptr_cap[64] = {0};
+
+cudaError_t upload_ptrs(uint32_t *const *host, uint32_t n, uint32_t ***dev_out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (g_ptr_cap[dev] < n) {
+        if (g_ptr_buf[dev]) cudaFree(g_ptr_buf[dev]);
+        g_ptr_buf[dev] = nullptr;
+        g_ptr_cap[dev] = 0;
+        uint32_t cap = n < 64u ? 64u : n;
+        e = cudaMalloc(&g_ptr_buf[dev], cap * sizeof(uint32_t *));
+        if (e != cudaSuccess) return e;
+        g_ptr_cap[dev] = cap;
+    }
+    e = cudaMemcpy(g_ptr_buf[dev], host, n * sizeof(uint32_t *), cudaMemcpyHostToDevice);
+    *dev_out = g_ptr_buf[dev];
+    return e;
+}
+
+bool stwo_size_ok(uint32_t n, const char *who) {
+    uint32_t l = log2_of(n);
+    if (n < 4 || (1ull << l) != n || l > 30) {
+        set_last_error(VX_ERR_ARG, "%s: n = %u must be a power of two >= 4", who, n);
+        return false;
+    }
+    return true;
+}
+
+// ---- QM31 bit reverse (bit_reverse_wide.cu:21-36), out of place ----
+// Tiled: index bits [lo: 5][mid: L-10][hi: 5] go to [brev hi][brev mid][brev lo];
+// a block moves the 32 x 32 (hi, lo) tile of one mid value through shared
+// memory, reading rows of 32 consecutive elements and writing rows of 32.
+constexpr uint32_t kBrT = 5;                 // tile side 2^5
+constexpr uint32_t kBrS = 1u << kBrT;
+__global__ void __launch_bounds__(256) brev_qm31_tiled_kernel(const uint4 *__restrict__ in, uint4 *__restrict__ out,
+                                                               uint32_t log_n) {
+    __shared__ uint4 tile[kBrS][kBrS + 1];
+    const uint32_t mid_bits = log_n - 2 * kBrT;
+    const uint64_t mid = blockIdx.x;
+    const uint64_t bmid = mid_bits ? brev_bits((uint32_t)mid, mid_bits) : 0u;
+    const uint32_t tx = threadIdx.x & (kBrS - 1u), ty = threadIdx.x >> kBrT;  // 32 x 8
+#pragma unroll
+    for (uint32_t r = 0; r < kBrS; r += 8) {
+        const uint32_t hi = ty + r, lo = tx;
+        const uint64_t i = lo | (mid << kBrT) | ((uint64_t)hi << (log_n - kBrT));
+        tile[hi][lo] = in[i];
+    }
+    __syncthreads();
+#pragma unroll
+    for (uint32_t r = 0; r < kBrS; r += 8) {
+        const uint32_t row = ty + r, col = tx;  // row = brev(lo), col = brev(hi)
+        const uint32_t lo = brev_bits(row, kBrT), hi = brev_bits(col, kBrT);
+        const uint64_t j = col | (bmid << kBrT) | ((uint64_t)row << (log_n - kBrT));
+        out[j] = tile[hi][lo];
+    }
+}
+
+__global__ void brev_qm31_kernel(const uint32_t *__restrict__ in, uint32_t *__restrict__ out, uint64_t n,
+                                 uint32_t log_n) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint64_t j = brev_bits((uint32_t)i, log_n);
+#pragma unroll
+    for (int c = 0; c < 4; c++) out[4 * j + c] = in[4 * i + c];
+}
+
+// ---- lift_and_accumulate pass (accumulate_lift.cu:16-31): col[i] +=
+// curr[((i >> (r + 1)) << 1) | (i & 1)], four elements per thread ----
+__global__ void accumulate_lift4_kernel(uint4 *__restrict__ col, const uint32_t *__restrict__ curr, uint64_t n4,
+                                        uint32_t r) {
+    uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n4) return;
+    const uint64_t i = 4 * t;
+    uint4 v = col[t];
+    uint32_t s0, s1, s2, s3;
+    if (r == 0) {
+        uint4 c = __ldg((const uint4 *)curr + t);
+        s0 = c.x; s1 = c.y; s2 = c.z; s3 = c.w;
+    } else {
+        // 2^(r+1) >= 4: the four indices share i >> (r + 1)
+        uint2 c = __ldg((const uint2 *)(curr + ((i >> (r + 1)) << 1)));
+        s0 = c.x; s1 = c.y; s2 = c.x; s3 = c.y;
+    }
+    v.x = madd(v.x, s0); v.y = madd(v.y, s1); v.z = madd(v.z, s2); v.w = madd(v.w, s3);
+    col[t] = v;
+}
+
+__global__ void accumulate_lift_kernel(uint32_t *__restrict__ col, const uint32_t *__restrict__ curr, uint64_t n,
+                                       uint32_t r) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    col[i] = madd(col[i], curr[((i >> (r + 1)) << 1) | (i & 1)]);
+}
+
+// ---- pack_leaves (pack_leaves.cu:22-38): out[c*16 + p][i] = in[c][16 i + p].
+// A block reads 16 x 32 consecutive words of one input column and writes 32
+// consecutive words to each of the 16 output columns. ----
+__global__ void __launch_bounds__(256) pack_leaves_kernel(const uint32_t *const *__restrict__ in,
+                                                          uint32_t *const *__restrict__ out, uint64_t n_out) {
+    __shared__ uint32_t tile[16][33];
+    const uint32_t c = blockIdx.y;
+    const uint64_t base = (uint64_t)blockIdx.x * 32u;  // output position of the tile
+    const uint32_t *src = in[c];
+    for (uint32_t k = threadIdx.x; k < 512u; k += blockDim.x) {
+        const uint64_t pos = base + (k >> 4);
+        if (pos < n_out) tile[k & 15u][k >> 4] = src[16ull * base + k];
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < 512u; k += blockDim.x) {
+        const uint32_t p = k >> 5, q = k & 31u;
+        if (base + q < n_out) out[c * 16u + p][base + q] = tile[p][q];
+    }
+}
+
+}  // namespace
+}  // namespace vx
+
+using namespace vx;
+
+extern "C" {
+
+void cuda_stwo_ntt_evaluate(uint32_t *d, const uint32_t *tw, uint32_t n) {
+    if (!stwo_size_ok(n, "cuda_stwo_ntt_evaluate")) return;
+    const uint32_t log_n = log2_of(n);
+    cudaError_t e = ntt_transform(d, nullptr, 0, 1, log_n, stwo_tables(tw, log_n), true, nullptr, 0, 0);
+    if (e != cudaSuccess) set_last_error(VX_ERR_CUDA, "cuda_stwo_ntt_evaluate: %s", cudaGetErrorString(e));
+    cudaDeviceSynchronize();
+}
+
+void cuda_stwo_ntt_interpolate(uint32_t *d, const uint32_t *itw, uint32_t n) {
+    if (!stwo_size_ok(n, "cuda_stwo_ntt_interpolate")) return;
+    const uint32_t log_n = log2_of(n);
+    cudaError_t e = ntt_transform(d, nullptr, 0, 1, log_n, stwo_tables(itw, log_n), false, nullptr, 0, 0);
+    if (e != cudaSuccess) set_last_error(VX_ERR_CUDA, "cuda_stwo_ntt_interpolate: %s", cudaGetErrorString(e));
+    cudaDeviceSynchronize();
+}
+
+static void stwo_batch(uint32_t *const *cols, const uint32_t *tw, uint32_t n, uint32_t n_cols, bool fwd,
+                       const char *who) {
+    if (n_cols == 0 || n < 2) return;  // the reference returns early for these
+    if (!stwo_size_ok(n, who)) return;
+    const uint32_t log_n = log2_of(n);
+    std::lock_guard<std::mutex> lk(g_ptr_mu);
+    uint32_t **dev = nullptr;
+    cudaError_t e = upload_ptrs(cols, n_cols, &dev);
+    if (e == cudaSuccess) e = ntt_transform(nullptr, dev, 0, n_cols, log_n, stwo_tables(tw, log_n), fwd, nullptr, 0, 0);
+    if (e != cudaSuccess) set_last_error(VX_ERR_CUDA, "%s: %s", who, cudaGetErrorString(e));
+    cudaDeviceSynchronize();  // the pointer buffer is reused by the next call
+}
+
+void cuda_stwo_ntt_batch_evaluate(uint32_t *const *cols, const uint32_t *tw, uint32_t n, uint32_t n_cols) {
+    stwo_batch(cols, tw, n, n_cols, true, "cuda_stwo_ntt_batch_evaluate");
+}
+
+void cuda_stwo_ntt_batch_interpolate(uint32_t *const *cols, const uint32_t *itw, uint32_t n, uint32_t n_cols) {
+    stwo_batch(cols, itw, n, n_cols, false, "cuda_stwo_ntt_batch_interpolate");
+}
+
+void cuda_bit_reverse_qm31(const uint32_t *in, uint32_t *out, uint32_t n, uint32_t log_n) {
+    if (n == 0) return;
+    if (log_n > 31 || (1ull << log_n) != n) {
+        set_last_error(VX_ERR_ARG, "cuda_bit_reverse_qm31: n = %u is not 2^log_n (log_n = %u)", n, log_n);
+        return;
+    }
+    const bool aligned = (((uintptr_t)in | (uintptr_t)out) & 15u) == 0;
+    if (log_n >= 2 * kBrT && aligned)
+        brev_qm31_tiled_kernel<<<(unsigned)(1ull << (log_n - 2 * kBrT)), 256>>>((const uint4 *)in, (uint4 *)out,
+                                                                                log_n);
+    else
+        brev_qm31_kernel<<<blocks_for(n, 256), 256>>>(in, out, n, log_n);
+    VX_LAUNCH_CHECK();
+}
+
+void cuda_accumulate_lift(uint32_t *col, const uint32_t *curr, uint32_t col_n, uint32_t log_ratio) {
+    if (col_n == 0) return;
+    const bool vec = (col_n % 4u == 0) && (((uintptr_t)col & 15u) == 0) &&
+                     (log_ratio == 0 ? (((uintptr_t)curr & 15u) == 0) : (((uintptr_t)curr & 7u) == 0));
+    if (vec)
+        accumulate_lift4_kernel<<<blocks_for(col_n / 4u, 256), 256>>>((uint4 *)col, curr, col_n / 4u, log_ratio);
+    else
+        accumulate_lift_kernel<<<blocks_for(col_n, 256), 256>>>(col, curr, col_n, log_ratio);
+    VX_LAUNCH_CHECK();
+}
+
+void cuda_pack_leaves(const uint32_t *const *input_col_ptrs, uint32_t *const *output_col_ptrs, uint32_t n) {
+    if (n == 0) return;
+    if (n % 16u) {
+        set_last_error(VX_ERR_ARG, "cuda_pack_leaves: N = %u is not a multiple of 16", n);
+        return;
+    }
+    const uint64_t n_out = n / 16u;
+    pack_leaves_kernel<<<dim3(blocks_for(n_out, 32), 4), 256>>>(input_col_ptrs, output_col_ptrs, n_out);
+    VX_LAUNCH_CHECK();
+}
+
+}  // extern "C"
+
+extern "C" int vx_stwo_twiddles(uint32_t log_n, int inverse, uint32_t *out, void *stream) {
+    VX_CHECK_ARG(out != nullptr, "vx_stwo_twiddles: out is null");
+    VX_CHECK_ARG(log_n >= 2 && log_n <= 29, "vx_stwo_twiddles: log_n %u outside 2..29", log_n);
+    GenTables g;
+    VX_CUDA_TRY(gen_tables_get(&g));
+    VX_CUDA_TRY(build_stwo_table_with(g, log_n, inverse != 0, out, (cudaStream_t)stream));
+    return VX_OK;
+}
+
+extern "C" int vx_stwo_fold_circle_twiddles(uint32_t log, uint32_t *out, void *stream) {
+    VX_CHECK_ARG(out != nullptr, "vx_stwo_fold_circle_twiddles: out is null");
+    VX_CHECK_ARG(log >= 2 && log <= 30, "vx_stwo_fold_circle_twiddles: log %u outside 2..30", log);
+    GenTables g;
+    VX_CUDA_TRY(gen_tables_get(&g));
+    VX_CUDA_TRY(build_stwo_fold_circle_with(g, log, out, (cudaStream_t)stream));
+    return VX_OK;
+}

@@ -98,3 +98,58 @@ def permute_hc_to_canonic_brt(src, dst, log_n: int) -> None:
 
 def permute_canonic_brt_to_hc_natural(src, dst, log_n: int) -> None:
     _lib.lib().cuda_permute_canonic_brt_to_hc_natural(src.data_ptr(), dst.data_ptr(), 1 << log_n, log_n)
+
+
+# ---- stwo format (ntt.rs:288-379, circle_ntt_stwo.cu, circle_ntt_stwo_batch.cu) ----
+class StwoNttCache:
+    """ntt.rs:288-362 — stwo twiddles of CanonicCoset(log_n)'s circle domain
+    (the layout of CpuBackend::precompute_twiddles), built on the device
+    (vx_stwo_twiddles) instead of on the CPU and uploaded."""
+
+    def __init__(self, log_n: int):
+        import torch
+
+        self.log_n = log_n
+        half = 1 << (log_n - 1)
+        self.d_fwd_twiddles = torch.empty(half, dtype=torch.int32, device="cuda")
+        self.d_inv_twiddles = torch.empty(half, dtype=torch.int32, device="cuda")
+        L = _lib.lib()
+        _lib.check(L.vx_stwo_twiddles(log_n, 0, self.d_fwd_twiddles.data_ptr(), None))
+        _lib.check(L.vx_stwo_twiddles(log_n, 1, self.d_inv_twiddles.data_ptr(), None))
+        torch.cuda.synchronize()
+
+
+def evaluate_stwo(d_data, cache: StwoNttCache) -> None:
+    """ntt.rs:365-371 — coefficients -> values in bit-reversed circle-domain order."""
+    _lib.clear_error()
+    _lib.lib().cuda_stwo_ntt_evaluate(d_data.data_ptr(), cache.d_fwd_twiddles.data_ptr(), 1 << cache.log_n)
+    _lib.raise_if_error()
+
+
+def interpolate_stwo(d_data, cache: StwoNttCache) -> None:
+    """ntt.rs:373-379 — values -> coefficients (with the 1/n scale)."""
+    _lib.clear_error()
+    _lib.lib().cuda_stwo_ntt_interpolate(d_data.data_ptr(), cache.d_inv_twiddles.data_ptr(), 1 << cache.log_n)
+    _lib.raise_if_error()
+
+
+def _host_ptrs(cols):
+    return (C.c_void_p * len(cols))(*[c.data_ptr() for c in cols])
+
+
+def evaluate_stwo_batch(columns, cache: StwoNttCache) -> None:
+    """poly_ops.rs:676-770 (cuda_stwo_ntt_batch_evaluate) — equal-size columns."""
+    if columns:
+        _lib.clear_error()
+        _lib.lib().cuda_stwo_ntt_batch_evaluate(_host_ptrs(columns), cache.d_fwd_twiddles.data_ptr(),
+                                                1 << cache.log_n, len(columns))
+        _lib.raise_if_error()
+
+
+def interpolate_stwo_batch(columns, cache: StwoNttCache) -> None:
+    """poly_ops.rs:772-830 (cuda_stwo_ntt_batch_interpolate) — equal-size columns."""
+    if columns:
+        _lib.clear_error()
+        _lib.lib().cuda_stwo_ntt_batch_interpolate(_host_ptrs(columns), cache.d_inv_twiddles.data_ptr(),
+                                                   1 << cache.log_n, len(columns))
+        _lib.raise_if_error()
