@@ -182,6 +182,11 @@ def served_benchmark(seed: int, n_requests: int = 512):
     }
 
 
+# DRAM bytes of one LDE (iNTT 2^24 + evaluate 2^26, six pass launches): the ncu
+# capture of the same passes at log_n = 23 read 585 MB and wrote 257 MB; the
+# log_n = 24 plan is the same with every array twice the size.
+LDE_TRAFFIC_LOG24 = 2 * (585e6 + 257e6)
+
 LIFT_LOGS = [16] * 8 + [18] * 16 + [20] * 10  # 34 columns, blowup 4: LDEs of 2^18 / 2^20 / 2^22
 
 
@@ -282,6 +287,25 @@ def batched_commit_benchmark(seed: int, steps: int, warmup: int, peak_gbs: float
     return out
 
 
+def blake2s_probe_rate(stream) -> float:
+    """Register-only Blake2s compressions/s on this GPU (the ALU roofline)."""
+    import torch
+
+    from vortexstark_b200 import _lib
+
+    L = _lib.lib()
+    s = stream.cuda_stream
+    out = torch.empty(148 * 8 * 256, dtype=torch.int32, device="cuda")
+    iters = 256
+    _lib.check(L.vx_probe_blake2s(148 * 8, 256, iters, out.data_ptr(), s))
+    pa, pb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    pa.record(stream)
+    _lib.check(L.vx_probe_blake2s(148 * 8, 256, iters, out.data_ptr(), s))
+    pb.record(stream)
+    stream.synchronize()
+    return 148 * 8 * 256 * iters / (pa.elapsed_time(pb) / 1e3)
+
+
 def run_reference(args, rank: int):
     """CPU oracle arm: each step one proof of the workload (or a bounded
     sample of it), all host threads."""
@@ -337,6 +361,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-served", action="store_true", help="skip the mixed-size served stream")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched lifted commitment")
+    ap.add_argument("--batched-only", action="store_true",
+                    help="run only the batched lifted commitment and print its object")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -358,6 +384,15 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
+
+    if args.batched_only:
+        peak, _ = _peaks()
+        probe = blake2s_probe_rate(torch.cuda.Stream())
+        res = batched_commit_benchmark(SEED, max(args.steps, 5), args.warmup, peak, probe,
+                                       cpu=not args.no_cpu_baseline)
+        if rank == 0:
+            print(json.dumps({"batched_commit": res}), flush=True)
+        return
 
     import ctypes as C
 
@@ -443,15 +478,7 @@ def main():
     stream.synchronize()
     tcommit_t = statistics.median([tc[2 * r].elapsed_time(tc[2 * r + 1]) for r in range(reps)]) / 1e3
     compressions = 2 * N - 1
-    probe_out = torch.empty(148 * 8 * 256, dtype=torch.int32, device="cuda")
-    iters = 256
-    _lib.check(L.vx_probe_blake2s(148 * 8, 256, iters, probe_out.data_ptr(), s))
-    pa, pb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    pa.record(stream)
-    _lib.check(L.vx_probe_blake2s(148 * 8, 256, iters, probe_out.data_ptr(), s))
-    pb.record(stream)
-    stream.synchronize()
-    probe_rate = 148 * 8 * 256 * iters / (pa.elapsed_time(pb) / 1e3)
+    probe_rate = blake2s_probe_rate(stream)
     merkle_rate = compressions / tcommit_t
 
     # per-stage device time of one proof (vx_prover_stage_async, stages in order)
@@ -493,7 +520,11 @@ def main():
             "lde_hbm_gbs": lde_gbs,
             "roofline": {"bound": "hbm", "kernel": "LDE (interpolate 2^24 + zero-pad + evaluate 2^26)",
                          "achieved": lde_gbs, "peak": peak, "unit": "GB/s", "frac": lde_gbs / peak,
-                         "peak_source": peak_kind, "traffic": None,
+                         "peak_source": peak_kind,
+                         "traffic": LDE_TRAFFIC_LOG24 if log_n == 24 else None,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the six LDE launches "
+                                           "at log_n=23 (842 MB), x2 for log_n=24 (same pass plan, arrays twice "
+                                           "the size)",
                          "algorithmic_bytes": lde_bytes, "time_ms": lde_t * 1e3},
             "roofline_alu": {"bound": "int-alu (Blake2s)", "kernel": "trace commitment (2^26 leaves)",
                              "achieved": merkle_rate, "peak": probe_rate, "unit": "compressions/s",
