@@ -163,7 +163,7 @@ def served_benchmark(seed: int, n_requests: int = 512):
             srv.prewarm(ln, counts.get(ln, 2))
         run_stream(srv, reqs[:64], [0.0] * 64)  # warm-up
         sweep = []
-        for mult in (0.8, 1.5, 2.0, 2.5, 3.0, 4.0, 6.0):
+        for mult in (0.8, 1.0, 1.1, 1.2, 1.35, 1.5, 2.0):
             r, _ = run_stream(srv, reqs, poisson_arrivals(n_requests, mult * cap, seed + 2))
             r["rate"] = mult * cap
             sweep.append(r)

@@ -864,6 +864,10 @@ int prover_capture_graph(vx_prover *p, cudaStream_t st, uint32_t *dev_ab, const 
     for (uint32_t stage = 0; stage < VX_N_STAGES && rc == VX_OK; stage++) rc = enqueue_stage(p, stage, 0u, 0u, st, &launches);
     if (rc == VX_OK && cudaMemcpyAsync(pinned_out, S.proof, S.L.words * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess)
         rc = VX_ERR_CUDA;
+    // the transcript status word right after the proof bytes
+    if (rc == VX_OK && cudaMemcpyAsync((uint8_t *)pinned_out + S.L.words * 4, &S.chan->err, 4, cudaMemcpyDeviceToHost,
+                                       st) != cudaSuccess)
+        rc = VX_ERR_CUDA;
     cudaError_t e = cudaStreamEndCapture(st, &g);
     S.inputs = nullptr;
     if (rc != VX_OK) { if (g) cudaGraphDestroy(g); return rc; }

@@ -59,6 +59,9 @@ struct ProofSlot {
 
 struct vx_prover;
 namespace vx {
+// One whole proof as a CUDA graph: (a, b) read from pinned_ab, the proof
+// bytes copied to pinned_out followed by the 4-byte transcript status word
+// (pinned_out holds prover_proof_bytes + 4 bytes).
 int prover_capture_graph(vx_prover *p, cudaStream_t st, uint32_t *dev_ab, const uint32_t *pinned_ab,
                          void *pinned_out, cudaGraphExec_t *exec);
 uint32_t prover_log_n(const vx_prover *p);

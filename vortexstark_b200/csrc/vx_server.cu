@@ -12,6 +12,14 @@
 // Proofs of different requests therefore overlap on the device while each
 // proof's own kernels stay in order; every proof is computed by the same
 // kernels on its own buffers, so its bytes do not depend on what else runs.
+//
+// Scheduling policy.  A proof with an evaluation domain of 2^24 points or
+// more fills every SM by itself for most of its kernels, so two of them in
+// flight only split the GPU and both finish later: at most one such "large"
+// proof is admitted at a time (others wait in the queue, oldest first).
+// Smaller proofs are chains of short kernels that leave most SMs idle; their
+// streams get the device's highest priority so their blocks are dispatched
+// ahead of a large proof's waiting blocks and fill the gaps it leaves.
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -38,9 +46,14 @@ struct Request {
     uint64_t submit_ns;
 };
 
+// Evaluation domains of at least 2^kLargeLogEval points fill the GPU alone.
+constexpr uint32_t kLargeLogEval = 24;
+constexpr uint32_t kMaxLargeInflight = 1;
+
 struct Slot {
     vx_prover *p = nullptr;
     uint32_t log_n = 0;
+    bool large = false;
     cudaStream_t st = nullptr;
     cudaEvent_t done = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -67,7 +80,7 @@ struct vx_server {
     std::thread worker;
     bool stop = false;
     size_t budget = 0, used = 0;
-    uint32_t max_inflight = 1, inflight = 0, blowup = 2, nq = 80;
+    uint32_t max_inflight = 1, inflight = 0, large_inflight = 0, blowup = 2, nq = 80;
     int device = 0;
     bool use_graphs = true;
     int fatal = VX_OK;
@@ -97,9 +110,15 @@ int slot_create(vx_server *s, uint32_t log_n, Slot **out) {
         return VX_ERR_CUDA;
     };
     cudaError_t e;
-    if ((e = cudaStreamCreateWithFlags(&sl->st, cudaStreamNonBlocking)) != cudaSuccess) return fail("stream", e);
+    sl->large = log_n + s->blowup >= kLargeLogEval;
+    int prio_least = 0, prio_greatest = 0;
+    if ((e = cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest)) != cudaSuccess) return fail("priorities", e);
+    if ((e = cudaStreamCreateWithPriority(&sl->st, cudaStreamNonBlocking, sl->large ? prio_least : prio_greatest)) !=
+        cudaSuccess)
+        return fail("stream", e);
     if ((e = cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming)) != cudaSuccess) return fail("event", e);
-    if ((e = cudaMallocHost(&sl->pinned_out, sl->bytes)) != cudaSuccess) return fail("pinned output", e);
+    // proof bytes, then the transcript status word
+    if ((e = cudaMallocHost(&sl->pinned_out, sl->bytes + 16)) != cudaSuccess) return fail("pinned output", e);
     if ((e = cudaMallocHost(&sl->pinned_ab, 8)) != cudaSuccess) return fail("pinned input", e);
     if ((e = cudaMalloc(&sl->dev_ab, 256)) != cudaSuccess) return fail("device input", e);
     if (s->use_graphs) {
@@ -137,6 +156,7 @@ int launch(vx_server *s, Slot *sl, const Request &r) {
     sl->req = r;
     sl->start_ns = now_ns();
     s->inflight++;
+    if (sl->large) s->large_inflight++;
     if (sl->exec) {
         sl->pinned_ab[0] = r.a;
         sl->pinned_ab[1] = r.b;
@@ -146,6 +166,8 @@ int launch(vx_server *s, Slot *sl, const Request &r) {
         if (rc) return rc;
         rc = vx_prover_fetch_async(sl->p, sl->pinned_out, sl->st);
         if (rc) return rc;
+        VX_CUDA_TRY(cudaMemcpyAsync(sl->pinned_out + sl->bytes, prover_chan_err(sl->p), 4, cudaMemcpyDeviceToHost,
+                                    sl->st));
     }
     VX_CUDA_TRY(cudaEventRecord(sl->done, sl->st));
     return VX_OK;
@@ -177,13 +199,14 @@ void worker_loop(vx_server *s) {
             c.status = q == cudaSuccess ? VX_OK : VX_ERR_CUDA;
             if (q == cudaSuccess) {
                 uint32_t err = 0;
-                cudaMemcpy(&err, prover_chan_err(sl->p), 4, cudaMemcpyDeviceToHost);
+                memcpy(&err, sl->pinned_out + sl->bytes, 4);  // copied by the proof's own stream
                 if (err) c.status = VX_ERR_DEVICE;
             }
             s->results[c.tag].assign(sl->pinned_out, sl->pinned_out + sl->bytes);
             s->completed.push_back(c);
             sl->busy = false;
             s->inflight--;
+            if (sl->large) s->large_inflight--;
             progress = true;
         }
         // admit queued requests, oldest first, skipping ones that cannot start
@@ -193,6 +216,10 @@ void worker_loop(vx_server *s) {
         // so an index keeps naming the same request.
         for (size_t qi = 0; qi < s->pending.size() && s->inflight < s->max_inflight;) {
             const uint32_t log_n = s->pending[qi].log_n;
+            if (log_n + s->blowup >= kLargeLogEval && s->large_inflight >= kMaxLargeInflight) {
+                ++qi;  // a large proof is running: this one waits, smaller ones behind it may start
+                continue;
+            }
             Slot *free_slot = nullptr;
             for (Slot *sl : s->slots)
                 if (!sl->busy && sl->log_n == log_n) { free_slot = sl; break; }
