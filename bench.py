@@ -287,6 +287,52 @@ def batched_commit_benchmark(seed: int, steps: int, warmup: int, peak_gbs: float
     return out
 
 
+def ntt_microbench(peak_gbs: float, sizes=(20, 24, 28), reps: int = 5):
+    """Standalone circle NTT / iNTT on 2^k uniform M31 values over
+    half_coset(k), through the reference-compatible launchers
+    (cuda_circle_ntt_evaluate / _interpolate, which synchronise like the
+    reference's), timed with CUDA events on the legacy stream around `reps`
+    calls; the reference's own kernels compiled for sm_100a are timed the same
+    way when they are built.  Algorithmic bytes: 8 per element (one read, one
+    write)."""
+    import torch
+
+    from vortexstark_b200 import ntt
+    from vortexstark_b200.circle import Coset
+    from vortexstark_b200.workload import m31_array
+
+    out = {}
+    ds = torch.cuda.default_stream()
+    for k in sizes:
+        n = 1 << k
+        cache = ntt.TwiddleCache(Coset.half_coset(k))
+        d = torch.from_numpy(m31_array(SEED + k, n).view("int32")).cuda()
+        ntt.evaluate(d, cache)
+        ntt.interpolate(d, cache)
+        res = {}
+        for name, fn in (("evaluate", ntt.evaluate), ("interpolate", ntt.interpolate)):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(ds)
+            for _ in range(reps):
+                fn(d, cache)
+            e1.record(ds)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            res[name] = {"ms": ms, "gbs": 8 * n / (ms / 1e3) / 1e9, "frac": 8 * n / (ms / 1e3) / 1e9 / peak_gbs}
+        try:
+            from oracle import oracle as O
+
+            if O.ref_available():
+                re_, ri = O.ref_ntt_time(k, reps)
+                res["reference_kernels_ms"] = {"evaluate": re_, "interpolate": ri}
+        except Exception as exc:  # the reference kernels are optional here
+            res["reference_kernels_ms"] = f"unavailable: {exc}"
+        out[f"2^{k}"] = res
+        del d, cache
+        torch.cuda.empty_cache()
+    return out
+
+
 def blake2s_probe_rate(stream) -> float:
     """Register-only Blake2s compressions/s on this GPU (the ALU roofline)."""
     import torch
@@ -361,6 +407,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-served", action="store_true", help="skip the mixed-size served stream")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched lifted commitment")
+    ap.add_argument("--no-micro", action="store_true", help="skip the NTT / iNTT microbench (2^20, 2^24, 2^28)")
     ap.add_argument("--batched-only", action="store_true",
                     help="run only the batched lifted commitment and print its object")
     args = ap.parse_args()
@@ -534,6 +581,8 @@ def main():
             "launches_per_proof": launches_per_proof,
             "clocks": clocks,
         }
+        if world == 1 and not args.no_micro:
+            line["ntt_microbench"] = ntt_microbench(peak)
         if world == 1 and not args.no_batched:
             line["batched_commit"] = batched_commit_benchmark(SEED, max(steps, 5), args.warmup, peak, probe_rate,
                                                               cpu=not args.no_cpu_baseline)

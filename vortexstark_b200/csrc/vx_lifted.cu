@@ -102,20 +102,35 @@ void lift_template(const LiftLayout &L, std::vector<uint32_t> &t) {
     for (uint32_t k = 0; k < L.nfri; k++) dec(L.fri[k]);
 }
 
+// x mod P folded once: (x & P) + (x >> 31) < 2^34 for any 64-bit x.
+__device__ __forceinline__ uint64_t fold64(uint64_t x) { return (x & VX_P) + (x >> 31); }
+// Canonical M31 of an accumulator below 2^34.
+__device__ __forceinline__ uint32_t reduce34(uint64_t x) {
+    const uint32_t r = (uint32_t)fold64(x);  // < 2^31 + 8
+    return umin32(r, r - VX_P);
+}
+
 // C[i] = sum_c alpha^c * lift(col_c)[i], computed while C's tree hashes it.
+// Each coordinate is a 64-bit multiply-accumulate of 31-bit products (one
+// IMAD.WIDE per column and coordinate), folded every 3 columns so the sum
+// stays below 2^34 + 3 * 2^62 < 2^64, and reduced to canonical M31 once.
 struct LeafCombine {
     LeafLifted cols;
     const uint32_t *pw;  // alpha^c as 4 words each
     uint32_t *o0, *o1, *o2, *o3;
     __device__ __forceinline__ void init() {}
     __device__ __forceinline__ uint32_t load(uint64_t i, uint32_t m[16]) const {
-        uint32_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-        for (uint32_t c = 0; c < cols.n_cols; c++) {
+        uint64_t s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+        const uint32_t nc = cols.n_cols;
+        for (uint32_t c = 0; c < nc; c++) {
             const uint32_t v = cols.word(c, i);
             const uint4 p = __ldg((const uint4 *)pw + c);
-            a0 = madd(a0, mmul(p.x, v)); a1 = madd(a1, mmul(p.y, v));
-            a2 = madd(a2, mmul(p.z, v)); a3 = madd(a3, mmul(p.w, v));
+            s0 += (uint64_t)p.x * v; s1 += (uint64_t)p.y * v;
+            s2 += (uint64_t)p.z * v; s3 += (uint64_t)p.w * v;
+            if (c % 3u == 2u) { s0 = fold64(s0); s1 = fold64(s1); s2 = fold64(s2); s3 = fold64(s3); }
         }
+        s0 = fold64(s0); s1 = fold64(s1); s2 = fold64(s2); s3 = fold64(s3);
+        const uint32_t a0 = reduce34(s0), a1 = reduce34(s1), a2 = reduce34(s2), a3 = reduce34(s3);
         o0[i] = a0; o1[i] = a1; o2[i] = a2; o3[i] = a3;
         m[0] = a0; m[1] = a1; m[2] = a2; m[3] = a3;
         return 16u;
