@@ -333,6 +333,45 @@ def ntt_microbench(peak_gbs: float, sizes=(20, 24, 28), reps: int = 5):
     return out
 
 
+def pow_benchmark(probe_rate: float, bits: int = 26, cpu: bool = True):
+    """Proof-of-work search at 26 bits (stwo's order (hi << 32) | low) from a
+    seeded channel state: device time of vx_grind_pow and the candidates it
+    had to hash, beside the CPU oracle's search of the same nonce."""
+    import hashlib
+    import struct
+
+    from vortexstark_b200.channel import Channel
+    from vortexstark_b200.grind import grind_prefixed
+
+    ch = Channel()
+    ch.mix_digest(struct.unpack("<8I", hashlib.blake2s(struct.pack("<Q", SEED)).digest()))
+    pre = ch.pow_prefix(bits)
+    grind_prefixed(pre, 8)  # warm-up
+    times, nonce = [], 0
+    for _ in range(3):
+        t0 = time.perf_counter()
+        nonce = grind_prefixed(pre, bits)
+        times.append(time.perf_counter() - t0)
+    t = statistics.median(times)
+    # candidates hashed: whole launches of 64 batches of 2^20 up to the one that found it
+    launches = (nonce >> 32) // 64 + 1
+    cand = launches * 64 * (1 << 20)
+    out = {"pow_bits": bits, "nonce": nonce, "valid": ch.verify_pow_nonce(bits, nonce), "ms": 1e3 * t,
+           "candidates_hashed_max": cand, "compressions_per_s_min": cand / t if launches > 1 else None,
+           "probe_compressions_per_s": probe_rate,
+           "note": "host-timed around the synchronous call (launches of 2^26 candidates, result read back "
+                   "between launches); each candidate is one Blake2s compression"}
+    if cpu:
+        from oracle import oracle as O
+
+        O.lib()
+        t0 = time.perf_counter()
+        cn = O.grind_pow(list(pre), bits)
+        out["cpu_baseline"] = {"ms": 1e3 * (time.perf_counter() - t0), "nonce_equal": cn == nonce,
+                               "cores": O.get_threads(), "kind": "port"}
+    return out
+
+
 def blake2s_probe_rate(stream) -> float:
     """Register-only Blake2s compressions/s on this GPU (the ALU roofline)."""
     import torch
@@ -583,6 +622,7 @@ def main():
         }
         if world == 1 and not args.no_micro:
             line["ntt_microbench"] = ntt_microbench(peak)
+            line["pow_grind"] = pow_benchmark(probe_rate, cpu=not args.no_cpu_baseline)
         if world == 1 and not args.no_batched:
             line["batched_commit"] = batched_commit_benchmark(SEED, max(steps, 5), args.warmup, peak, probe_rate,
                                                               cpu=not args.no_cpu_baseline)

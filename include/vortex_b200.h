@@ -157,6 +157,19 @@ void cuda_fold_circle_into_line_soa_forge(uint32_t *dst0, uint32_t *dst1, uint32
 /* replaces cuda_device_sync, fields.cu:44 */
 void cuda_device_sync(void);
 
+/* -- proof-of-work grinding (ffi.rs:761-772, 1195-1204) -- */
+/* replaces cuda_grind_pow, grind.cu:92-118: nonces batch_offset + i for
+ * i < n_threads; *result (device, set to UINT64_MAX by the caller) receives the
+ * smallest nonce whose Blake2s(prefixed_digest || nonce_le) has >= pow_bits
+ * trailing zeros in its first 16 bytes (LE u128).  prefixed_digest: 8 device
+ * words.  Asynchronous on the legacy stream, as the reference's. */
+void cuda_grind_pow(const uint32_t *prefixed_digest, uint64_t *result, uint32_t pow_bits, uint64_t batch_offset,
+                    uint32_t n_threads);
+/* replaces cuda_grind_pow_m31_output, grind_m31_output.cu: the same with the
+ * four output words reduced mod P before the trailing-zero count */
+void cuda_grind_pow_m31_output(const uint32_t *prefixed_digest, uint64_t *result, uint32_t pow_bits,
+                               uint64_t batch_offset, uint32_t n_threads);
+
 /* -- stwo-format path (crates/cuda-backend; ffi.rs:1182-1194) -- */
 /* replaces cuda_stwo_ntt_evaluate, circle_ntt_stwo.cu:268-330: bit-reversed
  * circle FFT of n = 2^k (k >= 2) words in place with the stwo twiddle table
@@ -241,6 +254,18 @@ int vx_prover_check(vx_prover *p);
  * tables are cached per size and reused by later calls. */
 int vx_prove_fib(uint32_t a, uint32_t b, uint32_t log_n, uint32_t blowup_bits, uint32_t n_queries, uint8_t *out,
                  size_t cap, size_t *out_len);
+
+/* ---- proof-of-work search on the device (new) ----
+ * Replaces the host loop of GrindOps::grind (crates/cuda-backend/src/
+ * grind_ops.rs:20-134): nonces (hi << 32) | low, low < 2^20, hi = 0 ..
+ * max_batches - 1 (stwo's search order), the smallest accepted one to
+ * *nonce_out; launches of 2^26 candidates with one 8-byte read-back between
+ * them.  prefixed_digest: 8 HOST words (Blake2s(0x12345678_le || 0^12 ||
+ * channel state || pow_bits_le), reduced mod P by the caller for the M31
+ * channel).  pow_bits = 0 gives nonce 0 without work.  VX_ERR_DEVICE if no
+ * nonce exists in the range.  Synchronous. */
+int vx_grind_pow(const uint32_t prefixed_digest[8], uint32_t pow_bits, int m31_output, uint32_t max_batches,
+                 uint64_t *nonce_out, void *stream);
 
 /* ---- stwo twiddles built on the device (new) ----
  * Replaces the CPU loops of StwoNttCache::new (ntt.rs:300-362) and the

@@ -75,6 +75,11 @@ def lib():
         L.vxo_commit_lifted.restype = C.c_int
         L.vxo_lifted_lde.argtypes = [C.POINTER(U32P), U32P, C.c_uint32, C.c_uint32, C.POINTER(U32P)]
         L.vxo_lifted_lde.restype = C.c_int
+        L.vxo_pow_prefix.argtypes = [U32P, C.c_uint32, U32P]
+        L.vxo_verify_pow_nonce.argtypes = [U32P, C.c_uint32, C.c_uint64, C.c_int]
+        L.vxo_verify_pow_nonce.restype = C.c_int
+        L.vxo_grind_pow.argtypes = [U32P, C.c_uint32, C.c_int, C.c_uint32, C.POINTER(C.c_uint64)]
+        L.vxo_grind_pow.restype = C.c_int
         for name in ("subgroup", "half_coset", "half_odds"):
             f = getattr(L, f"vxo_coset_{name}")
             f.argtypes = [C.c_uint32]
@@ -376,6 +381,25 @@ def lifted_lde(cols, blowup_bits: int = 2):
         res.append(np.ctypeslib.as_array(outs[c], shape=(m,)).copy())
         L.vxo_free(outs[c])
     return res
+
+
+# ---- proof of work ----
+def pow_prefix(state_words, pow_bits: int) -> np.ndarray:
+    st = np.array(state_words, np.uint32)
+    out = np.zeros(8, np.uint32)
+    lib().vxo_pow_prefix(_p(st), pow_bits, _p(out))
+    return out
+
+
+def verify_pow_nonce(prefix, pow_bits: int, nonce: int, m31: bool = False) -> bool:
+    return bool(lib().vxo_verify_pow_nonce(_p(np.array(prefix, np.uint32)), pow_bits, nonce, int(m31)))
+
+
+def grind_pow(prefix, pow_bits: int, m31: bool = False, max_batches: int = 1 << 12) -> int:
+    n = C.c_uint64()
+    if lib().vxo_grind_pow(_p(np.array(prefix, np.uint32)), pow_bits, int(m31), max_batches, C.byref(n)):
+        raise ValueError("no nonce found")
+    return int(n.value)
 
 
 # ---- the reference's own CUDA kernels (oracle/_ref/libvxref.so) ----

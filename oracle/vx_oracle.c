@@ -1094,3 +1094,55 @@ int vxo_lifted_lde(const uint32_t *const *cols, const uint32_t *log_sizes, uint3
                    uint32_t **lde_out) {
     return lifted_impl(cols, log_sizes, n_cols, blowup, 1, NULL, NULL, lde_out);
 }
+
+/* ------------------------------------------------------------------ */
+/* proof of work: channel.rs:140-168, grind.cu:26-90, grind_ops.rs     */
+/* ------------------------------------------------------------------ */
+void vxo_pow_prefix(const uint32_t state[8], uint32_t pow_bits, uint32_t out[8]) {
+    uint8_t in[52];
+    memset(in, 0, sizeof(in));
+    st32(in, 0x12345678u);
+    for (int i = 0; i < 8; i++) st32(in + 16 + 4 * i, state[i]);
+    st32(in + 48, pow_bits);
+    uint8_t dg[32];
+    vxo_blake2s(in, 52, dg);
+    for (int i = 0; i < 8; i++) out[i] = ld32(dg + 4 * i);
+}
+static uint32_t pow_tz(const uint32_t prefix[8], uint64_t nonce, int m31) {
+    uint32_t m[16] = {0}, h[8];
+    for (int i = 0; i < 8; i++) m[i] = prefix[i];
+    m[8] = (uint32_t)nonce;
+    m[9] = (uint32_t)(nonce >> 32);
+    for (int i = 0; i < 8; i++) h[i] = IV[i];
+    h[0] ^= 0x01010020u;
+    vxo_blake2s_compress_words(h, m, 40, 0xFFFFFFFFu);
+    uint32_t w[4];
+    for (int i = 0; i < 4; i++) w[i] = m31 ? m_red((uint64_t)h[i]) : h[i];
+    for (int i = 0; i < 4; i++)
+        if (w[i]) return 32u * (uint32_t)i + (uint32_t)__builtin_ctz(w[i]);
+    return 128u;
+}
+int vxo_verify_pow_nonce(const uint32_t prefix[8], uint32_t pow_bits, uint64_t nonce, int m31) {
+    return pow_tz(prefix, nonce, m31) >= pow_bits;
+}
+int vxo_grind_pow(const uint32_t prefix[8], uint32_t pow_bits, int m31, uint32_t max_batches, uint64_t *nonce) {
+    if (pow_bits == 0) { *nonce = 0; return 0; }
+    for (uint64_t hi = 0; hi < max_batches; hi++) {
+        /* each thread scans one contiguous run of lows in order: its first hit
+         * is its smallest, and the smallest over threads is the batch's */
+        int64_t found = -1;
+        #pragma omp parallel if (pow_bits > 8)
+        {
+            int64_t mine = -1;
+            #pragma omp for schedule(static)
+            for (int64_t low = 0; low < (int64_t)(1 << 20); low++) {
+                if (mine >= 0) continue;
+                if (pow_tz(prefix, (hi << 32) | (uint64_t)low, m31) >= pow_bits) mine = low;
+            }
+            #pragma omp critical
+            { if (mine >= 0 && (found < 0 || mine < found)) found = mine; }
+        }
+        if (found >= 0) { *nonce = (hi << 32) | (uint64_t)found; return 0; }
+    }
+    return 1;
+}

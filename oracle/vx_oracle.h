@@ -162,6 +162,17 @@ int vxo_commit_lifted(const uint32_t *const *cols, const uint32_t *log_sizes, ui
 int vxo_lifted_lde(const uint32_t *const *cols, const uint32_t *log_sizes, uint32_t n_cols, uint32_t blowup,
                    uint32_t **lde_out);
 
+/* ---- proof of work (channel.rs:140-168, grind.cu:26-90, grind_ops.rs) ----
+ * prefix = Blake2s(0x12345678_le || 0^12 || state || pow_bits_le); a nonce is
+ * accepted when Blake2s(prefix || nonce_le) has >= pow_bits trailing zeros in
+ * its first 16 bytes as a LE u128 (m31 != 0: those 4 words reduced mod P
+ * first, grind_m31_output.cu).  The search visits (hi << 32) | low, low <
+ * 2^20, hi = 0 .. max_batches-1, and returns the smallest accepted nonce
+ * (0 when pow_bits = 0); 1 if none. */
+void vxo_pow_prefix(const uint32_t state[8], uint32_t pow_bits, uint32_t out[8]);
+int vxo_verify_pow_nonce(const uint32_t prefix[8], uint32_t pow_bits, uint64_t nonce, int m31);
+int vxo_grind_pow(const uint32_t prefix[8], uint32_t pow_bits, int m31, uint32_t max_batches, uint64_t *nonce);
+
 void vxo_free(void *p);
 void vxo_set_threads(int n);
 int vxo_get_threads(void);

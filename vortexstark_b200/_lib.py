@@ -62,6 +62,10 @@ _SIGS = {
     "cuda_fold_line_soa_forge": [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, u32],
     "cuda_fold_circle_into_line_soa_forge": [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, u32],
     "cuda_device_sync": [],
+    # proof of work
+    "cuda_grind_pow": [vp, vp, u32, C.c_uint64, u32],
+    "cuda_grind_pow_m31_output": [vp, vp, u32, C.c_uint64, u32],
+    "vx_grind_pow": ([vp, u32, C.c_int, u32, C.POINTER(C.c_uint64), vp], C.c_int),
     # stwo-format path
     "cuda_stwo_ntt_evaluate": [vp, vp, u32],
     "cuda_stwo_ntt_interpolate": [vp, vp, u32],

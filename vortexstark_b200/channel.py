@@ -60,5 +60,23 @@ class Channel:
                     break
         return out
 
+    def mix_u64(self, value: int) -> None:
+        """channel.rs:120-130: state = B(state || lo_le || hi_le) (a PoW nonce)."""
+        self.state = _b2s(self.state + struct.pack("<Q", value))
+        self.n_draws = 0
+
+    def pow_prefix(self, pow_bits: int):
+        """channel.rs:149-155: B(0x12345678_le || 0^12 || state || pow_bits_le) as 8 LE words."""
+        raw = struct.pack("<I", 0x12345678) + bytes(12) + self.state + struct.pack("<I", pow_bits)
+        return struct.unpack("<8I", _b2s(raw))
+
+    def verify_pow_nonce(self, pow_bits: int, nonce: int) -> bool:
+        """channel.rs:149-168: >= pow_bits trailing zeros in the first 16 bytes
+        of B(prefix || nonce_le), read as a LE u128."""
+        h = _b2s(struct.pack("<8I", *self.pow_prefix(pow_bits)) + struct.pack("<Q", nonce))
+        v = int.from_bytes(h[:16], "little")
+        tz = (v & -v).bit_length() - 1 if v else 128
+        return tz >= pow_bits
+
     def state_words(self):
         return struct.unpack("<8I", self.state)
