@@ -353,13 +353,15 @@ def pow_benchmark(probe_rate: float, bits: int = 26, cpu: bool = True):
         nonce = grind_prefixed(pre, bits)
         times.append(time.perf_counter() - t0)
     t = statistics.median(times)
-    # candidates hashed: whole launches of 64 batches of 2^20 up to the one that found it
+    # candidates at or before the answer in the search order (hi * 2^20 + low + 1):
+    # the work any search that returns the smallest nonce must do
+    below = (nonce >> 32) * (1 << 20) + (nonce & 0xFFFFFFFF) + 1
     launches = (nonce >> 32) // 64 + 1
-    cand = launches * 64 * (1 << 20)
     out = {"pow_bits": bits, "nonce": nonce, "valid": ch.verify_pow_nonce(bits, nonce), "ms": 1e3 * t,
-           "candidates_hashed_max": cand, "compressions_per_s_min": cand / t if launches > 1 else None,
+           "candidates_to_answer": below, "launches": launches,
+           "candidates_per_s": below / t, "frac_of_probe": below / t / probe_rate,
            "probe_compressions_per_s": probe_rate,
-           "note": "host-timed around the synchronous call (launches of 2^26 candidates, result read back "
+           "note": "host-timed around the synchronous call (launches of 64 x 2^20 candidates, result read back "
                    "between launches); each candidate is one Blake2s compression"}
     if cpu:
         from oracle import oracle as O
@@ -447,6 +449,7 @@ def main():
     ap.add_argument("--no-served", action="store_true", help="skip the mixed-size served stream")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched lifted commitment")
     ap.add_argument("--no-micro", action="store_true", help="skip the NTT / iNTT microbench (2^20, 2^24, 2^28)")
+    ap.add_argument("--no-tune", action="store_true", help="keep the built-in NTT plans and leaf-kernel shapes")
     ap.add_argument("--batched-only", action="store_true",
                     help="run only the batched lifted commitment and print its object")
     args = ap.parse_args()
@@ -470,6 +473,18 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
+
+    # per-device launch shapes, chosen before any slot or context is carved
+    tuned = None
+    if not args.no_tune:
+        from vortexstark_b200 import tune
+
+        t0 = time.perf_counter()
+        tune_log = min(28, max(args.log_n + 2, 0 if args.no_micro else 28))
+        tuned = tune.autotune(tune_log)
+        tuned = {"max_log": tune_log, "seconds": round(time.perf_counter() - t0, 2),
+                 "ntt_plan": {k: v[:2] for k, v in tuned["ntt"].items()},
+                 "leaf_k": {k: v[0] for k, v in tuned["leaf_k"].items()}}
 
     if args.batched_only:
         peak, _ = _peaks()
@@ -619,6 +634,7 @@ def main():
             "gpu_launches": launches_per_proof * steps,
             "launches_per_proof": launches_per_proof,
             "clocks": clocks,
+            "autotune": tuned,
         }
         if world == 1 and not args.no_micro:
             line["ntt_microbench"] = ntt_microbench(peak)

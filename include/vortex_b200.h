@@ -380,6 +380,35 @@ int vx_probe_blake2s(uint32_t blocks, uint32_t threads, uint32_t iters, uint32_t
 int vx_tree_plan(uint32_t depth, uint32_t heights[12], uint32_t *n_levels, uint32_t *top, uint32_t *n_counters,
                  uint64_t *pool_words);
 
+/* Autotuner — no counterpart in the reference, whose kernels have fixed
+ * shapes (circle_ntt.cu: one launch per layer; blake2s.cu: one leaf per
+ * thread).  On the current device, times every distinct NTT pass plan
+ * (bottom pass of 10..12 layers, upper passes of at most 6..9) of each
+ * transform length 13..max_log (shorter ones are a single pass), and the Merkle leaf kernel's subtree size
+ * (2^1..2^4 leaves per thread) of each tree depth 17..max_log, on scratch
+ * buffers of that size (about 16 * 2^max_log bytes, freed before return),
+ * and keeps the fastest for later launches on this device.  Every choice
+ * computes identical values, so proofs do not change.  Plans are read when
+ * a transform is launched and when a tree is carved (prover slot or lifted
+ * context creation), so tune before creating those.  Writes a JSON report
+ * ({"ntt":{"log":[bottom,upper,ms]},"leaf_k":{"depth":[k,ms]}}) to `report`
+ * (cap bytes, NUL-terminated, truncated).  12 <= max_log <= 28.  Not safe
+ * to run while other host threads launch on the same device. */
+int vx_autotune(uint32_t max_log, char *report, size_t cap);
+/* Set one knob on the current device.  kind 0: NTT plan of `layers`-layer
+ * transforms, a = bottom pass maximum (9..12), b = upper pass maximum
+ * (3..9), a = 0 restores the default (12, 9).  kind 1: leaf kernel subtree
+ * log for trees of depth `layers`, a in 1..4, 0 restores the default. */
+int vx_tune_set(uint32_t kind, uint32_t layers, uint32_t a, uint32_t b);
+/* Read the knob that launches on the current device use (b = 0 for kind 1). */
+int vx_tune_get(uint32_t kind, uint32_t layers, uint32_t *a, uint32_t *b);
+/* Host-only: the pass plan of a `total`-layer transform (4..31) for a bottom
+ * pass of at most bottom_max (9..12) layers and upper passes of at most
+ * upper_max (3..9); transforms of at most 12 layers are one pass.  Pass i applies layers [starts[i], starts[i] + layers[i])
+ * on tiles of 2^tile_cols_log[i] contiguous columns (0 for the bottom pass). */
+int vx_ntt_plan(uint32_t total, uint32_t bottom_max, uint32_t upper_max, uint32_t starts[32], uint32_t layers[32],
+                uint32_t tile_cols_log[32], uint32_t *n_passes);
+
 /* Whole proof without any device allocation — no counterpart in the
  * reference.  For callers that may not allocate device memory: code inside a
  * stream capture or CUDA-graph construction, hosts whose device memory is

@@ -89,6 +89,10 @@ _SIGS = {
     "vx_probe_blake2s": ([u32, u32, u32, vp, vp], C.c_int),
     "vx_tree_plan": ([u32, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32), C.POINTER(u32),
                       C.POINTER(C.c_uint64)], C.c_int),
+    "vx_autotune": ([u32, C.c_char_p, C.c_size_t], C.c_int),
+    "vx_tune_set": ([u32, u32, u32, u32], C.c_int),
+    "vx_tune_get": ([u32, u32, C.POINTER(u32), C.POINTER(u32)], C.c_int),
+    "vx_ntt_plan": ([u32, u32, u32, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32), C.POINTER(u32)], C.c_int),
     "vx_prover_proof_device": ([vp, C.POINTER(vp), C.POINTER(C.c_size_t)], C.c_int),
     "vx_prover_check": ([vp], C.c_int),
     "vx_prove_fib": ([u32, u32, u32, u32, u32, vp, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),

@@ -474,10 +474,14 @@ extern "C" int vx_lifted_create(uint32_t n_cols, const uint32_t *log_sizes, uint
     uint64_t o_C = w; w += 4 * align64(1ull << S);
     uint64_t o_F[kMaxFri];
     for (uint32_t k = 0; k < L.nfri; k++) { o_F[k] = w; w += 4 * align64(1ull << (S - 1 - k)); }
-    const uint64_t o_t0 = w; w += align64(tree_pool_words(S));
-    const uint64_t o_t1 = w; w += align64(tree_pool_words(S));
+    // leaf-kernel shapes read once: the pools are sized and carved with them
+    const uint32_t kt = tree_leaf_k(S);
+    uint32_t kf[kMaxFri];
+    for (uint32_t k = 0; k < L.nfri; k++) kf[k] = tree_leaf_k(S - 1 - k);
+    const uint64_t o_t0 = w; w += align64(tree_pool_words(S, kt));
+    const uint64_t o_t1 = w; w += align64(tree_pool_words(S, kt));
     uint64_t o_ft[kMaxFri];
-    for (uint32_t k = 0; k < L.nfri; k++) { o_ft[k] = w; w += align64(tree_pool_words(S - 1 - k)); }
+    for (uint32_t k = 0; k < L.nfri; k++) { o_ft[k] = w; w += align64(tree_pool_words(S - 1 - k, kf[k])); }
     const uint64_t o_ch = w; w += align64(sizeof(DevChannel) / 4 + 1);
     const uint64_t o_al = w; w += align64(4);
     const uint64_t o_af = w; w += align64(4ull * (L.nfri + 1));
@@ -502,9 +506,9 @@ extern "C" int vx_lifted_create(uint32_t n_cols, const uint32_t *log_sizes, uint
     for (int c = 0; c < 4; c++) h->C[c] = b + o_C + c * align64(1ull << S);
     for (uint32_t k = 0; k < L.nfri; k++)
         for (int c = 0; c < 4; c++) h->F[k][c] = b + o_F[k] + c * align64(1ull << (S - 1 - k));
-    tree_plan(S, b + o_t0, &h->lv0);
-    tree_plan(S, b + o_t1, &h->lv1);
-    for (uint32_t k = 0; k < L.nfri; k++) tree_plan(S - 1 - k, b + o_ft[k], &h->flv[k]);
+    tree_plan(S, b + o_t0, &h->lv0, kt);
+    tree_plan(S, b + o_t1, &h->lv1, kt);
+    for (uint32_t k = 0; k < L.nfri; k++) tree_plan(S - 1 - k, b + o_ft[k], &h->flv[k], kf[k]);
     h->chan = (DevChannel *)(b + o_ch);
     h->alpha = b + o_al;
     h->alpha_f = b + o_af;

@@ -1,4 +1,6 @@
 // Merkle kernels that are not templated on a leaf source, plus tree planning.
+#include <cstring>
+
 #include "vx_common.cuh"
 #include "vx_merkle.cuh"
 
@@ -12,7 +14,32 @@ __global__ void __launch_bounds__(256) node_subtree_kernel(const uint32_t *in, u
     store_hash(out + 8ull * t, h);
 }
 
-uint64_t tree_plan(uint32_t depth, uint32_t *pool, TreeLevels *lv) {
+namespace {
+// Leaf-kernel subtree size (log2 leaves per thread, 1..4) per device and tree
+// depth, written by the autotuner; 0 = the default rule.
+uint8_t g_leaf_k[64][32];
+bool g_leaf_k_init[64] = {false};
+}  // namespace
+
+void tree_knob_set(int dev, uint32_t depth, uint32_t k) {
+    if (dev < 0 || dev >= 64 || depth >= 32 || k > 4) return;
+    if (!g_leaf_k_init[dev]) {
+        memset(g_leaf_k[dev], 0, sizeof(g_leaf_k[dev]));
+        g_leaf_k_init[dev] = true;
+    }
+    g_leaf_k[dev][depth] = (uint8_t)k;
+}
+
+uint32_t tree_leaf_k(uint32_t depth) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && g_leaf_k_init[dev] && depth < 32 && g_leaf_k[dev][depth]) return g_leaf_k[dev][depth];
+    // default: 2^k leaves per thread, k = 1..4, at least 2^16 threads
+    int k = (int)depth - 17;
+    return (uint32_t)(k < 1 ? 1 : (k > 4 ? 4 : k));
+}
+
+uint64_t tree_plan(uint32_t depth, uint32_t *pool, TreeLevels *lv, uint32_t leaf_k) {
     lv->n = 1;
     lv->height[0] = 0;
     lv->hashes[0] = nullptr;
@@ -26,10 +53,7 @@ uint64_t tree_plan(uint32_t depth, uint32_t *pool, TreeLevels *lv) {
     uint32_t h = 0;
     lv->top = 0;
     if (depth > 16) {
-        // leaf kernel: 2^k leaves per thread, k = 1..4, at least 2^16 threads
-        int k = (int)depth - 17;
-        k = k < 1 ? 1 : (k > 4 ? 4 : k);
-        h = (uint32_t)k;
+        h = (leaf_k >= 1 && leaf_k <= 4) ? leaf_k : tree_leaf_k(depth);  // leaf kernel: 2^h leaves per thread
         add(h);
         while (depth - h > 20) { h += 4; add(h); }  // node kernels, 16 -> 1
         lv->top = lv->n - 1;
@@ -52,9 +76,9 @@ uint64_t tree_plan(uint32_t depth, uint32_t *pool, TreeLevels *lv) {
     return used;
 }
 
-uint64_t tree_pool_words(uint32_t depth) {
+uint64_t tree_pool_words(uint32_t depth, uint32_t leaf_k) {
     TreeLevels lv;
-    return tree_plan(depth, nullptr, &lv);
+    return tree_plan(depth, nullptr, &lv, leaf_k);
 }
 
 cudaError_t tree_reset(const TreeLevels &lv, cudaStream_t stream) {
@@ -95,7 +119,7 @@ extern "C" int vx_tree_plan(uint32_t depth, uint32_t heights[12], uint32_t *n_le
     VX_CHECK_ARG(depth >= 1 && depth <= 31, "vx_tree_plan: depth %u outside 1..31", depth);
     VX_CHECK_ARG(heights && n_levels && top && n_counters && pool_words, "vx_tree_plan: null output");
     vx::TreeLevels lv;
-    uint64_t w = vx::tree_plan(depth, nullptr, &lv);
+    uint64_t w = vx::tree_plan(depth, nullptr, &lv, 0);
     for (uint32_t i = 0; i < 12; i++) heights[i] = i < lv.n ? lv.height[i] : 0u;
     *n_levels = lv.n;
     *top = lv.top;

@@ -278,8 +278,17 @@ struct TreeLevels {
 constexpr uint32_t kStageLog = 8;        // levels per reduce stage (256 hashes per block)
 constexpr uint32_t kReduceThreads = 128;
 
-uint64_t tree_plan(uint32_t depth, uint32_t *pool, TreeLevels *lv);
-uint64_t tree_pool_words(uint32_t depth);
+// Carve the stored levels and counters of a 2^depth-leaf tree from `pool`
+// (null: size only); returns the words used.  Trees deeper than 16 start
+// with the leaf kernel hashing 2^leaf_k leaves per thread (1..4; 0 = the
+// current device's choice, tree_leaf_k).  A layout that sizes a pool and
+// carves it later passes the same leaf_k to both calls.
+uint64_t tree_plan(uint32_t depth, uint32_t *pool, TreeLevels *lv, uint32_t leaf_k);
+uint64_t tree_pool_words(uint32_t depth, uint32_t leaf_k);
+// Leaf-kernel subtree size (log2 of leaves per thread) for trees of this
+// depth on the current device, and the autotuner's override (1..4; 0 resets).
+uint32_t tree_leaf_k(uint32_t depth);
+void tree_knob_set(int dev, uint32_t depth, uint32_t k);
 // Zero the group counters of a freshly carved tree.
 cudaError_t tree_reset(const TreeLevels &lv, cudaStream_t stream);
 

@@ -1,4 +1,6 @@
 // Circle NTT passes for sm_100a (see vx_ntt.cuh for the layout).
+#include <cstring>
+
 #include "vx_ntt.cuh"
 #include "vx_field.cuh"
 #include "vx_common.cuh"
@@ -299,20 +301,45 @@ void ntt_table_offsets(uint32_t log_n, uint32_t off[32]) {
     for (uint32_t l = 0; l < 32; l++) off[l] = (l + 1 < log_n) ? (uint32_t)(m - (m >> l)) : 0u;
 }
 
-// Pass plan for `total` layers (0 .. total-1): a bottom pass of up to 12
-// layers on contiguous tiles (WL = 0), then passes of 3..9 layers, sizes
-// balanced, on tiles of 2^(12-R) contiguous columns (every tile 4096
-// elements; rows of at least 8 words = one 32-byte sector).  Transforms of
-// fewer than 4 layers use the one-tile shared-memory kernel.
-static uint32_t plan_passes(uint32_t total, uint32_t ps[32], uint32_t pr[32], uint32_t pw[32]) {
+namespace {
+
+// Pass-plan knobs per device and transform length (in layers): the bottom
+// pass's maximum layers (10..12) and the upper passes' maximum (6..9).  The
+// autotuner writes them; every choice computes the same values.
+struct PlanKnobs { uint8_t bottom, upper; };
+PlanKnobs g_knobs[64][32];
+bool g_knobs_init[64] = {false};
+
+PlanKnobs knobs_for(uint32_t total) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    PlanKnobs k{12, 9};
+    if (dev >= 0 && dev < 64 && g_knobs_init[dev] && total < 32 && g_knobs[dev][total].bottom) k = g_knobs[dev][total];
+    return k;
+}
+
+}  // namespace
+
+// Pass plan for `total` layers (0 .. total-1): a bottom pass of up to
+// `bottom` layers on contiguous tiles (WL = 0), then passes of 3..`upper`
+// layers, sizes balanced, on tiles of 2^(12-R) contiguous columns (every tile
+// 4096 elements; rows of at least 8 words = one 32-byte sector).  An upper
+// pass starting at layer s reads rows 2^s apart, so its 2^(12-R) columns
+// must fit in one row gap: 12 - R <= s.  Transforms of at most 12 layers are
+// therefore one bottom pass, and a longer one keeps a bottom pass of at
+// least 9 layers (bottom_max >= 9; at least 10 after the 3-layer rule).
+// Transforms of fewer than 4 layers use the one-tile shared-memory kernel.
+uint32_t ntt_plan(uint32_t total, uint32_t bottom_max, uint32_t upper_max, uint32_t ps[32], uint32_t pr[32],
+                  uint32_t pw[32]) {
     uint32_t np = 0;
-    uint32_t bottom = total < 12u ? total : 12u;
-    if (total > 12u && total < 15u) bottom = total - 3u;  // leave at least 3 layers above
+    if (bottom_max < 9u) bottom_max = 9u;
+    uint32_t bottom = (total <= 12u || total < bottom_max) ? total : bottom_max;
+    if (total > bottom && total - bottom < 3u) bottom = total - 3u;  // leave at least 3 layers above
     ps[np] = 0; pr[np] = bottom; pw[np] = 0; np++;
     uint32_t rest = total - bottom;
     if (rest) {
-        uint32_t nu = (rest + 8u) / 9u;
-        if (rest < 3u * nu) nu = rest / 3u;  // every upper pass has 3..9 layers
+        uint32_t nu = (rest + upper_max - 1u) / upper_max;
+        if (rest < 3u * nu) nu = rest / 3u;  // every upper pass has at least 3 layers
         uint32_t lo = bottom;
         for (uint32_t i = 0; i < nu; i++) {
             uint32_t r = rest / nu + (i < rest % nu ? 1u : 0u);
@@ -322,6 +349,28 @@ static uint32_t plan_passes(uint32_t total, uint32_t ps[32], uint32_t pr[32], ui
     }
     return np;
 }
+
+void ntt_knobs_set(int dev, uint32_t total, uint32_t bottom, uint32_t upper) {
+    if (dev < 0 || dev >= 64 || total >= 32) return;
+    if (!g_knobs_init[dev]) {
+        memset(g_knobs[dev], 0, sizeof(g_knobs[dev]));
+        g_knobs_init[dev] = true;
+    }
+    g_knobs[dev][total] = PlanKnobs{(uint8_t)bottom, (uint8_t)upper};
+}
+
+void ntt_knobs_get(uint32_t total, uint32_t *bottom, uint32_t *upper) {
+    PlanKnobs k = knobs_for(total);
+    *bottom = k.bottom;
+    *upper = k.upper;
+}
+
+namespace {
+uint32_t plan_passes(uint32_t total, uint32_t ps[32], uint32_t pr[32], uint32_t pw[32]) {
+    PlanKnobs k = knobs_for(total);
+    return ntt_plan(total, k.bottom, k.upper, ps, pr, pw);
+}
+}  // namespace
 
 uint32_t ntt_pass_count(uint32_t layers) {
     if (layers == 0) return 0;
@@ -333,6 +382,12 @@ uint32_t ntt_pass_count(uint32_t layers) {
 cudaError_t ntt_transform(uint32_t *data, uint32_t *const *dev_cols, uint64_t col_stride, uint32_t n_cols,
                           uint32_t log_n, const NttTables &tw, bool forward, const uint32_t *src,
                           uint32_t src_log, cudaStream_t stream) {
+    return ntt_transform_planned(data, dev_cols, col_stride, n_cols, log_n, tw, forward, src, src_log, 0, 0, stream);
+}
+
+cudaError_t ntt_transform_planned(uint32_t *data, uint32_t *const *dev_cols, uint64_t col_stride, uint32_t n_cols,
+                                  uint32_t log_n, const NttTables &tw, bool forward, const uint32_t *src,
+                                  uint32_t src_log, uint32_t bottom_max, uint32_t upper_max, cudaStream_t stream) {
     if (log_n == 0 || n_cols == 0) return cudaSuccess;
     if (src && !forward && src_log != log_n) return cudaErrorInvalidValue;
     cudaError_t e = ensure_attrs();
@@ -359,7 +414,7 @@ cudaError_t ntt_transform(uint32_t *data, uint32_t *const *dev_cols, uint64_t co
         return cudaGetLastError();
     }
     uint32_t ps[32], pr[32], pw[32];
-    const uint32_t np = plan_passes(total, ps, pr, pw);
+    const uint32_t np = bottom_max ? ntt_plan(total, bottom_max, upper_max, ps, pr, pw) : plan_passes(total, ps, pr, pw);
     for (uint32_t q = 0; q < np; q++) {
         uint32_t i = forward ? np - 1u - q : q;   // forward: top pass first
         Pass2Args a;

@@ -37,8 +37,25 @@ cudaError_t ntt_transform(uint32_t *data, uint32_t *const *dev_cols, uint64_t co
                           uint32_t log_n, const NttTables &tw, bool forward, const uint32_t *src,
                           uint32_t src_log, cudaStream_t stream);
 
+// ntt_transform with an explicit pass plan (ntt_plan's bottom_max / upper_max;
+// 0 = the device's current choice).
+cudaError_t ntt_transform_planned(uint32_t *data, uint32_t *const *dev_cols, uint64_t col_stride, uint32_t n_cols,
+                                  uint32_t log_n, const NttTables &tw, bool forward, const uint32_t *src,
+                                  uint32_t src_log, uint32_t bottom_max, uint32_t upper_max, cudaStream_t stream);
+
 // Kernel launches of a transform that applies `layers` layers.
 uint32_t ntt_pass_count(uint32_t layers);
+
+// Pass plan of a `total`-layer transform for a bottom pass of at most
+// bottom_max (9..12) layers and upper passes of at most upper_max (3..9):
+// pass i covers layers [ps[i], ps[i] + pr[i]) on tiles with 2^pw[i] columns.
+// Transforms of at most 12 layers are one pass.
+uint32_t ntt_plan(uint32_t total, uint32_t bottom_max, uint32_t upper_max, uint32_t ps[32], uint32_t pr[32],
+                  uint32_t pw[32]);
+// Per-device plan choice for `total`-layer transforms (default 12 / 9);
+// every choice computes the same values.
+void ntt_knobs_set(int dev, uint32_t total, uint32_t bottom_max, uint32_t upper_max);
+void ntt_knobs_get(uint32_t total, uint32_t *bottom_max, uint32_t *upper_max);
 
 // One butterfly layer over the whole array (reference cuda_circle_ntt_layer).
 cudaError_t ntt_single_layer(uint32_t *data, const uint32_t *tw, uint32_t layer_idx, uint32_t log_n, bool forward,

@@ -423,10 +423,14 @@ extern "C" int vx_prover_create(uint32_t log_n, uint32_t blowup_bits, uint32_t n
     uint64_t o_eval = w; w += align_words(N);
     uint64_t o_fri[32];
     for (uint32_t k = 0; k < L.nfri; k++) { o_fri[k] = w; w += 4 * align_words(1ull << (le - 1 - k)); }
-    uint64_t o_tt = w; w += align_words(tree_pool_words(le));
-    uint64_t o_qt = w; w += align_words(tree_pool_words(le));
+    // leaf-kernel shapes read once: the pools are sized and carved with them
+    const uint32_t kt = tree_leaf_k(le);
+    uint32_t kf[32];
+    for (uint32_t k = 0; k < L.nfri; k++) kf[k] = tree_leaf_k(le - 1 - k);
+    uint64_t o_tt = w; w += align_words(tree_pool_words(le, kt));
+    uint64_t o_qt = w; w += align_words(tree_pool_words(le, kt));
     uint64_t o_ft[32];
-    for (uint32_t k = 0; k < L.nfri; k++) { o_ft[k] = w; w += align_words(tree_pool_words(le - 1 - k)); }
+    for (uint32_t k = 0; k < L.nfri; k++) { o_ft[k] = w; w += align_words(tree_pool_words(le - 1 - k, kf[k])); }
     uint64_t o_chan = w; w += align_words(sizeof(DevChannel) / 4 + 1);
     uint64_t o_aq = w; w += align_words(4);
     uint64_t o_af = w; w += align_words(4ull * (L.nfri + 1));
@@ -449,9 +453,9 @@ extern "C" int vx_prover_create(uint32_t log_n, uint32_t blowup_bits, uint32_t n
         uint64_t sz = align_words(1ull << (le - 1 - k));
         for (int c = 0; c < 4; c++) S.fri[k][c] = b + o_fri[k] + c * sz;
     }
-    tree_plan(le, b + o_tt, &S.trace_lv);
-    tree_plan(le, b + o_qt, &S.quot_lv);
-    for (uint32_t k = 0; k < L.nfri; k++) tree_plan(le - 1 - k, b + o_ft[k], &S.fri_lv[k]);
+    tree_plan(le, b + o_tt, &S.trace_lv, kt);
+    tree_plan(le, b + o_qt, &S.quot_lv, kt);
+    for (uint32_t k = 0; k < L.nfri; k++) tree_plan(le - 1 - k, b + o_ft[k], &S.fri_lv[k], kf[k]);
     S.chan = (DevChannel *)(b + o_chan);
     S.alpha_q = b + o_aq;
     S.alpha_f = b + o_af;
@@ -779,9 +783,9 @@ extern "C" int vx_prove_fib_noalloc(uint32_t a, uint32_t b, uint32_t log_n, uint
         for (int c = 0; c < 4; c++) S.fri[k][c] = base + w + c * sz;
         w += 4 * sz;
     }
-    w += align_words(tree_plan(le, base + w, &S.trace_lv));
-    w += align_words(tree_plan(le, base + w, &S.quot_lv));
-    for (uint32_t k = 0; k < L.nfri; k++) w += align_words(tree_plan(le - 1 - k, base + w, &S.fri_lv[k]));
+    w += align_words(tree_plan(le, base + w, &S.trace_lv, 0));
+    w += align_words(tree_plan(le, base + w, &S.quot_lv, 0));
+    for (uint32_t k = 0; k < L.nfri; k++) w += align_words(tree_plan(le - 1 - k, base + w, &S.fri_lv[k], 0));
     S.chan = (DevChannel *)(base + w); w += align_words(sizeof(DevChannel) / 4 + 1);
     S.alpha_q = base + w; w += align_words(4);
     S.alpha_f = base + w; w += align_words(4ull * (L.nfri + 1));
@@ -887,8 +891,8 @@ void prover_footprint(uint32_t log_n, uint32_t blowup, uint32_t nq, size_t *slot
     uint64_t n = 1ull << log_n, N = 1ull << le;
     uint64_t w = align_words(n) + align_words(N);
     for (uint32_t k = 0; k < L.nfri; k++) w += 4 * align_words(1ull << (le - 1 - k));
-    w += 2 * align_words(tree_pool_words(le));
-    for (uint32_t k = 0; k < L.nfri; k++) w += align_words(tree_pool_words(le - 1 - k));
+    w += 2 * align_words(tree_pool_words(le, 0));
+    for (uint32_t k = 0; k < L.nfri; k++) w += align_words(tree_pool_words(le - 1 - k, 0));
     w += align_words(sizeof(DevChannel) / 4 + 1) + align_words(4) + align_words(4ull * (L.nfri + 1)) +
          align_words(nq) + align_words(L.words);
     *slot_b = (size_t)(w * 4);

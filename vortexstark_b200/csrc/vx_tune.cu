@@ -1,0 +1,168 @@
+// Autotuner: picks, per device, the NTT pass plan of every transform length
+// and the Merkle leaf-kernel subtree size of every tree depth by timing the
+// candidates on scratch buffers of that size.  The knobs only change how the
+// work is split into launches and threads; every choice computes the same
+// values (the tests prove each plan against the oracle), so proofs stay
+// byte-identical whatever the tuner picks.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "vx_common.cuh"
+#include "vx_merkle.cuh"
+#include "vx_ntt.cuh"
+
+using namespace vx;
+
+namespace {
+
+struct Scratch {
+    void *p = nullptr;
+    ~Scratch() { if (p) cudaFree(p); }
+};
+
+// Median of `reps` timed runs of fn on `st` after two untimed ones.
+template <class F>
+float time_ms(F fn, cudaStream_t st, int reps, cudaError_t *err) {
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    std::vector<float> t;
+    for (int r = 0; r < reps + 2 && *err == cudaSuccess; r++) {
+        cudaEventRecord(a, st);
+        *err = fn();
+        cudaEventRecord(b, st);
+        cudaEventSynchronize(b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        if (r >= 2) t.push_back(ms);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (t.empty()) return 1e30f;
+    std::sort(t.begin(), t.end());
+    return t[t.size() / 2];
+}
+
+}  // namespace
+
+extern "C" int vx_tune_set(uint32_t kind, uint32_t layers, uint32_t a, uint32_t b) {
+    int dev = 0;
+    VX_CUDA_TRY(cudaGetDevice(&dev));
+    VX_CHECK_ARG(layers < 32, "vx_tune_set: layers %u >= 32", layers);
+    if (kind == 0) {
+        // a = 0 restores the default; a bottom pass of at least 9 layers lets
+        // every upper pass's columns fit between its rows
+        VX_CHECK_ARG(a == 0 || (a >= 9 && a <= 12 && b >= 3 && b <= 9),
+                     "vx_tune_set: NTT plan needs bottom 9..12 and upper 3..9 (or 0 for the default)");
+        ntt_knobs_set(dev, layers, a, b);
+    } else if (kind == 1) {
+        VX_CHECK_ARG(a <= 4, "vx_tune_set: leaf subtree log must be 0 (default) .. 4");
+        tree_knob_set(dev, layers, a);
+    } else {
+        VX_CHECK_ARG(false, "vx_tune_set: kind %u is not 0 (NTT plan) or 1 (leaf subtree)", kind);
+    }
+    return VX_OK;
+}
+
+extern "C" int vx_tune_get(uint32_t kind, uint32_t layers, uint32_t *a, uint32_t *b) {
+    VX_CHECK_ARG(a != nullptr && b != nullptr && layers < 32, "vx_tune_get: bad arguments");
+    if (kind == 0) {
+        ntt_knobs_get(layers, a, b);
+    } else if (kind == 1) {
+        *a = tree_leaf_k(layers);
+        *b = 0;
+    } else {
+        VX_CHECK_ARG(false, "vx_tune_get: kind %u is not 0 or 1", kind);
+    }
+    return VX_OK;
+}
+
+extern "C" int vx_ntt_plan(uint32_t total, uint32_t bottom_max, uint32_t upper_max, uint32_t starts[32],
+                           uint32_t layers[32], uint32_t tile_cols_log[32], uint32_t *n_passes) {
+    VX_CHECK_ARG(total >= 4 && total <= 31, "vx_ntt_plan: total %u outside 4..31", total);
+    VX_CHECK_ARG(bottom_max >= 9 && bottom_max <= 12 && upper_max >= 3 && upper_max <= 9,
+                 "vx_ntt_plan: bottom 9..12 and upper 3..9");
+    VX_CHECK_ARG(starts && layers && tile_cols_log && n_passes, "vx_ntt_plan: null output");
+    *n_passes = ntt_plan(total, bottom_max, upper_max, starts, layers, tile_cols_log);
+    return VX_OK;
+}
+
+extern "C" int vx_autotune(uint32_t max_log, char *report, size_t cap) {
+    VX_CHECK_ARG(max_log >= 12 && max_log <= 28, "vx_autotune: max_log %u outside 12..28", max_log);
+    int dev = 0;
+    VX_CUDA_TRY(cudaGetDevice(&dev));
+    const uint64_t n = 1ull << max_log;
+    // data (n words), line + circle tables (2n words), a Merkle pool (the
+    // largest is the one with one leaf pair per thread)
+    const uint64_t pool_max = tree_pool_words(max_log, 1);
+    Scratch sc;
+    const uint64_t words = 3 * n + pool_max + 64;
+    VX_CUDA_TRY(cudaMalloc(&sc.p, words * 4));
+    uint32_t *data = (uint32_t *)sc.p, *tab = data + n, *pool = tab + 2 * n;
+    VX_CUDA_TRY(cudaMemset(sc.p, 0, words * 4));
+    cudaStream_t st = nullptr;
+    cudaError_t err = cudaSuccess;
+    std::string js = "{\"ntt\":{";
+    // ---- NTT pass plans ----
+    for (uint32_t total = 13; total <= max_log && err == cudaSuccess; total++) {  // <= 12: one pass
+        NttTables tw{tab, tab + n, {}, 0u};
+        ntt_table_offsets(total, tw.off);
+        float best = 1e30f;
+        uint32_t bb = 12, bu = 9;
+        std::vector<std::vector<uint32_t>> seen;
+        for (uint32_t bottom = 10; bottom <= 12; bottom++)
+            for (uint32_t upper = 6; upper <= 9; upper++) {
+                uint32_t ps[32], pr[32], pw[32];
+                uint32_t np = ntt_plan(total, bottom, upper, ps, pr, pw);
+                std::vector<uint32_t> key(pr, pr + np);
+                if (std::find(seen.begin(), seen.end(), key) != seen.end()) continue;  // same plan
+                seen.push_back(key);
+                float ms = time_ms(
+                    [&] {
+                        return ntt_transform_planned(data, nullptr, 0, 1, total, tw, true, nullptr, 0, bottom, upper, st);
+                    },
+                    st, 3, &err);
+                if (ms < best) { best = ms; bb = bottom; bu = upper; }
+            }
+        ntt_knobs_set(dev, total, bb, bu);
+        char buf[96];
+        snprintf(buf, sizeof(buf), "%s\"%u\":[%u,%u,%.4f]", total == 13 ? "" : ",", total, bb, bu, best);
+        js += buf;
+    }
+    js += "},\"leaf_k\":{";
+    // ---- Merkle leaf-subtree sizes ----
+    for (uint32_t depth = 17; depth <= max_log && err == cudaSuccess; depth++) {
+        float best = 1e30f;
+        uint32_t bk = 0;
+        for (uint32_t k = 1; k <= 4; k++) {
+            if (depth - k < 13) continue;  // keep at least 2^13 threads
+            TreeLevels lv;
+            tree_plan(depth, pool, &lv, k);
+            if ((err = tree_reset(lv, st)) != cudaSuccess) break;
+            float ms = time_ms([&] { return tree_build(LeafM31{data}, lv, ChanStep{nullptr, nullptr, nullptr}, st); },
+                               st, 3, &err);
+            if (ms < best) { best = ms; bk = k; }
+        }
+        tree_knob_set(dev, depth, bk);
+        char buf[96];
+        snprintf(buf, sizeof(buf), "%s\"%u\":[%u,%.4f]", depth == 17 ? "" : ",", depth, bk, best);
+        js += buf;
+    }
+    js += "}}";
+    if (err != cudaSuccess) {
+        for (uint32_t l = 0; l < 32; l++) {  // back to the defaults
+            ntt_knobs_set(dev, l, 0, 0);
+            tree_knob_set(dev, l, 0);
+        }
+        set_last_error(VX_ERR_CUDA, "vx_autotune: %s", cudaGetErrorString(err));
+        return VX_ERR_CUDA;
+    }
+    if (report && cap) {
+        strncpy(report, js.c_str(), cap - 1);
+        report[cap - 1] = 0;
+    }
+    return VX_OK;
+}
