@@ -112,7 +112,8 @@ __global__ void permute_kernel(const uint32_t *src, uint32_t *dst, uint64_t n, u
 
 // ---- Merkle helpers ----
 template <class Src>
-__global__ void leaf_hash_kernel(Src src, uint32_t *hashes, uint64_t n) {
+// `one` (always 1): pipe balance of the Blake2s compression.
+__global__ void leaf_hash_kernel(Src src, uint32_t *hashes, uint64_t n, uint32_t one) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     src.init();
@@ -121,11 +122,11 @@ __global__ void leaf_hash_kernel(Src src, uint32_t *hashes, uint64_t n) {
     for (int w = 0; w < 16; w++) m[w] = 0u;
     uint32_t nb = src.load(i, m);
     uint32_t h[8];
-    blake2s_block(h, m, nb);
+    blake2s_block(h, m, nb, one);
     store_hash(hashes + 8 * i, h);
 }
 
-__global__ void node_hash_kernel(const uint32_t *children, uint32_t *parents, uint64_t n) {
+__global__ void node_hash_kernel(const uint32_t *children, uint32_t *parents, uint64_t n, uint32_t one) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     uint32_t m[16];
@@ -134,7 +135,7 @@ __global__ void node_hash_kernel(const uint32_t *children, uint32_t *parents, ui
     m[0] = a.x; m[1] = a.y; m[2] = a.z; m[3] = a.w; m[4] = b.x; m[5] = b.y; m[6] = b.z; m[7] = b.w;
     m[8] = d.x; m[9] = d.y; m[10] = d.z; m[11] = d.w; m[12] = e.x; m[13] = e.y; m[14] = e.z; m[15] = e.w;
     uint32_t h[8];
-    blake2s_block(h, m, 64u);
+    blake2s_block(h, m, 64u, one);
     store_hash(parents + 8 * i, h);
 }
 
@@ -163,12 +164,12 @@ __global__ void reduce_to_root_kernel(const uint32_t *nodes, uint32_t *root, uin
 // Tile of 2^tile_log leaves per block, 2^(tile_log-4) threads each hashing
 // 16 leaves into a subtree root, then a shared-memory reduction.
 template <class Src>
-__global__ void tile_root_kernel(Src src, uint32_t *roots, uint32_t tile_log) {
+__global__ void tile_root_kernel(Src src, uint32_t *roots, uint32_t tile_log, uint32_t one) {
     extern __shared__ uint32_t sh[];
     src.init();
     uint64_t base = ((uint64_t)blockIdx.x << tile_log) + ((uint64_t)threadIdx.x << 4);
     uint32_t h[8];
-    subtree_root(src, base, 4, h);
+    subtree_root(src, base, 4, h, one);
     for (int w = 0; w < 8; w++) sh[8 * threadIdx.x + w] = h[w];
     __syncthreads();
     block_reduce_hashes(sh, blockDim.x);
@@ -199,19 +200,19 @@ __global__ void abi_small_tree_kernel(Src src, uint32_t *root, uint32_t n) {
 }
 
 template <class Src>
-__global__ void leaf_merge_kernel(Src src, uint32_t *parents, uint64_t n_pairs) {
+__global__ void leaf_merge_kernel(Src src, uint32_t *parents, uint64_t n_pairs, uint32_t one) {
     uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n_pairs) return;
     src.init();
     uint32_t l[8], r[8], m[16];
     for (int w = 0; w < 16; w++) m[w] = 0u;
     uint32_t nb = src.load(2 * t, m);
-    blake2s_block(l, m, nb);
+    blake2s_block(l, m, nb, one);
     for (int w = 0; w < 16; w++) m[w] = 0u;
     nb = src.load(2 * t + 1, m);
-    blake2s_block(r, m, nb);
+    blake2s_block(r, m, nb, one);
     uint32_t h[8];
-    blake2s_node(h, l, r);
+    blake2s_node(h, l, r, one);
     store_hash(parents + 8 * t, h);
 }
 
@@ -459,23 +460,23 @@ void cuda_fibonacci_quotient(const uint32_t *tr, uint32_t *o0, uint32_t *o1, uin
 
 // ---------------- Merkle ----------------
 void cuda_merkle_hash_leaves(const uint32_t *const *cols, uint32_t *hashes, uint32_t n_cols, uint32_t n_leaves) {
-    leaf_hash_kernel<<<blocks_for(n_leaves, 128), 128>>>(LeafCols{cols, n_cols}, hashes, n_leaves);
+    leaf_hash_kernel<<<blocks_for(n_leaves, 128), 128>>>(LeafCols{cols, n_cols}, hashes, n_leaves, 1u);
     VX_LAUNCH_CHECK();
 }
 
 void cuda_merkle_hash_leaves_forge_single(const uint32_t *col, uint32_t *hashes, uint32_t n_leaves) {
-    leaf_hash_kernel<<<blocks_for(n_leaves, 128), 128>>>(LeafM31{col}, hashes, n_leaves);
+    leaf_hash_kernel<<<blocks_for(n_leaves, 128), 128>>>(LeafM31{col}, hashes, n_leaves, 1u);
     VX_LAUNCH_CHECK();
 }
 
 void cuda_merkle_hash_leaves_forge_quad(const uint32_t *c0, const uint32_t *c1, const uint32_t *c2,
                                         const uint32_t *c3, uint32_t *hashes, uint32_t n_leaves) {
-    leaf_hash_kernel<<<blocks_for(n_leaves, 128), 128>>>(LeafSoA4{c0, c1, c2, c3}, hashes, n_leaves);
+    leaf_hash_kernel<<<blocks_for(n_leaves, 128), 128>>>(LeafSoA4{c0, c1, c2, c3}, hashes, n_leaves, 1u);
     VX_LAUNCH_CHECK();
 }
 
 void cuda_merkle_hash_nodes(const uint32_t *children, uint32_t *parents, uint32_t n_parents) {
-    node_hash_kernel<<<blocks_for(n_parents, 128), 128>>>(children, parents, n_parents);
+    node_hash_kernel<<<blocks_for(n_parents, 128), 128>>>(children, parents, n_parents, 1u);
     VX_LAUNCH_CHECK();
 }
 
@@ -497,7 +498,7 @@ void cuda_merkle_commit_small_soa4(const uint32_t *c0, const uint32_t *c1, const
 void cuda_merkle_hash_leaves_merge_soa4(const uint32_t *c0, const uint32_t *c1, const uint32_t *c2,
                                         const uint32_t *c3, uint32_t *parents, uint32_t n_leaves) {
     uint64_t pairs = n_leaves / 2;
-    leaf_merge_kernel<<<blocks_for(pairs, 128), 128>>>(LeafSoA4{c0, c1, c2, c3}, parents, pairs);
+    leaf_merge_kernel<<<blocks_for(pairs, 128), 128>>>(LeafSoA4{c0, c1, c2, c3}, parents, pairs, 1u);
     VX_LAUNCH_CHECK();
 }
 
@@ -505,7 +506,7 @@ void cuda_merkle_tiled_soa4_stream(const uint32_t *c0, const uint32_t *c1, const
                                    uint32_t *roots, uint32_t n_leaves, void *stream) {
     uint32_t tiles = n_leaves / 1024u;
     if (!tiles) return;
-    tile_root_kernel<<<tiles, 64, 64 * 32, (cudaStream_t)stream>>>(LeafSoA4{c0, c1, c2, c3}, roots, 10u);
+    tile_root_kernel<<<tiles, 64, 64 * 32, (cudaStream_t)stream>>>(LeafSoA4{c0, c1, c2, c3}, roots, 10u, 1u);
     VX_LAUNCH_CHECK();
 }
 
@@ -517,7 +518,7 @@ void cuda_merkle_tiled_soa4(const uint32_t *c0, const uint32_t *c1, const uint32
 void cuda_merkle_tiled_generic(const uint32_t *const *cols, uint32_t *roots, uint32_t n_cols, uint32_t n_leaves) {
     uint32_t tiles = n_leaves / 1024u;
     if (!tiles) return;
-    tile_root_kernel<<<tiles, 64, 64 * 32>>>(LeafCols{cols, n_cols}, roots, 10u);
+    tile_root_kernel<<<tiles, 64, 64 * 32>>>(LeafCols{cols, n_cols}, roots, 10u, 1u);
     VX_LAUNCH_CHECK();
 }
 

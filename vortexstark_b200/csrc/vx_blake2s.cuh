@@ -3,9 +3,19 @@
 // The 16 message words and the 16-word working state live in registers; the
 // message schedule is resolved at compile time by full unrolling, so no
 // message word is ever indexed at run time.  Rotations by 16 and 8 are byte
-// permutes (PRMT), by 12 and 7 funnel shifts (SHF), and a + b + m is one
-// three-input add.  Leaves, nodes and the transcript all use the unkeyed,
-// unpersonalised parameter block (h0 ^= 0x01010020), as the reference does
+// permutes (PRMT), by 12 and 7 funnel shifts (SHF).
+//
+// Pipe balance: the xors and rotations (8 per G) run on the integer ALU
+// pipe, which bounds the compression rate.  a + b + m is written as
+// a + (b * one + m) with `one` a runtime 1 (a kernel parameter, which ptxas
+// cannot fold), so b * one + m can issue as an IMAD on the FMA pipe.
+// Measured on B200 with 16-word messages (tree nodes, wide leaves): 27.5 G
+// compressions/s against 22.7 G with the plain three-input add; leaves with
+// mostly zero words gain ~3%.  Callers that pass no `one` get the literal 1,
+// which folds back to the plain add.
+//
+// Leaves, nodes and the transcript all use the unkeyed, unpersonalised
+// parameter block (h0 ^= 0x01010020), as the reference does
 // (blake2s.cuh:70-136, blake2s.cu:47-60, channel.rs:256-262).
 #pragma once
 #include <cstdint>
@@ -28,11 +38,11 @@ __device__ __forceinline__ uint32_t ror7(uint32_t x) { return __funnelshift_r(x,
 
 #define VX_G(a, b, c, d, x, y)      \
     do {                            \
-        a = a + b + (x);            \
+        a = a + (b * one + (x));    \
         d = ror16(d ^ a);           \
         c = c + d;                  \
         b = ror12(b ^ c);           \
-        a = a + b + (y);            \
+        a = a + (b * one + (y));    \
         d = ror8(d ^ a);            \
         c = c + d;                  \
         b = ror7(b ^ c);            \
@@ -51,7 +61,8 @@ __device__ __forceinline__ uint32_t ror7(uint32_t x) { return __funnelshift_r(x,
     } while (0)
 
 // h[8] <- compress(h, m, t, last).  m is indexed only by literals.
-__device__ __forceinline__ void blake2s_compress(uint32_t h[8], const uint32_t m[16], uint32_t t, bool last) {
+__device__ __forceinline__ void blake2s_compress(uint32_t h[8], const uint32_t m[16], uint32_t t, bool last,
+                                                 uint32_t one = 1u) {
     uint32_t v0 = h[0], v1 = h[1], v2 = h[2], v3 = h[3], v4 = h[4], v5 = h[5], v6 = h[6], v7 = h[7];
     uint32_t v8 = VX_IV0, v9 = VX_IV1, v10 = VX_IV2, v11 = VX_IV3;
     uint32_t v12 = VX_IV4 ^ t, v13 = VX_IV5, v14 = last ? ~VX_IV6 : VX_IV6, v15 = VX_IV7;
@@ -75,17 +86,19 @@ __device__ __forceinline__ void blake2s_init(uint32_t h[8]) {
 }
 
 // One-block hash of `nbytes` (<= 64) already laid out as 16 LE words.
-__device__ __forceinline__ void blake2s_block(uint32_t out[8], const uint32_t m[16], uint32_t nbytes) {
+__device__ __forceinline__ void blake2s_block(uint32_t out[8], const uint32_t m[16], uint32_t nbytes,
+                                              uint32_t one = 1u) {
     blake2s_init(out);
-    blake2s_compress(out, m, nbytes, true);
+    blake2s_compress(out, m, nbytes, true, one);
 }
 
 // Parent of two 8-word children (t = 64, final).
-__device__ __forceinline__ void blake2s_node(uint32_t out[8], const uint32_t l[8], const uint32_t r[8]) {
+__device__ __forceinline__ void blake2s_node(uint32_t out[8], const uint32_t l[8], const uint32_t r[8],
+                                             uint32_t one = 1u) {
     uint32_t m[16];
 #pragma unroll
     for (int i = 0; i < 8; i++) { m[i] = l[i]; m[8 + i] = r[i]; }
-    blake2s_block(out, m, 64u);
+    blake2s_block(out, m, 64u, one);
 }
 
 // General (multi-block) hash of a byte string held in global/shared memory

@@ -46,7 +46,7 @@ __device__ __forceinline__ uint32_t mod_p(uint32_t h) {
 template <bool M31OUT>
 __global__ void __launch_bounds__(256) grind_kernel(Digest8 d, const uint32_t *dptr, unsigned long long *result,
                                                     uint32_t pow_bits, uint64_t base, uint64_t count,
-                                                    uint32_t lowbits) {
+                                                    uint32_t lowbits, uint32_t one) {
     if (dptr) {
 #pragma unroll
         for (int i = 0; i < 8; i++) d.w[i] = __ldg(dptr + i);
@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(256) grind_kernel(Digest8 d, const uint32_t *d
 #pragma unroll
         for (int i = 10; i < 16; i++) m[i] = 0u;
         uint32_t h[8];
-        blake2s_block(h, m, 40u);
+        blake2s_block(h, m, 40u, one);  // one == 1: Blake2s pipe balance
         uint32_t h0 = h[0], h1 = h[1], h2 = h[2], h3 = h[3];
         if (M31OUT) { h0 = mod_p(h0); h1 = mod_p(h1); h2 = mod_p(h2); h3 = mod_p(h3); }
         if (tz128(h0, h1, h2, h3) >= pow_bits) atomicMin(result, (unsigned long long)nonce);
@@ -93,9 +93,9 @@ cudaError_t grind_launch(bool m31, const uint32_t *digest_words, const uint32_t 
     unsigned blocks = grind_blocks();
     if (need < blocks) blocks = (unsigned)(need ? need : 1);
     if (m31)
-        grind_kernel<true><<<blocks, 256, 0, st>>>(d, dptr, result, pow_bits, base, count, lowbits);
+        grind_kernel<true><<<blocks, 256, 0, st>>>(d, dptr, result, pow_bits, base, count, lowbits, 1u);
     else
-        grind_kernel<false><<<blocks, 256, 0, st>>>(d, dptr, result, pow_bits, base, count, lowbits);
+        grind_kernel<false><<<blocks, 256, 0, st>>>(d, dptr, result, pow_bits, base, count, lowbits, 1u);
     return cudaGetLastError();
 }
 

@@ -115,6 +115,7 @@ __device__ __forceinline__ uint32_t reduce34(uint64_t x) {
 // IMAD.WIDE per column and coordinate), folded every 3 columns so the sum
 // stays below 2^34 + 3 * 2^62 < 2^64, and reduced to canonical M31 once.
 struct LeafCombine {
+    static constexpr bool kPlainAdds = true;  // 4 x n_cols wide multiplies per leaf
     LeafLifted cols;
     const uint32_t *pw;  // alpha^c as 4 words each
     uint32_t *o0, *o1, *o2, *o3;

@@ -6,11 +6,12 @@
 
 namespace vx {
 
-__global__ void __launch_bounds__(256) node_subtree_kernel(const uint32_t *in, uint32_t *out, uint64_t n_threads, uint32_t k) {
+__global__ void __launch_bounds__(256) node_subtree_kernel(const uint32_t *in, uint32_t *out, uint64_t n_threads,
+                                                           uint32_t k, uint32_t one) {
     uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n_threads) return;
     uint32_t h[8];
-    node_subtree_root(in, t << k, k, h);
+    node_subtree_root(in, t << k, k, h, one);
     store_hash(out + 8ull * t, h);
 }
 
@@ -91,8 +92,9 @@ cudaError_t tree_reset(const TreeLevels &lv, cudaStream_t stream) {
 namespace vx {
 namespace {
 // Register-only Blake2s chain: the message is the previous digest twice, so
-// every compression depends on the last and nothing touches memory.
-__global__ void __launch_bounds__(256) blake2s_probe_kernel(uint32_t iters, uint32_t *out) {
+// every compression depends on the last and nothing touches memory.  Same
+// pipe-balanced compression (one == 1) as the tree kernels.
+__global__ void __launch_bounds__(256) blake2s_probe_kernel(uint32_t iters, uint32_t *out, uint32_t one) {
     uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t h[8];
     for (int i = 0; i < 8; i++) h[i] = tid * 0x9E3779B9u + i;
@@ -100,7 +102,7 @@ __global__ void __launch_bounds__(256) blake2s_probe_kernel(uint32_t iters, uint
         uint32_t m[16];
 #pragma unroll
         for (int i = 0; i < 8; i++) { m[i] = h[i]; m[8 + i] = h[i] ^ it; }
-        blake2s_block(h, m, 64u);
+        blake2s_block(h, m, 64u, one);
     }
     out[tid] = h[0] ^ h[1] ^ h[2] ^ h[3] ^ h[4] ^ h[5] ^ h[6] ^ h[7];
 }
@@ -109,7 +111,7 @@ __global__ void __launch_bounds__(256) blake2s_probe_kernel(uint32_t iters, uint
 
 extern "C" int vx_probe_blake2s(uint32_t blocks, uint32_t threads, uint32_t iters, uint32_t *out, void *stream) {
     VX_CHECK_ARG(out != nullptr && blocks > 0 && threads > 0 && threads <= 256, "vx_probe_blake2s: bad launch shape");
-    vx::blake2s_probe_kernel<<<blocks, threads, 0, (cudaStream_t)stream>>>(iters, out);
+    vx::blake2s_probe_kernel<<<blocks, threads, 0, (cudaStream_t)stream>>>(iters, out, 1u);
     VX_CUDA_TRY(cudaGetLastError());
     return VX_OK;
 }

@@ -81,16 +81,25 @@ struct is_wide_leaf : std::false_type {};
 template <class Src>
 struct is_wide_leaf<Src, std::void_t<decltype(&Src::digest)>> : std::true_type {};
 
+// Leaf sources whose load is itself multiply-heavy (the FMA pipe is busy)
+// declare `static constexpr bool kPlainAdds = true`; the kernels that hash
+// their leaves (and the nodes above them) then use the plain three-input add.
+template <class Src, class = void>
+struct plain_adds : std::false_type {};
 template <class Src>
-__device__ __forceinline__ void leaf_digest(const Src &src, uint64_t i, uint32_t h[8]) {
+struct plain_adds<Src, std::void_t<decltype(Src::kPlainAdds)>> : std::bool_constant<Src::kPlainAdds> {};
+
+template <class Src>
+__device__ __forceinline__ void leaf_digest(const Src &src, uint64_t i, uint32_t h[8], uint32_t one = 1u) {
+    if constexpr (plain_adds<Src>::value) one = 1u;
     if constexpr (is_wide_leaf<Src>::value) {
-        src.digest(i, h);
+        src.digest(i, h, one);
     } else {
         uint32_t m[16];
 #pragma unroll
         for (int w = 0; w < 16; w++) m[w] = 0u;
         uint32_t nb = src.load(i, m);
-        blake2s_block(h, m, nb);
+        blake2s_block(h, m, nb, one);
     }
 }
 
@@ -110,7 +119,7 @@ struct LeafLifted {
         const uint64_t row = sh ? (((idx >> sh) << 1) | (idx & 1ull)) : idx;
         return __ldg(col[c] + row);
     }
-    __device__ __forceinline__ void digest(uint64_t idx, uint32_t h[8]) const {
+    __device__ __forceinline__ void digest(uint64_t idx, uint32_t h[8], uint32_t one = 1u) const {
         blake2s_init(h);
         const uint32_t nblk = n_cols ? (n_cols + 15u) / 16u : 1u;
         for (uint32_t b = 0; b < nblk; b++) {
@@ -121,26 +130,27 @@ struct LeafLifted {
                 m[w] = c < n_cols ? word(c, idx) : 0u;
             }
             const bool last = b + 1 == nblk;
-            blake2s_compress(h, m, last ? 4u * n_cols : 64u * (b + 1), last);
+            blake2s_compress(h, m, last ? 4u * n_cols : 64u * (b + 1), last, one);
         }
     }
 };
 
 // Fold a subtree of 2^kl leaves starting at `base` into its root.
 template <class Src>
-__device__ __forceinline__ void subtree_root(const Src &src, uint64_t base, uint32_t kl, uint32_t root[8]) {
+__device__ __forceinline__ void subtree_root(const Src &src, uint64_t base, uint32_t kl, uint32_t root[8],
+                                             uint32_t one = 1u) {
     uint32_t stk[5][8];
     uint32_t sp = 0;
     const uint32_t K = 1u << kl;
     for (uint32_t j = 0; j < K; j++) {
         uint32_t h[8];
-        leaf_digest(src, base + j, h);
+        leaf_digest(src, base + j, h, one);
         for (uint32_t jj = j; jj & 1u; jj >>= 1) {
             --sp;
             uint32_t mm[16];
 #pragma unroll
             for (int w = 0; w < 8; w++) { mm[w] = stk[sp][w]; mm[8 + w] = h[w]; }
-            blake2s_block(h, mm, 64u);
+            blake2s_block(h, mm, 64u, one);
         }
 #pragma unroll
         for (int w = 0; w < 8; w++) stk[sp][w] = h[w];
@@ -151,7 +161,8 @@ __device__ __forceinline__ void subtree_root(const Src &src, uint64_t base, uint
 }
 
 // Reduce 2^k consecutive 8-word hashes starting at hashes + 8*base.
-__device__ __forceinline__ void node_subtree_root(const uint32_t *hashes, uint64_t base, uint32_t k, uint32_t root[8]) {
+__device__ __forceinline__ void node_subtree_root(const uint32_t *hashes, uint64_t base, uint32_t k, uint32_t root[8],
+                                                  uint32_t one = 1u) {
     uint32_t stk[5][8];
     uint32_t sp = 0;
     const uint32_t K = 1u << k;
@@ -165,7 +176,7 @@ __device__ __forceinline__ void node_subtree_root(const uint32_t *hashes, uint64
             uint32_t mm[16];
 #pragma unroll
             for (int w = 0; w < 8; w++) { mm[w] = stk[sp][w]; mm[8 + w] = h[w]; }
-            blake2s_block(h, mm, 64u);
+            blake2s_block(h, mm, 64u, one);
         }
 #pragma unroll
         for (int w = 0; w < 8; w++) stk[sp][w] = h[w];
@@ -181,17 +192,21 @@ __device__ __forceinline__ void store_hash(uint32_t *dst, const uint32_t h[8]) {
     p[1] = make_uint4(h[4], h[5], h[6], h[7]);
 }
 
+// The hashing kernels take `one` (always 1) as a parameter for the pipe
+// balance of the Blake2s compression.
 template <class Src>
-__global__ void __launch_bounds__(256) leaf_subtree_kernel(Src src, uint32_t *out, uint64_t n_threads, uint32_t kl) {
+__global__ void __launch_bounds__(256) leaf_subtree_kernel(Src src, uint32_t *out, uint64_t n_threads, uint32_t kl,
+                                                           uint32_t one) {
     uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n_threads) return;
+    if constexpr (plain_adds<Src>::value) one = 1u;
     src.init();
     uint32_t h[8];
-    subtree_root(src, t << kl, kl, h);
+    subtree_root(src, t << kl, kl, h, one);
     store_hash(out + 8ull * t, h);
 }
 
-__global__ void node_subtree_kernel(const uint32_t *in, uint32_t *out, uint64_t n_threads, uint32_t k);
+__global__ void node_subtree_kernel(const uint32_t *in, uint32_t *out, uint64_t n_threads, uint32_t k, uint32_t one);
 
 // Device transcript state (channel.rs:15-185), advanced by the kernel that
 // finishes a commitment.
@@ -305,9 +320,10 @@ __device__ __forceinline__ void store_level_part(const TreeLevels &lv, uint32_t 
 }
 
 template <class Src>
-__global__ void __launch_bounds__(kReduceThreads) tree_reduce_kernel(Src src, TreeLevels lv, ChanStep cs) {
+__global__ void __launch_bounds__(kReduceThreads) tree_reduce_kernel(Src src, TreeLevels lv, ChanStep cs, uint32_t one) {
     __shared__ __align__(16) uint32_t sh[8u << kStageLog];
     __shared__ uint32_t is_last;
+    if constexpr (plain_adds<Src>::value) one = 1u;
     const uint32_t depth = lv.height[lv.n - 1];
     uint32_t h = lv.height[lv.top];
     const uint32_t *in = lv.top ? lv.hashes[lv.top] : nullptr;
@@ -321,7 +337,7 @@ __global__ void __launch_bounds__(kReduceThreads) tree_reduce_kernel(Src src, Tr
             src.init();
             for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
                 uint32_t hv[8];
-                leaf_digest(src, (part << c) + i, hv);
+                leaf_digest(src, (part << c) + i, hv, one);
                 store_hash(sh + 8 * i, hv);
             }
         } else {
@@ -335,7 +351,7 @@ __global__ void __launch_bounds__(kReduceThreads) tree_reduce_kernel(Src src, Tr
                 const uint32_t t = base + threadIdx.x;
                 uint32_t hv[8];
                 const bool act = t < half;
-                if (act) blake2s_node(hv, sh + 16 * t, sh + 16 * t + 8);
+                if (act) blake2s_node(hv, sh + 16 * t, sh + 16 * t + 8, one);
                 __syncthreads();
                 if (act) store_hash(sh + 8 * t, hv);
                 __syncthreads();
@@ -377,17 +393,17 @@ cudaError_t tree_build(const Src &src, const TreeLevels &lv, const ChanStep &cs,
     if (lv.top > 0) {
         uint32_t kl = lv.height[1];
         uint64_t n1 = 1ull << (depth - kl);
-        leaf_subtree_kernel<Src><<<(unsigned)((n1 + 255) / 256), 256, 0, stream>>>(src, lv.hashes[1], n1, kl);
+        leaf_subtree_kernel<Src><<<(unsigned)((n1 + 255) / 256), 256, 0, stream>>>(src, lv.hashes[1], n1, kl, 1u);
         for (uint32_t i = 2; i <= lv.top; i++) {
             uint32_t k = lv.height[i] - lv.height[i - 1];
             uint64_t nt = 1ull << (depth - lv.height[i]);
             node_subtree_kernel<<<(unsigned)((nt + 255) / 256), 256, 0, stream>>>(lv.hashes[i - 1], lv.hashes[i], nt,
-                                                                                  k);
+                                                                                  k, 1u);
         }
     }
     const uint32_t u = depth - lv.height[lv.top];
     const uint32_t c0 = u < kStageLog ? u : kStageLog;
-    tree_reduce_kernel<Src><<<(unsigned)(1ull << (u - c0)), kReduceThreads, 0, stream>>>(src, lv, cs);
+    tree_reduce_kernel<Src><<<(unsigned)(1ull << (u - c0)), kReduceThreads, 0, stream>>>(src, lv, cs, 1u);
     return cudaGetLastError();
 }
 
