@@ -333,6 +333,154 @@ def ntt_microbench(peak_gbs: float, sizes=(20, 24, 28), reps: int = 5):
     return out
 
 
+def _time_ms(fn, stream, reps):
+    import torch
+
+    fn()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def kernel_microbench(peak_gbs: float, probe_rate: float, log_n: int = 26, reps: int = 5):
+    """The standalone kernels of the log_n=24 proof's configuration at 2^26:
+    a Blake2s Merkle commitment over 2^26 M31 leaves, a FRI fold of a
+    2^26-point QM31 codeword down to 2 values (circle fold, then line folds),
+    the QM31 / M31 bit-reversals and the half-coset-to-canonic permutation.  Each runs through this library's
+    reference-compatible launchers (the reference's own call sequence:
+    merkle.rs commit_root_only = tiled 1024-leaf roots + hash_nodes +
+    reduce_to_root; fri.rs fold_*_with_twiddles) and, when they are built,
+    through the reference's own kernels (same symbols, same calls); the
+    Merkle commitment also through this library's fused tree
+    (vx_merkle_root_cols).  CUDA events on the legacy stream around `reps`
+    calls.  HBM figures use algorithmic bytes (each array read and written
+    once); the Merkle figures count compressions (2^26 leaves + 2^26 - 1
+    nodes)."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from vortexstark_b200 import _lib, fri
+    from vortexstark_b200.field import qm31_mul
+    from vortexstark_b200.merkle import FusedRoot
+    from vortexstark_b200.workload import m31_array
+
+    ds = torch.cuda.default_stream()
+    n = 1 << log_n
+    libs = {"vortex": _lib.lib()}
+    try:
+        from oracle import oracle as O
+
+        if O.ref_available():
+            R = O.ref_lib()
+            for name in ("cuda_merkle_tiled_generic", "cuda_merkle_hash_nodes", "cuda_merkle_reduce_to_root",
+                         "cuda_fold_line_soa", "cuda_fold_circle_into_line_soa", "cuda_bit_reverse_qm31",
+                         "cuda_bit_reverse_m31", "cuda_permute_hc_to_canonic_brt"):
+                getattr(R, name).argtypes = _lib._SIGS[name]
+            libs["reference_kernels"] = R
+    except Exception:
+        pass
+    out = {"log_n": log_n, "reps": reps}
+
+    # ---- Merkle commitment over 2^26 M31 leaves ----
+    col = torch.from_numpy(m31_array(SEED + 1, n).view("int32")).cuda()
+    ptrs = torch.tensor([col.data_ptr()], dtype=torch.int64, device="cuda")
+    tiles = n // 1024
+    sub_roots = torch.empty(tiles * 8, dtype=torch.int32, device="cuda")
+    scratch = [torch.empty(max(tiles >> (j + 1), 1) * 8, dtype=torch.int32, device="cuda") for j in range(20)]
+    root = torch.empty(8, dtype=torch.int32, device="cuda")
+    comps = 2 * n - 1
+    merkle = {}
+    roots = {}
+    for name, Lx in libs.items():
+        def commit(Lx=Lx):
+            Lx.cuda_merkle_tiled_generic(ptrs.data_ptr(), sub_roots.data_ptr(), 1, n)
+            cur, size, j = sub_roots, tiles, 0
+            while size > 1024:
+                size //= 2
+                Lx.cuda_merkle_hash_nodes(cur.data_ptr(), scratch[j].data_ptr(), size)
+                cur, j = scratch[j], j + 1
+            Lx.cuda_merkle_reduce_to_root(cur.data_ptr(), root.data_ptr(), size)
+        ms = _time_ms(commit, ds, reps)
+        roots[name] = bytes(root.cpu().numpy().tobytes())
+        merkle[name] = {"ms": ms, "compressions_per_s": comps / (ms / 1e3),
+                        "frac_of_probe": comps / (ms / 1e3) / probe_rate}
+    fr = FusedRoot(log_n)
+    ms = _time_ms(lambda: fr.commit_async([col]), ds, reps)
+    roots["fused"] = bytes(fr.root_dev.cpu().numpy().tobytes())
+    merkle["vortex_fused_tree"] = {"ms": ms, "compressions_per_s": comps / (ms / 1e3),
+                                   "frac_of_probe": comps / (ms / 1e3) / probe_rate}
+    merkle["roots_equal"] = len(set(roots.values())) == 1
+    out["merkle_commit_m31"] = merkle
+    del col, ptrs, sub_roots, scratch, fr
+    torch.cuda.empty_cache()
+
+    # ---- FRI fold chain 2^26 -> 2 ----
+    rng = np.random.default_rng(SEED + 2)
+    src = [torch.from_numpy(rng.integers(0, 0x7FFFFFFF, n, dtype=np.uint32).view(np.int32)).cuda() for _ in range(4)]
+    dst = [torch.empty(n // 2, dtype=torch.int32, device="cuda") for _ in range(4)]
+    ping = [[torch.empty(n // 4, dtype=torch.int32, device="cuda") for _ in range(4)] for _ in range(2)]
+    tws = fri.precompute_fri_twiddles(log_n, 1)  # circle fold at 2^26, line folds 2^25 .. 2^2
+    a4 = [int(x) for x in rng.integers(0, 0x7FFFFFFF, 4)]
+    alpha = (C.c_uint32 * 4)(*a4)
+    alpha_sq = (C.c_uint32 * 4)(*[int(x) for x in qm31_mul(a4, a4)])
+    fold_bytes = 16 * n + 2 * 16 * (n // 2) + 4 * (n // 2)  # circle: src, dst read+write, twiddles
+    m = n // 2
+    while m > 2:
+        fold_bytes += 16 * m + 4 * (m // 2) + 16 * (m // 2)
+        m //= 2
+    fold = {"bytes": fold_bytes}
+    finals = {}
+    for name, Lx in libs.items():
+        def chain(Lx=Lx):
+            Lx.cuda_fold_circle_into_line_soa(*[d.data_ptr() for d in dst], *[s.data_ptr() for s in src],
+                                              tws[0].data_ptr(), alpha, alpha_sq, n // 2)
+            cur, m, j = dst, n // 2, 0
+            while m > 2:
+                nxt = ping[j & 1]
+                Lx.cuda_fold_line_soa(*[c.data_ptr() for c in cur], tws[j + 1].data_ptr(),
+                                      *[c.data_ptr() for c in nxt], alpha, m // 2)
+                cur, m, j = nxt, m // 2, j + 1
+            return cur
+        for d in dst:
+            d.zero_()
+        last = chain()  # the circle fold accumulates into dst: time from a fixed start
+        finals[name] = b"".join(bytes(c[:2].cpu().numpy().tobytes()) for c in last)
+        def timed(Lx=Lx):
+            chain(Lx)
+        ms = _time_ms(timed, ds, reps)
+        fold[name] = {"ms": ms, "gbs": fold_bytes / (ms / 1e3) / 1e9, "frac": fold_bytes / (ms / 1e3) / 1e9 / peak_gbs}
+    fold["final_values_equal"] = len(set(finals.values())) == 1
+    out["fri_fold_qm31_to_2"] = fold
+    del src, dst, ping, tws
+    torch.cuda.empty_cache()
+
+    # ---- bit-reversals ----
+    qa = torch.from_numpy(rng.integers(0, 0x7FFFFFFF, 4 * n, dtype=np.uint32).view(np.int32)).cuda()
+    qb = torch.empty_like(qa)
+    br = {}
+    for name, Lx in libs.items():
+        ms = _time_ms(lambda Lx=Lx: Lx.cuda_bit_reverse_qm31(qa.data_ptr(), qb.data_ptr(), n, log_n), ds, reps)
+        br[f"qm31_{name}"] = {"ms": ms, "gbs": 32 * n / (ms / 1e3) / 1e9,
+                              "frac": 32 * n / (ms / 1e3) / 1e9 / peak_gbs}
+        ms = _time_ms(lambda Lx=Lx: Lx.cuda_bit_reverse_m31(qa.data_ptr(), log_n + 2), ds, reps)
+        br[f"m31_2^{log_n + 2}_{name}"] = {"ms": ms, "gbs": 32 * n / (ms / 1e3) / 1e9,
+                                          "frac": 32 * n / (ms / 1e3) / 1e9 / peak_gbs}
+        ms = _time_ms(lambda Lx=Lx: Lx.cuda_permute_hc_to_canonic_brt(qa.data_ptr(), qb.data_ptr(), 4 * n, log_n + 2),
+                      ds, reps)
+        br[f"permute_m31_2^{log_n + 2}_{name}"] = {"ms": ms, "gbs": 32 * n / (ms / 1e3) / 1e9,
+                                                  "frac": 32 * n / (ms / 1e3) / 1e9 / peak_gbs}
+    out["bit_reverse"] = br
+    del qa, qb
+    torch.cuda.empty_cache()
+    return out
+
+
 def pow_benchmark(probe_rate: float, bits: int = 26, cpu: bool = True):
     """Proof-of-work search at 26 bits (stwo's order (hi << 32) | low) from a
     seeded channel state: device time of vx_grind_pow and the candidates it
@@ -638,6 +786,7 @@ def main():
         }
         if world == 1 and not args.no_micro:
             line["ntt_microbench"] = ntt_microbench(peak)
+            line["kernel_microbench"] = kernel_microbench(peak, probe_rate)
             line["pow_grind"] = pow_benchmark(probe_rate, cpu=not args.no_cpu_baseline)
         if world == 1 and not args.no_batched:
             line["batched_commit"] = batched_commit_benchmark(SEED, max(steps, 5), args.warmup, peak, probe_rate,

@@ -380,6 +380,21 @@ int vx_probe_blake2s(uint32_t blocks, uint32_t threads, uint32_t iters, uint32_t
 int vx_tree_plan(uint32_t depth, uint32_t heights[12], uint32_t *n_levels, uint32_t *top, uint32_t *n_counters,
                  uint64_t *pool_words);
 
+/* Root-only Merkle commitment through the fused tree kernels (leaf
+ * subtrees, 16 -> 1 node kernels, one reduce launch) — replaces
+ * MerkleTree::commit_root_only (merkle.rs:142-231) and commit_root_soa4
+ * (merkle.rs:236-312), whose reference form is a launch per tree level.
+ * Leaf i = Blake2s of the LE words col[0][i] .. col[n_cols-1][i]
+ * (1 <= n_cols <= 16), node = Blake2s(left || right), 2^log_n_leaves leaves
+ * (1..31).  host_col_ptrs: HOST array of device column pointers.
+ * workspace: device memory of workspace_words words (at least
+ * vx_merkle_workspace_words(log_n_leaves); it holds the stored levels and
+ * is reused across calls).  root_out: 8 device words.  Enqueued on
+ * `stream`, no host synchronisation. */
+uint64_t vx_merkle_workspace_words(uint32_t log_n_leaves);
+int vx_merkle_root_cols(const uint32_t *const *host_col_ptrs, uint32_t n_cols, uint32_t log_n_leaves,
+                        uint32_t *workspace, uint64_t workspace_words, uint32_t *root_out, void *stream);
+
 /* Autotuner — no counterpart in the reference, whose kernels have fixed
  * shapes (circle_ntt.cu: one launch per layer; blake2s.cu: one leaf per
  * thread).  On the current device, times every distinct NTT pass plan

@@ -104,7 +104,7 @@ def test_ntt_single_layers(oracle, L):
     assert np.array_equal(to_host(d), oracle.ntt_evaluate(x, oracle.coset("half_coset", k)))
 
 
-@pytest.mark.parametrize("k", [1, 5, 10, 17])
+@pytest.mark.parametrize("k", [1, 5, 9, 10, 11, 12, 13, 17, 22])
 def test_bit_reverse_and_permute(oracle, L, k):
     x = m31_array(k, 1 << k)
     d = to_dev(x)
@@ -272,3 +272,43 @@ def test_no_launch_errors(L):
     import torch
     torch.cuda.synchronize()
     assert _lib.last_error() == ""
+
+
+@pytest.mark.parametrize("log_n,ncols", [(1, 1), (4, 4), (12, 1), (12, 3), (17, 1), (18, 4), (20, 16), (21, 1)])
+def test_fused_root_only_commit(oracle, log_n, ncols):
+    """vx_merkle_root_cols against the oracle's Merkle root (merkle.rs:142-312)."""
+    from vortexstark_b200.merkle import FusedRoot
+    cols = [m31_array(11 * log_n + i, 1 << log_n) for i in range(ncols)]
+    want = tuple(oracle.merkle_root(cols).tolist())
+    fr = FusedRoot(log_n)
+    d = [to_dev(c) for c in cols]
+    assert fr.commit(d) == want
+    assert fr.commit(d) == want  # workspace reused
+
+
+def test_fused_root_workspace_bounds(oracle, L):
+    import ctypes as C
+
+    from vortexstark_b200.merkle import FusedRoot
+    log_n = 20
+    col = m31_array(5, 1 << log_n)
+    want = tuple(oracle.merkle_root([col]).tolist())
+    d = to_dev(col)
+    fr = FusedRoot(log_n)
+    ptrs = (C.c_void_p * 1)(d.data_ptr())
+    # a workspace sized for the largest leaf subtree (smallest stored level) still works
+    small = L.vx_merkle_workspace_words(log_n)
+    for k in (4, 3, 2, 1):
+        from vortexstark_b200 import tune
+        tune.set_leaf_k(log_n, k)
+        small = min(small, int(L.vx_merkle_workspace_words(log_n)))
+    tune.set_leaf_k(log_n, 1)  # the device prefers a bigger pool than given
+    _lib.check(L.vx_merkle_root_cols(ptrs, 1, log_n, fr.workspace.data_ptr(), small, fr.root_dev.data_ptr(), None))
+    assert tuple(int(x) for x in to_host(fr.root_dev)) == want
+    with pytest.raises(_lib.VortexError):
+        _lib.check(L.vx_merkle_root_cols(ptrs, 1, log_n, fr.workspace.data_ptr(), small - 1, fr.root_dev.data_ptr(),
+                                         None))
+    with pytest.raises(_lib.VortexError):
+        _lib.check(L.vx_merkle_root_cols(ptrs, 17, log_n, fr.workspace.data_ptr(), small, fr.root_dev.data_ptr(),
+                                         None))
+    tune.set_leaf_k(log_n, 0)

@@ -90,6 +90,8 @@ _SIGS = {
     "vx_tree_plan": ([u32, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32), C.POINTER(u32),
                       C.POINTER(C.c_uint64)], C.c_int),
     "vx_autotune": ([u32, C.c_char_p, C.c_size_t], C.c_int),
+    "vx_merkle_workspace_words": ([u32], C.c_uint64),
+    "vx_merkle_root_cols": ([vp, u32, u32, vp, C.c_uint64, vp, vp], C.c_int),
     "vx_tune_set": ([u32, u32, u32, u32], C.c_int),
     "vx_tune_get": ([u32, u32, C.POINTER(u32), C.POINTER(u32)], C.c_int),
     "vx_ntt_plan": ([u32, u32, u32, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32), C.POINTER(u32)], C.c_int),

@@ -90,6 +90,69 @@ __global__ void quotient_kernel(const uint32_t *tr, uint32_t *o0, uint32_t *o1, 
 }
 
 // ---- bit reverse / permute ----
+// In place, tiled (log_n >= 10): write i = hi | mid << 5 | lo << ... as
+// (hi: top 5 bits, mid, lo: low 5 bits); brev(i) lies in tile brev(mid) at
+// row brev(lo), column brev(hi).  The block of tile pair (mid, brev(mid)),
+// mid <= brev(mid), reads both 32 x 32 tiles (128-byte rows) before writing
+// either, so the swap is race-free; blocks with mid > brev(mid) exit.
+constexpr uint32_t kBrevT = 5, kBrevS = 1u << kBrevT;
+__global__ void __launch_bounds__(256) bit_reverse_tiled_kernel(uint32_t *d, uint32_t log_n) {
+    __shared__ uint32_t ta[kBrevS][kBrevS + 1], tb[kBrevS][kBrevS + 1];
+    const uint32_t mid_bits = log_n - 2 * kBrevT;
+    const uint32_t mid = blockIdx.x;
+    const uint32_t bmid = mid_bits ? brev_bits(mid, mid_bits) : 0u;
+    if (mid > bmid) return;
+    const uint32_t tx = threadIdx.x & (kBrevS - 1u), ty = threadIdx.x >> kBrevT;  // 32 x 8
+    const uint32_t hs = log_n - kBrevT;
+#pragma unroll
+    for (uint32_t r = 0; r < kBrevS; r += 8) {
+        const uint32_t h = ty + r;
+        ta[h][tx] = d[tx | ((uint64_t)mid << kBrevT) | ((uint64_t)h << hs)];
+        if (bmid != mid) tb[h][tx] = d[tx | ((uint64_t)bmid << kBrevT) | ((uint64_t)h << hs)];
+    }
+    __syncthreads();
+    // new[tile t](h', l') = old[tile brev(t)](brev(l'), brev(h'))
+#pragma unroll
+    for (uint32_t r = 0; r < kBrevS; r += 8) {
+        const uint32_t h2 = ty + r, l2 = tx;
+        const uint32_t sh = brev_bits(l2, kBrevT), sl = brev_bits(h2, kBrevT);
+        d[l2 | ((uint64_t)bmid << kBrevT) | ((uint64_t)h2 << hs)] = ta[sh][sl];
+        if (bmid != mid) d[l2 | ((uint64_t)mid << kBrevT) | ((uint64_t)h2 << hs)] = tb[sh][sl];
+    }
+}
+
+// The same with 64 x 64 tiles (log_n >= 12): rows of 64 words move as one
+// 256-byte uint2 access per warp, like the permutation below.
+constexpr uint32_t kBrevT6 = 6, kBrevS6 = 1u << kBrevT6;
+__global__ void __launch_bounds__(256) bit_reverse_tiled64_kernel(uint32_t *d, uint32_t log_n) {
+    __shared__ uint32_t ta[kBrevS6][kBrevS6 + 1], tb[kBrevS6][kBrevS6 + 1];
+    const uint32_t mid_bits = log_n - 2 * kBrevT6;
+    const uint32_t mid = blockIdx.x;
+    const uint32_t bmid = mid_bits ? brev_bits(mid, mid_bits) : 0u;
+    if (mid > bmid) return;
+    const uint32_t tx = threadIdx.x & 31u, ty = threadIdx.x >> 5;  // 32 lanes x 8 rows, 2 words per lane
+    const uint32_t hs = log_n - kBrevT6;
+#pragma unroll
+    for (uint32_t r = 0; r < kBrevS6; r += 8) {
+        const uint32_t h = ty + r;
+        const uint2 va = ((const uint2 *)(d + ((uint64_t)mid << kBrevT6) + ((uint64_t)h << hs)))[tx];
+        ta[h][2 * tx] = va.x; ta[h][2 * tx + 1] = va.y;
+        if (bmid != mid) {
+            const uint2 vb = ((const uint2 *)(d + ((uint64_t)bmid << kBrevT6) + ((uint64_t)h << hs)))[tx];
+            tb[h][2 * tx] = vb.x; tb[h][2 * tx + 1] = vb.y;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (uint32_t r = 0; r < kBrevS6; r += 8) {
+        const uint32_t h2 = ty + r;
+        const uint32_t c = brev_bits(h2, kBrevT6), r0 = brev_bits(2 * tx, kBrevT6), r1 = brev_bits(2 * tx + 1, kBrevT6);
+        ((uint2 *)(d + ((uint64_t)bmid << kBrevT6) + ((uint64_t)h2 << hs)))[tx] = make_uint2(ta[r0][c], ta[r1][c]);
+        if (bmid != mid)
+            ((uint2 *)(d + ((uint64_t)mid << kBrevT6) + ((uint64_t)h2 << hs)))[tx] = make_uint2(tb[r0][c], tb[r1][c]);
+    }
+}
+
 __global__ void bit_reverse_kernel(uint32_t *d, uint32_t log_n, uint64_t n) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -100,6 +163,47 @@ __global__ void bit_reverse_kernel(uint32_t *d, uint32_t log_n, uint64_t n) {
 __device__ __forceinline__ uint64_t hc_to_canonic_brt(uint64_t k, uint64_t n, uint32_t log_n) {
     uint64_t cn = (k & 1ull) ? n - 1ull - (k >> 1) : (k >> 1);
     return brev_bits((uint32_t)cn, log_n);
+}
+
+// Tiled form of the permutation (log_n >= 12).  With k = 2q + b (b the
+// parity) and M = 2^(log_n-1) - 1, j(k) = 2 (brev(q) ^ (b ? M : 0)) + b: a
+// bit reversal of the even words and a complemented one of the odd words
+// over the (log_n - 1)-bit pair index.  j is an involution, so the forward
+// scatter and the inverse gather are the same out-of-place gather
+// dst[2u + b] = src[j(2u + b)].  Pairs u = lo | mid << 5 | hi << (L - 5),
+// L = log_n - 1: destination tiles m and ~m (complement in the mid bits)
+// read exactly the source tiles brev(m) and ~brev(m), 32 x 32 pairs each.
+__global__ void __launch_bounds__(256) permute_tiled_kernel(const uint2 *__restrict__ src, uint2 *__restrict__ dst,
+                                                            uint32_t log_n) {
+    __shared__ uint32_t ax[kBrevS][kBrevS + 1], ay[kBrevS][kBrevS + 1];
+    __shared__ uint32_t bx[kBrevS][kBrevS + 1], by[kBrevS][kBrevS + 1];
+    const uint32_t L = log_n - 1, mid_bits = L - 2 * kBrevT, mmask = (1u << mid_bits) - 1u;
+    const uint32_t m = blockIdx.x, m2 = m ^ mmask;          // m has its top mid bit clear
+    const uint32_t sa = brev_bits(m, mid_bits), sb = sa ^ mmask;
+    const uint32_t tx = threadIdx.x & (kBrevS - 1u), ty = threadIdx.x >> kBrevT;
+    const uint32_t hs = L - kBrevT;
+#pragma unroll
+    for (uint32_t r = 0; r < kBrevS; r += 8) {
+        const uint32_t h = ty + r;
+        const uint2 va = src[tx | ((uint64_t)sa << kBrevT) | ((uint64_t)h << hs)];
+        const uint2 vb = src[tx | ((uint64_t)sb << kBrevT) | ((uint64_t)h << hs)];
+        ax[h][tx] = va.x; ay[h][tx] = va.y;
+        bx[h][tx] = vb.x; by[h][tx] = vb.y;
+    }
+    __syncthreads();
+#pragma unroll
+    for (uint32_t r = 0; r < kBrevS; r += 8) {
+        const uint32_t h2 = ty + r, l2 = tx;
+        const uint32_t rr = brev_bits(l2, kBrevT), cc = brev_bits(h2, kBrevT);
+        const uint32_t nr = rr ^ (kBrevS - 1u), nc = cc ^ (kBrevS - 1u);
+        dst[l2 | ((uint64_t)m << kBrevT) | ((uint64_t)h2 << hs)] = make_uint2(ax[rr][cc], by[nr][nc]);
+        dst[l2 | ((uint64_t)m2 << kBrevT) | ((uint64_t)h2 << hs)] = make_uint2(bx[rr][cc], ay[nr][nc]);
+    }
+}
+
+bool permute_tiled_ok(const uint32_t *src, const uint32_t *dst, uint32_t n, uint32_t log_n) {
+    return log_n >= 12 && log_n <= 31 && (1ull << log_n) == n && src != dst &&
+           ((((uintptr_t)src) | ((uintptr_t)dst)) & 7u) == 0;
 }
 
 // permute.cu:30-58: forward scatters dst[j(k)] = src[k]; inverse gathers.
@@ -379,17 +483,28 @@ void cuda_circle_ntt_layer(uint32_t *d, const uint32_t *tw, uint32_t layer_idx, 
 
 void cuda_bit_reverse_m31(uint32_t *data, uint32_t log_n) {
     uint64_t n = 1ull << log_n;
-    bit_reverse_kernel<<<blocks_for(n, 256), 256>>>(data, log_n, n);
+    if (log_n >= 2 * kBrevT6 && log_n <= 31 && ((uintptr_t)data & 7u) == 0)
+        bit_reverse_tiled64_kernel<<<1u << (log_n - 2 * kBrevT6), 256>>>(data, log_n);
+    else if (log_n >= 2 * kBrevT && log_n <= 31)
+        bit_reverse_tiled_kernel<<<1u << (log_n - 2 * kBrevT), 256>>>(data, log_n);
+    else
+        bit_reverse_kernel<<<blocks_for(n, 256), 256>>>(data, log_n, n);
     VX_LAUNCH_CHECK();
 }
 
 void cuda_permute_hc_to_canonic_brt(const uint32_t *src, uint32_t *dst, uint32_t n, uint32_t log_n) {
-    permute_kernel<<<blocks_for(n, 256), 256>>>(src, dst, n, log_n, 0);
+    if (permute_tiled_ok(src, dst, n, log_n))
+        permute_tiled_kernel<<<1u << (log_n - 2 - 2 * kBrevT), 256>>>((const uint2 *)src, (uint2 *)dst, log_n);
+    else
+        permute_kernel<<<blocks_for(n, 256), 256>>>(src, dst, n, log_n, 0);
     VX_LAUNCH_CHECK();
 }
 
 void cuda_permute_canonic_brt_to_hc_natural(const uint32_t *src, uint32_t *dst, uint32_t n, uint32_t log_n) {
-    permute_kernel<<<blocks_for(n, 256), 256>>>(src, dst, n, log_n, 1);
+    if (permute_tiled_ok(src, dst, n, log_n))
+        permute_tiled_kernel<<<1u << (log_n - 2 - 2 * kBrevT), 256>>>((const uint2 *)src, (uint2 *)dst, log_n);
+    else
+        permute_kernel<<<blocks_for(n, 256), 256>>>(src, dst, n, log_n, 1);
     VX_LAUNCH_CHECK();
 }
 

@@ -129,3 +129,45 @@ extern "C" int vx_tree_plan(uint32_t depth, uint32_t heights[12], uint32_t *n_le
     *pool_words = w;
     return VX_OK;
 }
+
+extern "C" uint64_t vx_merkle_workspace_words(uint32_t log_n_leaves) {
+    if (log_n_leaves < 1 || log_n_leaves > 31) return 0;
+    return vx::tree_pool_words(log_n_leaves, vx::tree_leaf_k(log_n_leaves));
+}
+
+extern "C" int vx_merkle_root_cols(const uint32_t *const *host_col_ptrs, uint32_t n_cols, uint32_t log_n_leaves,
+                                   uint32_t *workspace, uint64_t workspace_words, uint32_t *root_out, void *stream) {
+    using namespace vx;
+    VX_CHECK_ARG(log_n_leaves >= 1 && log_n_leaves <= 31, "vx_merkle_root_cols: log_n_leaves %u outside 1..31",
+                 log_n_leaves);
+    VX_CHECK_ARG(host_col_ptrs && n_cols >= 1 && n_cols <= 16, "vx_merkle_root_cols: 1..16 columns");
+    VX_CHECK_ARG(workspace && root_out, "vx_merkle_root_cols: null workspace or root");
+    for (uint32_t c = 0; c < n_cols; c++) VX_CHECK_ARG(host_col_ptrs[c], "vx_merkle_root_cols: column %u is null", c);
+    const uint32_t d = log_n_leaves;
+    // the device's leaf-kernel shape, or a larger subtree (smaller stored
+    // level) if the workspace was sized for one
+    uint32_t k = tree_leaf_k(d);
+    while (k < 4 && tree_pool_words(d, k) > workspace_words) k++;
+    VX_CHECK_ARG(tree_pool_words(d, k) <= workspace_words,
+                 "vx_merkle_root_cols: workspace of %llu words, %llu needed", (unsigned long long)workspace_words,
+                 (unsigned long long)tree_pool_words(d, k));
+    cudaStream_t st = (cudaStream_t)stream;
+    TreeLevels lv;
+    tree_plan(d, workspace, &lv, k);
+    VX_CUDA_TRY(tree_reset(lv, st));
+    const ChanStep none{nullptr, nullptr, nullptr};
+    cudaError_t e;
+    if (n_cols == 1) {
+        e = tree_build(LeafM31{host_col_ptrs[0]}, lv, none, st);
+    } else if (n_cols == 4) {
+        e = tree_build(LeafSoA4{host_col_ptrs[0], host_col_ptrs[1], host_col_ptrs[2], host_col_ptrs[3]}, lv, none, st);
+    } else {
+        LeafColsV src{};
+        for (uint32_t c = 0; c < n_cols; c++) src.col[c] = host_col_ptrs[c];
+        src.n = n_cols;
+        e = tree_build(src, lv, none, st);
+    }
+    VX_CUDA_TRY(e);
+    VX_CUDA_TRY(cudaMemcpyAsync(root_out, lv.hashes[lv.n - 1], 32, cudaMemcpyDeviceToDevice, st));
+    return VX_OK;
+}

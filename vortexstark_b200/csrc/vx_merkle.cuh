@@ -50,6 +50,17 @@ struct LeafCols {
         return 4u * n;
     }
 };
+// Up to 16 columns passed by value (host-side pointer list); t = 4 * n.
+struct LeafColsV {
+    const uint32_t *col[16];
+    uint32_t n;
+    __device__ __forceinline__ void init() {}
+    __device__ __forceinline__ uint32_t load(uint64_t i, uint32_t m[16]) const {
+#pragma unroll
+        for (uint32_t c = 0; c < 16; c++) if (c < n) m[c] = __ldg(col[c] + i);
+        return 4u * n;
+    }
+};
 // Fibonacci quotient recomputed from the trace evaluation:
 // q[i] = alpha * (t[i+2] - (t[i+1] + t[i]))  (constraint.cu:10-33), i mod N.
 struct LeafQuotient {

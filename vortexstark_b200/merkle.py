@@ -161,6 +161,34 @@ class MerkleTree:
         return tuple(int(x) for x in _words(cur[:8]))
 
 
+class FusedRoot:
+    """Root-only commitment through the fused tree kernels
+    (vx_merkle_root_cols): the drop-in for ``commit_root_only`` /
+    ``commit_root_soa4`` with a reusable device workspace."""
+
+    def __init__(self, log_n_leaves: int):
+        import torch
+
+        self.log_n_leaves = log_n_leaves
+        self.words = int(_lib.lib().vx_merkle_workspace_words(log_n_leaves))
+        if not self.words:
+            raise _lib.VortexError(_lib.VX_ERR_ARG, f"unsupported tree size 2^{log_n_leaves}")
+        self.workspace = torch.empty(self.words, dtype=torch.int32, device="cuda")
+        self.root_dev = torch.empty(8, dtype=torch.int32, device="cuda")
+
+    def commit_async(self, columns, stream=None) -> None:
+        import ctypes as C
+
+        ptrs = (C.c_void_p * len(columns))(*[c.data_ptr() for c in columns])
+        _lib.check(_lib.lib().vx_merkle_root_cols(ptrs, len(columns), self.log_n_leaves, self.workspace.data_ptr(),
+                                                  self.words, self.root_dev.data_ptr(),
+                                                  C.c_void_p(stream) if stream else None))
+
+    def commit(self, columns) -> tuple:
+        self.commit_async(columns)
+        return tuple(int(x) for x in _words(self.root_dev))
+
+
 def build_leaves_lifted(columns, lifting_log_size: int):
     """crates/cuda-backend/src/merkle_ops.rs:48-173 — one lifted leaf hash per
     row of the largest column; columns must be sorted by ascending size."""
