@@ -243,7 +243,7 @@ def test_lifted_leaves(oracle):
     assert np.array_equal(to_host(out).reshape(-1, 8), oracle.lifted_leaves(cols, 10))
 
 
-@pytest.mark.parametrize("k", [4, 9, 16])
+@pytest.mark.parametrize("k", [2, 3, 4, 9, 16, 20])
 def test_folds(oracle, k):
     from vortexstark_b200 import fri
     from vortexstark_b200.circle import Coset
@@ -266,6 +266,28 @@ def test_folds(oracle, k):
     fri.fold_circle_into_line_with_twiddles(dst2, col, alpha, twc)
     want2 = oracle.fold_circle_into_line(prev, src, oracle.fold_twiddles(oracle.coset("half_coset", k), True), alpha)
     assert np.array_equal(dst2.to_words(), want2)
+
+
+def test_folds_unaligned_match_aligned(oracle, L):
+    """The scalar fold kernels (pointers only 4-byte aligned) and the
+    vectorised ones give the same words."""
+    import ctypes as C
+
+    import torch
+
+    k = 12
+    src = np.stack([m31_array(900 + c, 1 << k) for c in range(4)])
+    tw = np.asarray(oracle.fold_twiddles(oracle.coset("half_odds", k), False), np.uint32)
+    want = oracle.fold_line(src, tw, (5, 6, 7, 8))
+    alpha = (C.c_uint32 * 4)(5, 6, 7, 8)
+    for off in (0, 1):
+        ins = [torch.from_numpy(np.concatenate([np.zeros(off, np.uint32), c]).view(np.int32)).cuda() for c in src]
+        t = torch.from_numpy(np.concatenate([np.zeros(off, np.uint32), tw]).view(np.int32)).cuda()
+        outs = [torch.zeros((1 << (k - 1)) + off, dtype=torch.int32, device="cuda") for _ in range(4)]
+        L.cuda_fold_line_soa(*[x.data_ptr() + 4 * off for x in ins], t.data_ptr() + 4 * off,
+                             *[o.data_ptr() + 4 * off for o in outs], alpha, 1 << (k - 1))
+        got = np.stack([to_host(o)[off:] for o in outs])
+        assert np.array_equal(got, want), off
 
 
 def test_no_launch_errors(L):

@@ -371,8 +371,9 @@ __global__ void fold_line_kernel(const uint32_t *i0, const uint32_t *i1, const u
                                  uint64_t half) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= half) return;
+    const qmat am = qmat_of(al);
     qm31 f0{{i0[2 * i], i1[2 * i], i2[2 * i], i3[2 * i]}}, f1{{i0[2 * i + 1], i1[2 * i + 1], i2[2 * i + 1], i3[2 * i + 1]}};
-    qm31 r = qadd(qadd(f0, f1), qmul(al, qmulm(qsub(f0, f1), tw[i])));
+    qm31 r = qadd(qadd(f0, f1), qmul_mat(am, qmulm(qsub(f0, f1), tw[i])));
     o0[i] = r.v[0]; o1[i] = r.v[1]; o2[i] = r.v[2]; o3[i] = r.v[3];
 }
 __global__ void fold_circle_kernel(uint32_t *d0, uint32_t *d1, uint32_t *d2, uint32_t *d3, const uint32_t *s0,
@@ -380,11 +381,57 @@ __global__ void fold_circle_kernel(uint32_t *d0, uint32_t *d1, uint32_t *d2, uin
                                    qm31 al, qm31 al2, uint64_t half) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= half) return;
+    const qmat am = qmat_of(al), am2 = qmat_of(al2);
     qm31 f0{{s0[2 * i], s1[2 * i], s2[2 * i], s3[2 * i]}}, f1{{s0[2 * i + 1], s1[2 * i + 1], s2[2 * i + 1], s3[2 * i + 1]}};
-    qm31 fp = qadd(qadd(f0, f1), qmul(al, qmulm(qsub(f0, f1), tw[i])));
+    qm31 fp = qadd(qadd(f0, f1), qmul_mat(am, qmulm(qsub(f0, f1), tw[i])));
     qm31 prev{{d0[i], d1[i], d2[i], d3[i]}};
-    qm31 r = qadd(qmul(prev, al2), fp);
+    qm31 r = qadd(qmul_mat(am2, prev), fp);
     d0[i] = r.v[0]; d1[i] = r.v[1]; d2[i] = r.v[2]; d3[i] = r.v[3];
+}
+
+// Two outputs per thread: one 16-byte load per input column (pairs 2t and
+// 2t + 1), 8-byte twiddle, accumulator and output accesses.  Used when every
+// pointer is 16-byte (inputs) / 8-byte (the rest) aligned and half is even.
+__device__ __forceinline__ qm31 fold_pair(qm31 f0, qm31 f1, const qmat &am, uint32_t t) {
+    return qadd(qadd(f0, f1), qmul_mat(am, qmulm(qsub(f0, f1), t)));
+}
+__global__ void __launch_bounds__(256) fold_line2_kernel(const uint4 *i0, const uint4 *i1, const uint4 *i2,
+                                                         const uint4 *i3, const uint2 *tw, uint2 *o0, uint2 *o1,
+                                                         uint2 *o2, uint2 *o3, qm31 al, uint64_t half2) {
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= half2) return;
+    const qmat am = qmat_of(al);
+    const uint4 a = __ldcs(i0 + t), b = __ldcs(i1 + t), c = __ldcs(i2 + t), d = __ldcs(i3 + t);
+    const uint2 w = __ldg(tw + t);
+    const qm31 r0 = fold_pair(qm31{{a.x, b.x, c.x, d.x}}, qm31{{a.y, b.y, c.y, d.y}}, am, w.x);
+    const qm31 r1 = fold_pair(qm31{{a.z, b.z, c.z, d.z}}, qm31{{a.w, b.w, c.w, d.w}}, am, w.y);
+    o0[t] = make_uint2(r0.v[0], r1.v[0]); o1[t] = make_uint2(r0.v[1], r1.v[1]);
+    o2[t] = make_uint2(r0.v[2], r1.v[2]); o3[t] = make_uint2(r0.v[3], r1.v[3]);
+}
+__global__ void __launch_bounds__(256) fold_circle2_kernel(uint2 *d0, uint2 *d1, uint2 *d2, uint2 *d3,
+                                                           const uint4 *s0, const uint4 *s1, const uint4 *s2,
+                                                           const uint4 *s3, const uint2 *tw, qm31 al, qm31 al2,
+                                                           uint64_t half2) {
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= half2) return;
+    const qmat am = qmat_of(al), am2 = qmat_of(al2);
+    const uint4 a = __ldcs(s0 + t), b = __ldcs(s1 + t), c = __ldcs(s2 + t), d = __ldcs(s3 + t);
+    const uint2 w = __ldg(tw + t);
+    const uint2 p0 = d0[t], p1 = d1[t], p2 = d2[t], p3 = d3[t];
+    const qm31 r0 = qadd(qmul_mat(am2, qm31{{p0.x, p1.x, p2.x, p3.x}}),
+                         fold_pair(qm31{{a.x, b.x, c.x, d.x}}, qm31{{a.y, b.y, c.y, d.y}}, am, w.x));
+    const qm31 r1 = qadd(qmul_mat(am2, qm31{{p0.y, p1.y, p2.y, p3.y}}),
+                         fold_pair(qm31{{a.z, b.z, c.z, d.z}}, qm31{{a.w, b.w, c.w, d.w}}, am, w.y));
+    d0[t] = make_uint2(r0.v[0], r1.v[0]); d1[t] = make_uint2(r0.v[1], r1.v[1]);
+    d2[t] = make_uint2(r0.v[2], r1.v[2]); d3[t] = make_uint2(r0.v[3], r1.v[3]);
+}
+bool fold_vec_ok(const void *const *in, const void *const *rest, int n_rest, uint32_t half_n) {
+    if (half_n < 2 || (half_n & 1u)) return false;
+    for (int k = 0; k < 4; k++)
+        if ((uintptr_t)in[k] & 15u) return false;
+    for (int k = 0; k < n_rest; k++)
+        if ((uintptr_t)rest[k] & 7u) return false;
+    return true;
 }
 
 NttTables ref_tables(const uint32_t *line, const uint32_t *circle, const uint32_t *h_offsets, uint32_t n_line) {
@@ -649,7 +696,14 @@ void cuda_fold_line_soa(const uint32_t *i0, const uint32_t *i1, const uint32_t *
                         const uint32_t *tw, uint32_t *o0, uint32_t *o1, uint32_t *o2, uint32_t *o3,
                         const uint32_t *alpha, uint32_t half_n) {
     qm31 al{{alpha[0], alpha[1], alpha[2], alpha[3]}};
-    fold_line_kernel<<<blocks_for(half_n, 256), 256>>>(i0, i1, i2, i3, tw, o0, o1, o2, o3, al, half_n);
+    const void *in[4] = {i0, i1, i2, i3}, *rest[5] = {tw, o0, o1, o2, o3};
+    if (fold_vec_ok(in, rest, 5, half_n))
+        fold_line2_kernel<<<blocks_for(half_n / 2, 256), 256>>>((const uint4 *)i0, (const uint4 *)i1,
+                                                                (const uint4 *)i2, (const uint4 *)i3,
+                                                                (const uint2 *)tw, (uint2 *)o0, (uint2 *)o1,
+                                                                (uint2 *)o2, (uint2 *)o3, al, half_n / 2);
+    else
+        fold_line_kernel<<<blocks_for(half_n, 256), 256>>>(i0, i1, i2, i3, tw, o0, o1, o2, o3, al, half_n);
     VX_LAUNCH_CHECK();
 }
 
@@ -657,7 +711,14 @@ void cuda_fold_circle_into_line_soa(uint32_t *d0, uint32_t *d1, uint32_t *d2, ui
                                     const uint32_t *s1, const uint32_t *s2, const uint32_t *s3, const uint32_t *tw,
                                     const uint32_t *alpha, const uint32_t *alpha_sq, uint32_t half_n) {
     qm31 al{{alpha[0], alpha[1], alpha[2], alpha[3]}}, al2{{alpha_sq[0], alpha_sq[1], alpha_sq[2], alpha_sq[3]}};
-    fold_circle_kernel<<<blocks_for(half_n, 256), 256>>>(d0, d1, d2, d3, s0, s1, s2, s3, tw, al, al2, half_n);
+    const void *in[4] = {s0, s1, s2, s3}, *rest[5] = {tw, d0, d1, d2, d3};
+    if (fold_vec_ok(in, rest, 5, half_n))
+        fold_circle2_kernel<<<blocks_for(half_n / 2, 256), 256>>>((uint2 *)d0, (uint2 *)d1, (uint2 *)d2,
+                                                                  (uint2 *)d3, (const uint4 *)s0, (const uint4 *)s1,
+                                                                  (const uint4 *)s2, (const uint4 *)s3,
+                                                                  (const uint2 *)tw, al, al2, half_n / 2);
+    else
+        fold_circle_kernel<<<blocks_for(half_n, 256), 256>>>(d0, d1, d2, d3, s0, s1, s2, s3, tw, al, al2, half_n);
     VX_LAUNCH_CHECK();
 }
 

@@ -161,14 +161,14 @@ struct LeafCircleFold {
     const uint32_t *tw;
     const uint32_t *alpha_ptr;
     uint32_t *o0, *o1, *o2, *o3;
-    qm31 al;
+    qmat am;  // multiplication by the fold challenge
     __device__ __forceinline__ void init() {
         q.init();
-        al = {{alpha_ptr[0], alpha_ptr[1], alpha_ptr[2], alpha_ptr[3]}};
+        am = qmat_of(qm31{{alpha_ptr[0], alpha_ptr[1], alpha_ptr[2], alpha_ptr[3]}});
     }
     __device__ __forceinline__ uint32_t load(uint64_t j, uint32_t m[16]) const {
         qm31 f0 = q.value(2 * j), f1 = q.value(2 * j + 1);
-        qm31 r = qadd(qadd(f0, f1), qmul(al, qmulm(qsub(f0, f1), __ldg(tw + j))));
+        qm31 r = qadd(qadd(f0, f1), qmul_mat(am, qmulm(qsub(f0, f1), __ldg(tw + j))));
         o0[j] = r.v[0]; o1[j] = r.v[1]; o2[j] = r.v[2]; o3[j] = r.v[3];
         m[0] = r.v[0]; m[1] = r.v[1]; m[2] = r.v[2]; m[3] = r.v[3];
         return 16u;
