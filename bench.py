@@ -346,10 +346,12 @@ def _time_ms(fn, stream, reps):
     return e0.elapsed_time(e1) / reps
 
 
-def kernel_microbench(peak_gbs: float, probe_rate: float, log_n: int = 26, reps: int = 5):
+def kernel_microbench(peak_gbs: float, probe_rate: float, log_n: int = 26, reps: int = 5, cpu: bool = True):
     """The standalone kernels of the log_n=24 proof's configuration at 2^26:
     a Blake2s Merkle commitment over 2^26 M31 leaves, a FRI fold of a
-    2^26-point QM31 codeword down to 2 values (circle fold, then line folds),
+    2^26-point QM31 codeword down to 2 values (circle fold, then line folds;
+    once as bare folds, once with every layer committed and its challenge
+    drawn from the transcript, beside the CPU oracle),
     the QM31 / M31 bit-reversals and the half-coset-to-canonic permutation.  Each runs through this library's
     reference-compatible launchers (the reference's own call sequence:
     merkle.rs commit_root_only = tiled 1024-leaf roots + hash_nodes +
@@ -429,12 +431,15 @@ def kernel_microbench(peak_gbs: float, probe_rate: float, log_n: int = 26, reps:
     a4 = [int(x) for x in rng.integers(0, 0x7FFFFFFF, 4)]
     alpha = (C.c_uint32 * 4)(*a4)
     alpha_sq = (C.c_uint32 * 4)(*[int(x) for x in qm31_mul(a4, a4)])
-    fold_bytes = 16 * n + 2 * 16 * (n // 2) + 4 * (n // 2)  # circle: src, dst read+write, twiddles
+    # algorithmic bytes (fixed formulas: circle fold N -> N/2 = 24N, line fold M -> M/2 = 24M; twiddles and
+    # the circle fold's accumulator read excluded), and the bytes the launchers actually move
+    fold_bytes, moved = 24 * n, 16 * n + 2 * 16 * (n // 2) + 4 * (n // 2)
     m = n // 2
     while m > 2:
-        fold_bytes += 16 * m + 4 * (m // 2) + 16 * (m // 2)
+        fold_bytes += 24 * m
+        moved += 16 * m + 4 * (m // 2) + 16 * (m // 2)
         m //= 2
-    fold = {"bytes": fold_bytes}
+    fold = {"bytes": fold_bytes, "bytes_moved_incl_twiddles_and_accumulator": moved}
     finals = {}
     for name, Lx in libs.items():
         def chain(Lx=Lx):
@@ -457,7 +462,32 @@ def kernel_microbench(peak_gbs: float, probe_rate: float, log_n: int = 26, reps:
         fold[name] = {"ms": ms, "gbs": fold_bytes / (ms / 1e3) / 1e9, "frac": fold_bytes / (ms / 1e3) / 1e9 / peak_gbs}
     fold["final_values_equal"] = len(set(finals.values())) == 1
     out["fri_fold_qm31_to_2"] = fold
-    del src, dst, ping, tws
+    del dst, ping, tws
+    torch.cuda.empty_cache()
+
+    # ---- FRI chain with a commitment per layer, transcript-drawn challenges (vx_fri_chain) ----
+    from vortexstark_b200.fri import FriChain
+
+    state = [int(x) for x in rng.integers(0, 1 << 32, 8, dtype=np.uint64)]
+    chain = FriChain(log_n)
+    ms = _time_ms(lambda: chain.commit_async(src, state), ds, reps)
+    roots, _, last = chain.result()
+    comps = sum((1 << l) + (1 << l) - 1 for l in range(1, log_n))  # layer of 2^l values: leaves + nodes
+    fc = {"ms": ms, "layers": chain.layers, "launches": chain.launches(), "compressions": comps,
+          "compressions_per_s": comps / (ms / 1e3), "frac_of_probe": comps / (ms / 1e3) / probe_rate,
+          "fold_bytes": fold_bytes, "fold_gbs": fold_bytes / (ms / 1e3) / 1e9}
+    if cpu:
+        from oracle import oracle as O
+
+        host = np.stack([s.cpu().numpy().view(np.uint32) for s in src])
+        t0 = time.perf_counter()
+        oroots, _, olast = O.fri_chain(host, state)
+        fc["cpu_baseline"] = {"ms": 1e3 * (time.perf_counter() - t0), "cores": O.get_threads(), "kind": "port",
+                              "equal": bool(np.array_equal(np.array(roots, np.uint32), oroots)
+                                            and np.array_equal(np.array(last, np.uint32), olast))}
+    out["fri_chain_committed"] = fc
+    chain.close()
+    del src
     torch.cuda.empty_cache()
 
     # ---- bit-reversals ----
@@ -791,7 +821,7 @@ def main():
         }
         if world == 1 and not args.no_micro:
             line["ntt_microbench"] = ntt_microbench(peak)
-            line["kernel_microbench"] = kernel_microbench(peak, probe_rate)
+            line["kernel_microbench"] = kernel_microbench(peak, probe_rate, cpu=not args.no_cpu_baseline)
             line["pow_grind"] = pow_benchmark(probe_rate, cpu=not args.no_cpu_baseline)
         if world == 1 and not args.no_batched:
             line["batched_commit"] = batched_commit_benchmark(SEED, max(steps, 5), args.warmup, peak, probe_rate,

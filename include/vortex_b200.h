@@ -395,6 +395,31 @@ uint64_t vx_merkle_workspace_words(uint32_t log_n_leaves);
 int vx_merkle_root_cols(const uint32_t *const *host_col_ptrs, uint32_t n_cols, uint32_t log_n_leaves,
                         uint32_t *workspace, uint64_t workspace_words, uint32_t *root_out, void *stream);
 
+/* FRI chain of a QM31 codeword with a commitment per layer — the proof's
+ * FRI (prover.rs:860-926; folds fri.rs:163-224) run down to 2 values, as
+ * one call.  The codeword is 4 SoA device columns of 2^log_size words
+ * (3 <= log_size <= 30), its evaluation on half_coset(log_size).  With the
+ * transcript started from `state` (8 host words): alpha_0 = draw_felt;
+ * layer 0 = circle fold of the codeword (into zero); for k >= 1 layer k =
+ * line fold of layer k-1 with the half_odds twiddles and alpha_k; every
+ * layer committed as a tree of 4-word leaves, its root mixed, then the
+ * next challenge drawn.  log_size - 1 layers; the last holds 2 values.
+ * Folds run inside the hashing kernels, transcript steps in the kernel
+ * that finishes each tree; no host synchronisation until fetch. */
+typedef struct vx_fri_chain vx_fri_chain;
+int vx_fri_chain_create(uint32_t log_size, vx_fri_chain **out);
+void vx_fri_chain_destroy(vx_fri_chain *h);
+uint32_t vx_fri_chain_layers(const vx_fri_chain *h);
+/* host_cols: HOST array of 4 device pointers (8-byte aligned). */
+int vx_fri_chain_commit_async(vx_fri_chain *h, const uint32_t *const *host_cols, const uint32_t state[8],
+                              void *stream);
+/* Kernels enqueued by the last commit. */
+uint32_t vx_fri_chain_launches(const vx_fri_chain *h);
+/* Waits for `stream`, then: roots (8 words per layer), alphas (4 per layer),
+ * last = the 2 values of the last layer, 4 words each.  VX_ERR_DEVICE if a
+ * challenge draw gave up. */
+int vx_fri_chain_fetch(vx_fri_chain *h, uint32_t *roots, uint32_t *alphas, uint32_t last[8], void *stream);
+
 /* Autotuner — no counterpart in the reference, whose kernels have fixed
  * shapes (circle_ntt.cu: one launch per layer; blake2s.cu: one leaf per
  * thread).  On the current device, times every distinct NTT pass plan

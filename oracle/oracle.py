@@ -67,6 +67,7 @@ def lib():
         L.vxo_bit_reverse_qm31.argtypes = [U32P, U32P, C.c_uint32]
         L.vxo_accumulate_lift.argtypes = [U32P, U32P, C.c_uint64, C.c_uint32]
         L.vxo_pack_leaves.argtypes = [C.POINTER(U32P), C.POINTER(U32P), C.c_uint64]
+        L.vxo_fri_chain.argtypes = [C.POINTER(U32P), C.c_uint32, U32P, U32P, U32P, U32P]
         L.vxo_stwo_fold_circle_twiddles.argtypes = [C.c_uint32, U32P]
         L.vxo_lifted_size.argtypes = [C.c_uint32, U32P, C.c_uint32, C.c_uint32]
         L.vxo_lifted_size.restype = C.c_size_t
@@ -273,6 +274,21 @@ def fold_circle_into_line(dst: np.ndarray, src: np.ndarray, tw: np.ndarray, alph
     outs = (U32P * 4)(*[_p(dst[c]) for c in range(4)])
     lib().vxo_fold_circle_into_line(outs, ins, _p(np.ascontiguousarray(tw, dtype=np.uint32)), _p(al), _p(al2), half)
     return dst
+
+
+def fri_chain(src: np.ndarray, state_words):
+    """FRI chain with per-layer commitments of a QM31 codeword (4 x 2^L
+    words, SoA) on half_coset(L), transcript started from `state_words`
+    (8 words): (roots [L-1, 8], alphas [L-1, 4], last [2, 4])."""
+    src = np.ascontiguousarray(src, dtype=np.uint32)
+    L = int(src.shape[1]).bit_length() - 1
+    ins = (U32P * 4)(*[_p(src[c]) for c in range(4)])
+    st = np.ascontiguousarray(state_words, dtype=np.uint32)
+    roots = np.zeros((L - 1, 8), np.uint32)
+    alphas = np.zeros((L - 1, 4), np.uint32)
+    last = np.zeros((2, 4), np.uint32)
+    lib().vxo_fri_chain(ins, L, _p(st), _p(roots), _p(alphas), _p(last))
+    return roots, alphas, last
 
 
 def batch_inverse(x: np.ndarray) -> np.ndarray:

@@ -1146,3 +1146,50 @@ int vxo_grind_pow(const uint32_t prefix[8], uint32_t pow_bits, int m31, uint32_t
     }
     return 1;
 }
+
+/* ------------------------------------------------------------------ */
+/* FRI chain of a QM31 codeword with per-layer commitments: the FRI    */
+/* item of the log_n = 24 configuration, composed from the pieces of   */
+/* the proof's FRI (prover.rs:860-926, fri.rs:163-224):                */
+/*  alpha_0 = draw_felt(state); layer 0 = circle fold of the codeword  */
+/*  on half_coset(L) (dst zero); then for k >= 1: mix(root_{k-1}),     */
+/*  alpha_k = draw_felt, layer k = line fold of layer k-1 with the     */
+/*  half_odds(l) twiddles; every layer committed as a 4-word-leaf tree  */
+/*  (the last, of 2 values, too) and its root mixed.                   */
+/* ------------------------------------------------------------------ */
+void vxo_fri_chain(const uint32_t *const src[4], uint32_t log_size, const uint32_t state[8], uint32_t *roots,
+                   uint32_t *alphas, uint32_t last[8]) {
+    const uint32_t L = log_size, nl = L - 1;
+    vxo_channel ch;
+    for (int i = 0; i < 8; i++) st32(ch.state + 4 * i, state[i]);
+    ch.n_draws = 0;
+    uint64_t m = 1ull << (L - 1);
+    uint32_t *cur[4], *nxt[4];
+    for (int c = 0; c < 4; c++) {
+        cur[c] = (uint32_t *)calloc(m, 4);
+        nxt[c] = (uint32_t *)calloc(m / 2 ? m / 2 : 1, 4);
+    }
+    uint32_t *tw = (uint32_t *)malloc(m * 4);
+    vxo_coset dom = vxo_coset_half_coset(L);
+    vxo_fold_twiddles(&dom, 1, tw);
+    static const uint32_t zero4[4] = {0, 0, 0, 0};
+    vxo_channel_draw_felt(&ch, alphas);
+    vxo_fold_circle_into_line(cur, src, tw, alphas, zero4, m);
+    vxo_merkle_root((const uint32_t *const *)cur, 4, L - 1, roots);
+    vxo_channel_mix_digest(&ch, roots);
+    for (uint32_t k = 1; k < nl; k++) {
+        const uint32_t l = L - k;  /* log size of the layer being folded */
+        const uint64_t half = 1ull << (l - 1);
+        vxo_channel_draw_felt(&ch, alphas + 4 * k);
+        vxo_coset od = vxo_coset_half_odds(l);
+        vxo_fold_twiddles(&od, 0, tw);
+        vxo_fold_line((const uint32_t *const *)cur, tw, alphas + 4 * k, nxt, half);
+        vxo_merkle_root((const uint32_t *const *)nxt, 4, l - 1, roots + 8 * k);
+        vxo_channel_mix_digest(&ch, roots + 8 * k);
+        for (int c = 0; c < 4; c++) { uint32_t *t = cur[c]; cur[c] = nxt[c]; nxt[c] = t; }
+    }
+    for (int i = 0; i < 2; i++)
+        for (int c = 0; c < 4; c++) last[4 * i + c] = cur[c][i];
+    for (int c = 0; c < 4; c++) { free(cur[c]); free(nxt[c]); }
+    free(tw);
+}

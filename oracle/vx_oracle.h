@@ -97,6 +97,13 @@ void vxo_fold_circle_into_line(uint32_t *const dst[4], const uint32_t *const src
                                const uint32_t *tw, const uint32_t alpha[4],
                                const uint32_t alpha_sq[4], uint64_t half_n);
 
+/* FRI chain with per-layer commitments of a 2^log_size QM31 codeword (SoA4)
+ * on half_coset(log_size): log_size - 1 layers down to 2 values; roots
+ * (8 words per layer), the challenges (4 words per layer), the last layer
+ * (2 QM31, 4 words each). */
+void vxo_fri_chain(const uint32_t *const src[4], uint32_t log_size, const uint32_t state[8], uint32_t *roots,
+                   uint32_t *alphas, uint32_t last[8]);
+
 /* ---- channel (channel.rs:15-185) ---- */
 typedef struct { uint8_t state[32]; uint32_t n_draws; } vxo_channel;
 void vxo_channel_init(vxo_channel *ch);

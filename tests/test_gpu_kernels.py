@@ -334,3 +334,24 @@ def test_fused_root_workspace_bounds(oracle, L):
         _lib.check(L.vx_merkle_root_cols(ptrs, 17, log_n, fr.workspace.data_ptr(), small, fr.root_dev.data_ptr(),
                                          None))
     tune.set_leaf_k(log_n, 0)
+
+
+@pytest.mark.parametrize("L", [3, 4, 8, 13, 17, 20])
+def test_fri_chain_matches_oracle(oracle, L):
+    """vx_fri_chain against the oracle's composition of the proof's FRI
+    pieces (circle fold, line folds, 4-word-leaf trees, transcript)."""
+    from vortexstark_b200.fri import FriChain
+    src = np.stack([m31_array(70 * L + c, 1 << L) for c in range(4)])
+    state = [int(x) for x in m31_array(3 + L, 8)]
+    want_roots, want_alphas, want_last = oracle.fri_chain(src, state)
+    ch = FriChain(L)
+    assert ch.layers == L - 1
+    cols = [to_dev(c) for c in src]
+    for _ in range(2):  # reusable: the second run must give the same words
+        ch.commit_async(cols, state)
+        roots, alphas, last = ch.result()
+        assert np.array_equal(np.array(alphas, np.uint32), want_alphas)
+        assert np.array_equal(np.array(roots, np.uint32), want_roots)
+        assert np.array_equal(np.array(last, np.uint32), want_last)
+    assert ch.launches() >= L
+    ch.close()

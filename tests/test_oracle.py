@@ -200,3 +200,37 @@ def test_lifted_leaves(oracle):
             words.append(int(c[row]))
         h = struct.unpack("<8I", hashlib.blake2s(struct.pack(f"<{len(words)}I", *words)).digest())
         assert tuple(got[idx].tolist()) == h
+
+
+def test_fri_chain_composition():
+    """vxo_fri_chain against a composition of the oracle's fold and tree
+    functions with the host channel restatement (channel.rs): the order of
+    draws, folds, commitments and mixes."""
+    import struct
+
+    import numpy as np
+
+    from oracle import oracle as O
+    from vortexstark_b200.channel import Channel
+
+    L = 7
+    rng = np.random.default_rng(11)
+    src = rng.integers(0, (1 << 31) - 1, (4, 1 << L), dtype=np.uint32)
+    state = [int(x) for x in rng.integers(0, 1 << 32, 8, dtype=np.uint64)]
+    roots, alphas, last = O.fri_chain(src, state)
+    ch = Channel()
+    ch.state = struct.pack("<8I", *state)
+    cur = src
+    for k in range(L - 1):
+        a = ch.draw_felt()
+        assert tuple(alphas[k]) == tuple(a), k
+        if k == 0:
+            tw = O.fold_twiddles(O.coset("half_coset", L), True)
+            cur = O.fold_circle_into_line(np.zeros((4, 1 << (L - 1)), np.uint32), cur, tw, a)
+        else:
+            l = L - k
+            cur = O.fold_line(cur, O.fold_twiddles(O.coset("half_odds", l), False), a)
+        r = O.merkle_root([cur[c] for c in range(4)])
+        assert np.array_equal(r, roots[k]), k
+        ch.mix_digest(tuple(int(x) for x in r))
+    assert np.array_equal(cur.T, last)

@@ -91,6 +91,12 @@ _SIGS = {
                       C.POINTER(C.c_uint64)], C.c_int),
     "vx_autotune": ([u32, C.c_char_p, C.c_size_t], C.c_int),
     "vx_merkle_workspace_words": ([u32], C.c_uint64),
+    "vx_fri_chain_create": ([u32, C.POINTER(vp)], C.c_int),
+    "vx_fri_chain_destroy": [vp],
+    "vx_fri_chain_layers": ([vp], u32),
+    "vx_fri_chain_commit_async": ([vp, vp, vp, vp], C.c_int),
+    "vx_fri_chain_launches": ([vp], u32),
+    "vx_fri_chain_fetch": ([vp, vp, vp, vp, vp], C.c_int),
     "vx_merkle_root_cols": ([vp, u32, u32, vp, C.c_uint64, vp, vp], C.c_int),
     "vx_tune_set": ([u32, u32, u32, u32], C.c_int),
     "vx_tune_get": ([u32, u32, C.POINTER(u32), C.POINTER(u32)], C.c_int),

@@ -99,3 +99,44 @@ def fold_circle_into_line(dst: SecureColumn, src: SecureColumn, alpha, domain: C
 
 def fold_line(ev: SecureColumn, alpha, domain: Coset) -> SecureColumn:
     return fold_line_with_twiddles(ev, alpha, compute_fold_twiddles_on_demand(domain, False))
+
+
+class FriChain:
+    """FRI of a QM31 codeword on half_coset(log_size) with a commitment per
+    layer, down to 2 values (vx_fri_chain_*): the proof's FRI
+    (prover.rs:860-926) as one device call."""
+
+    def __init__(self, log_size: int):
+        self.log_size = log_size
+        self._h = C.c_void_p()
+        _lib.check(_lib.lib().vx_fri_chain_create(log_size, C.byref(self._h)))
+        self.layers = int(_lib.lib().vx_fri_chain_layers(self._h))
+
+    def commit_async(self, cols, state_words, stream=None) -> None:
+        """cols: 4 device tensors of 2^log_size words; state_words: 8 ints."""
+        ptrs = (C.c_void_p * 4)(*[c.data_ptr() for c in cols])
+        st = (C.c_uint32 * 8)(*[int(x) for x in state_words])
+        _lib.check(_lib.lib().vx_fri_chain_commit_async(self._h, ptrs, st, C.c_void_p(stream) if stream else None))
+
+    def result(self, stream=None):
+        """(roots [layers][8], alphas [layers][4], last [2][4]) after the stream drains."""
+        nl = self.layers
+        roots, alphas, last = (C.c_uint32 * (8 * nl))(), (C.c_uint32 * (4 * nl))(), (C.c_uint32 * 8)()
+        _lib.check(_lib.lib().vx_fri_chain_fetch(self._h, roots, alphas, last, C.c_void_p(stream) if stream else None))
+        return ([tuple(roots[8 * k: 8 * k + 8]) for k in range(nl)],
+                [tuple(alphas[4 * k: 4 * k + 4]) for k in range(nl)],
+                [tuple(last[0:4]), tuple(last[4:8])])
+
+    def launches(self) -> int:
+        return int(_lib.lib().vx_fri_chain_launches(self._h))
+
+    def close(self) -> None:
+        if self._h:
+            _lib.lib().vx_fri_chain_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
