@@ -333,6 +333,42 @@ def ntt_microbench(peak_gbs: float, sizes=(20, 24, 28), reps: int = 5):
     return out
 
 
+def stage_roofline_table(stages_ms: dict, log_n: int, peak_gbs: float, probe_rate: float) -> dict:
+    """Each proof stage against its bound, with the fixed algorithmic work:
+    HBM stages in bytes (NTT of m = 8m, zero-pad + evaluate = 4n + 4N, trace
+    written = 4n), hashing stages in Blake2s compressions (a tree of M leaves
+    of at most 16 words = 2M - 1) against the register-only probe; the folds
+    and the quotient fused into the hashing stages are listed as their bytes
+    beside the compressions."""
+    n, N = 1 << log_n, 1 << (log_n + 2)
+    layers = [N >> k for k in range(1, log_n + 2 - 3 + 1)]  # FRI layer sizes N/2 .. 8
+    line_bytes = sum(24 * m for m in layers[:-1])           # line fold M -> M/2 for M = N/2 .. 16
+    work = {
+        "trace": ("hbm", 4 * n, "bytes"),
+        "interpolate": ("hbm", 8 * n, "bytes"),
+        "lde_evaluate": ("hbm", 4 * n + 4 * N, "bytes"),
+        "trace_commit": ("int-alu", 2 * N - 1, "compressions"),
+        "quotient_commit": ("int-alu", 2 * N - 1, "compressions", 20 * N),
+        "circle_fold_commit": ("int-alu", 2 * (N // 2) - 1, "compressions", 24 * N),
+        "line_folds_commit": ("int-alu", sum(2 * m - 1 for m in layers[1:]), "compressions", line_bytes),
+    }
+    out = {}
+    for name, w in work.items():
+        ms = stages_ms.get(name)
+        if not ms:
+            continue
+        rate = w[1] / (ms / 1e3)
+        row = {"bound": w[0], "work": w[1], "unit": w[2], "ms": ms}
+        if w[0] == "hbm":
+            row.update(achieved_gbs=rate / 1e9, frac=rate / 1e9 / peak_gbs)
+        else:
+            row.update(achieved_per_s=rate, frac=rate / probe_rate, int_ops_per_s=1120 * rate)
+            if len(w) > 3:
+                row["fused_bytes"] = w[3]
+        out[name] = row
+    return out
+
+
 def _time_ms(fn, stream, reps):
     import torch
 
@@ -814,6 +850,7 @@ def main():
                              "achieved": merkle_rate, "peak": probe_rate, "unit": "compressions/s",
                              "frac": merkle_rate / probe_rate, "time_ms": tcommit_t * 1e3},
             "stages_ms": stages_ms,
+            "stage_rooflines": stage_roofline_table(stages_ms, log_n, peak, probe_rate),
             "gpu_launches": launches_per_proof * steps,
             "launches_per_proof": launches_per_proof,
             "clocks": clocks,
