@@ -114,6 +114,7 @@ struct Pass2Args {
     PassOff off;
     uint32_t s;       // lowest layer of the pass
     uint32_t scale;   // 1 = none
+    uint32_t vec;     // 1: columns and source 16-byte aligned, 4 consecutive elements per access
 };
 
 __device__ __forceinline__ uint32_t pad32(uint32_t e) { return e + (e >> 5); }
@@ -191,46 +192,85 @@ __global__ void __launch_bounds__((1 << (R + WL)) / 16) ntt_pass2_kernel(Pass2Ar
     const uint32_t *in = p.src ? p.src + (uint64_t)blockIdx.y * p.src_stride : col;
     const uint64_t gbase = (hb << (s + R)) | (cb << WL);
 
-    // twiddles of layer j (pass-relative) are h in [hb 2^(R-1-j), (hb+1) 2^(R-1-j));
-    // every load is issued before any shared-memory store so they overlap
-    constexpr int TWN = (1 << R) - 1;
-    constexpr int TWPT = (TWN + NT - 1) / NT;   // twiddle loads per thread
-    constexpr int DPT = TS / NT;                // 16 data loads per thread
-    uint32_t tv[TWPT];
+    constexpr int DPT = TS / NT;                // 16 data elements per thread
+    // Data loads first (their latency overlaps the twiddle loads).  The
+    // vector form moves 4 consecutive tile elements per access: a row of the
+    // tile is 2^WL >= 4 contiguous words (or the whole tile is contiguous,
+    // WL = 0 with s = 0), and 4-element groups start on multiples of 4.
+    uint32_t dv[DPT];
+    if (p.vec) {
 #pragma unroll
-    for (int k = 0; k < TWPT; k++) {
-        uint32_t f = tid + (uint32_t)k * NT;
-        if (f < (uint32_t)TWN) {
-            uint32_t lg = 31u - __clz(f + 1u);   // floor(log2(f + 1))
-            uint32_t j = R - 1 - lg;
-            uint32_t t = f + 1u - (1u << lg);
-            uint32_t L = s + j;
-            uint64_t h = (hb << lg) | t;
-            tv[k] = L ? __ldg(p.line + p.off.v[L - 1] + h) : circle_tw(p.circle, p.cmode, h);
+        for (int k = 0; k < DPT / 4; k++) {
+            const uint32_t e = 4u * (tid + (uint32_t)k * NT);
+            const uint64_t g = gbase | ((uint64_t)(e >> WL) << s) | (e & (W - 1u));
+            const uint4 q = *(const uint4 *)(in + (p.src ? (g & p.src_mask) : g));
+            dv[4 * k] = q.x; dv[4 * k + 1] = q.y; dv[4 * k + 2] = q.z; dv[4 * k + 3] = q.w;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < DPT; k++) {
+            const uint32_t e = tid + (uint32_t)k * NT;
+            const uint64_t g = gbase | ((uint64_t)(e >> WL) << s) | (e & (W - 1u));
+            dv[k] = in[p.src ? (g & p.src_mask) : g];
         }
     }
-    uint32_t dv[DPT];
+    // Twiddles of pass layer j are table words h in [hb 2^(R-1-j), (hb+1) 2^(R-1-j)),
+    // staged at smtw[2^(R-1-j) - 1 ..]; a flat index f decodes to (layer, offset).
+    // All loads are issued before the shared-memory stores.  (Per-layer loops
+    // over the contiguous runs measured slower: most of their predicated loads idle.)
+    {
+        constexpr int TWN = (1 << R) - 1;
+        constexpr int TWPT = (TWN + NT - 1) / NT;
+        uint32_t tv[TWPT];
 #pragma unroll
-    for (int k = 0; k < DPT; k++) {
-        uint32_t e = tid + (uint32_t)k * NT;
-        uint64_t g = gbase | ((uint64_t)(e >> WL) << s) | (e & (W - 1u));
-        dv[k] = in[p.src ? (g & p.src_mask) : g];
+        for (int k = 0; k < TWPT; k++) {
+            uint32_t f = tid + (uint32_t)k * NT;
+            if (f < (uint32_t)TWN) {
+                uint32_t lg = 31u - __clz(f + 1u);
+                uint32_t j = R - 1 - lg;
+                uint32_t t = f + 1u - (1u << lg);
+                uint32_t L = s + j;
+                uint64_t h = (hb << lg) | t;
+                tv[k] = L ? __ldg(p.line + p.off.v[L - 1] + h) : circle_tw(p.circle, p.cmode, h);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < TWPT; k++) {
+            uint32_t f = tid + (uint32_t)k * NT;
+            if (f < (uint32_t)TWN) smtw[f] = tv[k];
+        }
     }
+    if (p.vec) {
 #pragma unroll
-    for (int k = 0; k < TWPT; k++) {
-        uint32_t f = tid + (uint32_t)k * NT;
-        if (f < (uint32_t)TWN) smtw[f] = tv[k];
+        for (int k = 0; k < DPT / 4; k++) {
+            const uint32_t e = 4u * (tid + (uint32_t)k * NT);
+#pragma unroll
+            for (int q = 0; q < 4; q++) sm[pad32(e + q)] = dv[4 * k + q];
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < DPT; k++) sm[pad32(tid + (uint32_t)k * NT)] = dv[k];
     }
-#pragma unroll
-    for (int k = 0; k < DPT; k++) sm[pad32(tid + (uint32_t)k * NT)] = dv[k];
     __syncthreads();
     run_stages<FWD, R, WL, 0>(sm, smtw, tid);
+    if (p.vec) {
 #pragma unroll
-    for (int k = 0; k < DPT; k++) {
-        uint32_t e = tid + (uint32_t)k * NT;
-        uint64_t g = gbase | ((uint64_t)(e >> WL) << s) | (e & (W - 1u));
-        uint32_t v = sm[pad32(e)];
-        col[g] = p.scale != 1u ? mmul(v, p.scale) : v;
+        for (int k = 0; k < DPT / 4; k++) {
+            const uint32_t e = 4u * (tid + (uint32_t)k * NT);
+            const uint64_t g = gbase | ((uint64_t)(e >> WL) << s) | (e & (W - 1u));
+            uint32_t v[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) v[q] = p.scale != 1u ? mmul(sm[pad32(e + q)], p.scale) : sm[pad32(e + q)];
+            *(uint4 *)(col + g) = make_uint4(v[0], v[1], v[2], v[3]);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < DPT; k++) {
+            const uint32_t e = tid + (uint32_t)k * NT;
+            const uint64_t g = gbase | ((uint64_t)(e >> WL) << s) | (e & (W - 1u));
+            const uint32_t v = sm[pad32(e)];
+            col[g] = p.scale != 1u ? mmul(v, p.scale) : v;
+        }
     }
 }
 
@@ -415,6 +455,11 @@ cudaError_t ntt_transform_planned(uint32_t *data, uint32_t *const *dev_cols, uin
     }
     uint32_t ps[32], pr[32], pw[32];
     const uint32_t np = bottom_max ? ntt_plan(total, bottom_max, upper_max, ps, pr, pw) : plan_passes(total, ps, pr, pw);
+    // 16-byte accesses of 4 consecutive elements: contiguous columns with
+    // 16-byte aligned bases (a device pointer array is not inspected on the
+    // host, so it keeps the scalar form), a source of at least 4 words
+    const bool vec = !dev_cols && (((uintptr_t)data & 15u) == 0) && (n_cols == 1 || col_stride % 4u == 0) &&
+                     (!src || ((((uintptr_t)src & 15u) == 0) && src_log >= 2 && (n_cols == 1 || src_stride % 4u == 0)));
     for (uint32_t q = 0; q < np; q++) {
         uint32_t i = forward ? np - 1u - q : q;   // forward: top pass first
         Pass2Args a;
@@ -424,6 +469,7 @@ cudaError_t ntt_transform_planned(uint32_t *data, uint32_t *const *dev_cols, uin
         a.line = tw.line; a.circle = tw.circle; a.cmode = tw.circle_mode; a.off = off;
         a.s = ps[i];
         a.scale = (!forward && q == np - 1u) ? inv_n : 1u;
+        a.vec = (vec && (pw[i] >= 2u || ps[i] == 0u)) ? 1u : 0u;
         uint64_t tiles = (1ull << log_n) >> (pr[i] + pw[i]);
         e = forward ? dispatch_pass2<true>(pr[i], pw[i], a, tiles, n_cols, stream)
                     : dispatch_pass2<false>(pr[i], pw[i], a, tiles, n_cols, stream);
