@@ -118,14 +118,20 @@ struct Pass2Args {
 };
 
 __device__ __forceinline__ uint32_t pad32(uint32_t e) { return e + (e >> 5); }
+// pad32(a | b) = pad32(a) + b + (b >> 5) when a and b have no bit in common
+// (a shift distributes over OR, and an OR of disjoint fields is a sum).  The
+// stage and tile accesses below are all of this form with b a compile-time
+// offset, so each thread computes one padded base and the accesses use
+// immediate offsets.
 
 template <bool FWD, int R, int WL, int LO, int HI, int A>
 __device__ __forceinline__ void ntt_stage(uint32_t *sm, const uint32_t *smtw, uint32_t tid) {
     constexpr int TB = R + WL;
-    const uint32_t base = (tid & ((1u << A) - 1u)) | ((tid >> A) << (A + 4));
+    const uint32_t base = (tid & ((1u << A) - 1u)) | ((tid >> A) << (A + 4));  // bits [A, A+4) zero
+    const uint32_t pb = pad32(base);
     uint32_t v[16];
 #pragma unroll
-    for (int i = 0; i < 16; i++) v[i] = sm[pad32(base | ((uint32_t)i << A))];
+    for (int i = 0; i < 16; i++) v[i] = sm[pb + ((uint32_t)i << A) + (((uint32_t)i << A) >> 5)];
 #pragma unroll
     for (int jj = 0; jj < HI - LO; jj++) {
         const int j = FWD ? (HI - 1 - jj) : (LO + jj);
@@ -149,7 +155,7 @@ __device__ __forceinline__ void ntt_stage(uint32_t *sm, const uint32_t *smtw, ui
         }
     }
 #pragma unroll
-    for (int i = 0; i < 16; i++) sm[pad32(base | ((uint32_t)i << A))] = v[i];
+    for (int i = 0; i < 16; i++) sm[pb + ((uint32_t)i << A) + (((uint32_t)i << A) >> 5)] = v[i];
     (void)TB;
 }
 
@@ -240,16 +246,21 @@ __global__ void __launch_bounds__((1 << (R + WL)) / 16) ntt_pass2_kernel(Pass2Ar
             if (f < (uint32_t)TWN) smtw[f] = tv[k];
         }
     }
+    // tid < NT and k NT (resp. 4 tid + q and 4 k NT) have disjoint bits
+    const uint32_t ps1 = pad32(tid), ps4 = pad32(4u * tid);
     if (p.vec) {
 #pragma unroll
         for (int k = 0; k < DPT / 4; k++) {
-            const uint32_t e = 4u * (tid + (uint32_t)k * NT);
+            const uint32_t o = 4u * (uint32_t)k * NT;
 #pragma unroll
-            for (int q = 0; q < 4; q++) sm[pad32(e + q)] = dv[4 * k + q];
+            for (int q = 0; q < 4; q++) sm[ps4 + q + o + (o >> 5)] = dv[4 * k + q];
         }
     } else {
 #pragma unroll
-        for (int k = 0; k < DPT; k++) sm[pad32(tid + (uint32_t)k * NT)] = dv[k];
+        for (int k = 0; k < DPT; k++) {
+            const uint32_t o = (uint32_t)k * NT;
+            sm[ps1 + o + (o >> 5)] = dv[k];
+        }
     }
     __syncthreads();
     run_stages<FWD, R, WL, 0>(sm, smtw, tid);
@@ -258,9 +269,13 @@ __global__ void __launch_bounds__((1 << (R + WL)) / 16) ntt_pass2_kernel(Pass2Ar
         for (int k = 0; k < DPT / 4; k++) {
             const uint32_t e = 4u * (tid + (uint32_t)k * NT);
             const uint64_t g = gbase | ((uint64_t)(e >> WL) << s) | (e & (W - 1u));
+            const uint32_t o = 4u * (uint32_t)k * NT;
             uint32_t v[4];
 #pragma unroll
-            for (int q = 0; q < 4; q++) v[q] = p.scale != 1u ? mmul(sm[pad32(e + q)], p.scale) : sm[pad32(e + q)];
+            for (int q = 0; q < 4; q++) {
+                const uint32_t w = sm[ps4 + q + o + (o >> 5)];
+                v[q] = p.scale != 1u ? mmul(w, p.scale) : w;
+            }
             *(uint4 *)(col + g) = make_uint4(v[0], v[1], v[2], v[3]);
         }
     } else {
@@ -268,7 +283,8 @@ __global__ void __launch_bounds__((1 << (R + WL)) / 16) ntt_pass2_kernel(Pass2Ar
         for (int k = 0; k < DPT; k++) {
             const uint32_t e = tid + (uint32_t)k * NT;
             const uint64_t g = gbase | ((uint64_t)(e >> WL) << s) | (e & (W - 1u));
-            const uint32_t v = sm[pad32(e)];
+            const uint32_t o = (uint32_t)k * NT;
+            const uint32_t v = sm[ps1 + o + (o >> 5)];
             col[g] = p.scale != 1u ? mmul(v, p.scale) : v;
         }
     }
