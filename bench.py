@@ -700,7 +700,8 @@ def main():
         tuned = tune.autotune(tune_log)
         tuned = {"max_log": tune_log, "seconds": round(time.perf_counter() - t0, 2),
                  "ntt_plan": {k: v[:2] for k, v in tuned["ntt"].items()},
-                 "leaf_k": {k: v[0] for k, v in tuned["leaf_k"].items()}}
+                 "leaf_k": {k: v[0] for k, v in tuned["leaf_k"].items()},
+                 "fold_leaf_k": {k: v[0] for k, v in tuned["fold_leaf_k"].items()}}
 
     if args.batched_only:
         peak, _ = _peaks()

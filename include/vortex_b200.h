@@ -424,23 +424,27 @@ int vx_fri_chain_fetch(vx_fri_chain *h, uint32_t *roots, uint32_t *alphas, uint3
  * shapes (circle_ntt.cu: one launch per layer; blake2s.cu: one leaf per
  * thread).  On the current device, times every distinct NTT pass plan
  * (bottom pass of 10..12 layers, upper passes of at most 6..9) of each
- * transform length 13..max_log (shorter ones are a single pass), and the Merkle leaf kernel's subtree size
- * (2^1..2^4 leaves per thread) of each tree depth 17..max_log, on scratch
- * buffers of that size (about 16 * 2^max_log bytes, freed before return),
+ * transform length 13..max_log (shorter ones are a single pass), and the
+ * Merkle leaf kernel's subtree size (2^1..2^4 leaves per thread) of each tree
+ * depth 17..max_log, separately for narrow leaves (M31 columns) and for fold
+ * leaves (FRI layers, depths up to 25), on scratch buffers of that size
+ * (about 16 * 2^max_log + 52 * 2^min(max_log, 25) bytes, freed before return),
  * and keeps the fastest for later launches on this device.  Every choice
  * computes identical values, so proofs do not change.  Plans are read when
  * a transform is launched and when a tree is carved (prover slot or lifted
  * context creation), so tune before creating those.  Writes a JSON report
- * ({"ntt":{"log":[bottom,upper,ms]},"leaf_k":{"depth":[k,ms]}}) to `report`
+ * ({"ntt":{"log":[bottom,upper,ms]},"leaf_k":{"depth":[k,ms]},
+ * "fold_leaf_k":{"depth":[k,ms]}}) to `report`
  * (cap bytes, NUL-terminated, truncated).  12 <= max_log <= 28.  Not safe
  * to run while other host threads launch on the same device. */
 int vx_autotune(uint32_t max_log, char *report, size_t cap);
 /* Set one knob on the current device.  kind 0: NTT plan of `layers`-layer
  * transforms, a = bottom pass maximum (9..12), b = upper pass maximum
  * (3..9), a = 0 restores the default (12, 9).  kind 1: leaf kernel subtree
- * log for trees of depth `layers`, a in 1..4, 0 restores the default. */
+ * log for narrow-leaf trees of depth `layers`, a in 1..4, 0 restores the
+ * default; kind 2: the same for fold-leaf (FRI layer) trees. */
 int vx_tune_set(uint32_t kind, uint32_t layers, uint32_t a, uint32_t b);
-/* Read the knob that launches on the current device use (b = 0 for kind 1). */
+/* Read the knob that launches on the current device use (b = 0 for kinds 1, 2). */
 int vx_tune_get(uint32_t kind, uint32_t layers, uint32_t *a, uint32_t *b);
 /* Host-only: the pass plan of a `total`-layer transform (4..31) for a bottom
  * pass of at most bottom_max (9..12) layers and upper passes of at most

@@ -70,7 +70,9 @@ def test_proofs_identical_under_leaf_k_and_ntt_plans(oracle):
     for k in (1, 2, 3, 4):
         for d in range(le - 4, le + 1):
             tune.set_leaf_k(d, k)
+            tune.set_fold_leaf_k(d, 5 - k)
         assert tune.get(tune.LEAF_K, le)[0] == k
+        assert tune.get(tune.FOLD_LEAF_K, le - 1)[0] == 5 - k
         _proof(log_n, want)
     for bottom, upper in NTT_PLANS[:3]:
         for t in range(4, le + 1):
@@ -97,6 +99,10 @@ def test_autotune_report_and_results(oracle):
     rep = tune.autotune(19)
     assert sorted(rep["ntt"]) == list(range(13, 20))
     assert sorted(rep["leaf_k"]) == [17, 18, 19]
+    assert sorted(rep["fold_leaf_k"]) == [17, 18, 19]
+    for d, (k, ms) in rep["fold_leaf_k"].items():
+        assert 1 <= k <= 4 and ms > 0
+        assert tune.get(tune.FOLD_LEAF_K, d)[0] == k
     for t, (b, u, ms) in rep["ntt"].items():
         assert 10 <= b <= 12 and 6 <= u <= 9 and ms > 0
         assert tune.get(tune.NTT_PLAN, t) == (b, u)
@@ -109,6 +115,24 @@ def test_autotune_report_and_results(oracle):
 
 def test_tune_set_rejects_bad_knobs():
     from vortexstark_b200 import _lib
-    for args in ((0, 20, 8, 9), (0, 20, 12, 10), (1, 20, 5, 0), (2, 20, 1, 0), (0, 40, 12, 9)):
+    for args in ((0, 20, 8, 9), (0, 20, 12, 10), (1, 20, 5, 0), (2, 20, 5, 0), (3, 20, 1, 0), (0, 40, 12, 9)):
         with pytest.raises(_lib.VortexError):
             _lib.check(_lib.lib().vx_tune_set(*args))
+
+
+def test_fri_chain_identical_under_fold_leaf_k(oracle):
+    from vortexstark_b200.fri import FriChain
+    L = 19
+    src = np.stack([m31_array(500 + c, 1 << L) for c in range(4)])
+    state = list(range(8))
+    want = oracle.fri_chain(src, state)
+    cols = [to_dev(c) for c in src]
+    for k in (1, 2, 3, 4):
+        for d in range(17, 19):
+            tune.set_fold_leaf_k(d, k)
+        ch = FriChain(L)  # trees carved with the current knob
+        ch.commit_async(cols, state)
+        roots, alphas, last = ch.result()
+        ch.close()
+        assert np.array_equal(np.array(roots, np.uint32), want[0]), k
+        assert np.array_equal(np.array(last, np.uint32), want[2]), k

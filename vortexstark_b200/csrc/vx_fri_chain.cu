@@ -67,7 +67,7 @@ extern "C" int vx_fri_chain_create(uint32_t log_size, vx_fri_chain **out) {
     uint32_t kk[32];
     uint64_t o_t[32];
     for (uint32_t k = 0; k < h->nl; k++) {
-        kk[k] = tree_leaf_k(L - 1 - k);
+        kk[k] = tree_leaf_k(L - 1 - k, kLeafFold);
         o_t[k] = w;
         w += align64(tree_pool_words(L - 1 - k, kk[k]));
     }

@@ -312,9 +312,12 @@ constexpr uint32_t kReduceThreads = 128;
 uint64_t tree_plan(uint32_t depth, uint32_t *pool, TreeLevels *lv, uint32_t leaf_k);
 uint64_t tree_pool_words(uint32_t depth, uint32_t leaf_k);
 // Leaf-kernel subtree size (log2 of leaves per thread) for trees of this
-// depth on the current device, and the autotuner's override (1..4; 0 resets).
-uint32_t tree_leaf_k(uint32_t depth);
-void tree_knob_set(int dev, uint32_t depth, uint32_t k);
+// depth on the current device, and the autotuner's override (1..4; 0 resets),
+// per leaf kind: narrow leaves (columns of M31 words, the quotient, lifted
+// rows) and fold leaves (FRI layers: a QM31 fold of two loaded values).
+constexpr uint32_t kLeafNarrow = 0, kLeafFold = 1, kLeafKinds = 2;
+uint32_t tree_leaf_k(uint32_t depth, uint32_t kind = kLeafNarrow);
+void tree_knob_set(int dev, uint32_t depth, uint32_t k, uint32_t kind = kLeafNarrow);
 // Zero the group counters of a freshly carved tree.
 cudaError_t tree_reset(const TreeLevels &lv, cudaStream_t stream);
 

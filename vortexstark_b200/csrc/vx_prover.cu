@@ -426,7 +426,7 @@ extern "C" int vx_prover_create(uint32_t log_n, uint32_t blowup_bits, uint32_t n
     // leaf-kernel shapes read once: the pools are sized and carved with them
     const uint32_t kt = tree_leaf_k(le);
     uint32_t kf[32];
-    for (uint32_t k = 0; k < L.nfri; k++) kf[k] = tree_leaf_k(le - 1 - k);
+    for (uint32_t k = 0; k < L.nfri; k++) kf[k] = tree_leaf_k(le - 1 - k, kLeafFold);
     uint64_t o_tt = w; w += align_words(tree_pool_words(le, kt));
     uint64_t o_qt = w; w += align_words(tree_pool_words(le, kt));
     uint64_t o_ft[32];
@@ -785,7 +785,8 @@ extern "C" int vx_prove_fib_noalloc(uint32_t a, uint32_t b, uint32_t log_n, uint
     }
     w += align_words(tree_plan(le, base + w, &S.trace_lv, 0));
     w += align_words(tree_plan(le, base + w, &S.quot_lv, 0));
-    for (uint32_t k = 0; k < L.nfri; k++) w += align_words(tree_plan(le - 1 - k, base + w, &S.fri_lv[k], 0));
+    for (uint32_t k = 0; k < L.nfri; k++)
+        w += align_words(tree_plan(le - 1 - k, base + w, &S.fri_lv[k], tree_leaf_k(le - 1 - k, kLeafFold)));
     S.chan = (DevChannel *)(base + w); w += align_words(sizeof(DevChannel) / 4 + 1);
     S.alpha_q = base + w; w += align_words(4);
     S.alpha_f = base + w; w += align_words(4ull * (L.nfri + 1));
@@ -892,7 +893,7 @@ void prover_footprint(uint32_t log_n, uint32_t blowup, uint32_t nq, size_t *slot
     uint64_t w = align_words(n) + align_words(N);
     for (uint32_t k = 0; k < L.nfri; k++) w += 4 * align_words(1ull << (le - 1 - k));
     w += 2 * align_words(tree_pool_words(le, 0));
-    for (uint32_t k = 0; k < L.nfri; k++) w += align_words(tree_pool_words(le - 1 - k, 0));
+    for (uint32_t k = 0; k < L.nfri; k++) w += align_words(tree_pool_words(le - 1 - k, tree_leaf_k(le - 1 - k, kLeafFold)));
     w += align_words(sizeof(DevChannel) / 4 + 1) + align_words(4) + align_words(4ull * (L.nfri + 1)) +
          align_words(nq) + align_words(L.words);
     *slot_b = (size_t)(w * 4);

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "vx_common.cuh"
+#include "vx_fri.cuh"
 #include "vx_merkle.cuh"
 #include "vx_ntt.cuh"
 
@@ -58,11 +59,12 @@ extern "C" int vx_tune_set(uint32_t kind, uint32_t layers, uint32_t a, uint32_t 
         VX_CHECK_ARG(a == 0 || (a >= 9 && a <= 12 && b >= 3 && b <= 9),
                      "vx_tune_set: NTT plan needs bottom 9..12 and upper 3..9 (or 0 for the default)");
         ntt_knobs_set(dev, layers, a, b);
-    } else if (kind == 1) {
+    } else if (kind == 1 || kind == 2) {
         VX_CHECK_ARG(a <= 4, "vx_tune_set: leaf subtree log must be 0 (default) .. 4");
-        tree_knob_set(dev, layers, a);
+        tree_knob_set(dev, layers, a, kind == 1 ? kLeafNarrow : kLeafFold);
     } else {
-        VX_CHECK_ARG(false, "vx_tune_set: kind %u is not 0 (NTT plan) or 1 (leaf subtree)", kind);
+        VX_CHECK_ARG(false, "vx_tune_set: kind %u is not 0 (NTT plan), 1 (leaf subtree) or 2 (fold-leaf subtree)",
+                     kind);
     }
     return VX_OK;
 }
@@ -71,11 +73,11 @@ extern "C" int vx_tune_get(uint32_t kind, uint32_t layers, uint32_t *a, uint32_t
     VX_CHECK_ARG(a != nullptr && b != nullptr && layers < 32, "vx_tune_get: bad arguments");
     if (kind == 0) {
         ntt_knobs_get(layers, a, b);
-    } else if (kind == 1) {
-        *a = tree_leaf_k(layers);
+    } else if (kind == 1 || kind == 2) {
+        *a = tree_leaf_k(layers, kind == 1 ? kLeafNarrow : kLeafFold);
         *b = 0;
     } else {
-        VX_CHECK_ARG(false, "vx_tune_get: kind %u is not 0 or 1", kind);
+        VX_CHECK_ARG(false, "vx_tune_get: kind %u is not 0, 1 or 2", kind);
     }
     return VX_OK;
 }
@@ -97,11 +99,19 @@ extern "C" int vx_autotune(uint32_t max_log, char *report, size_t cap) {
     const uint64_t n = 1ull << max_log;
     // data (n words), line + circle tables (2n words), a Merkle pool (the
     // largest is the one with one leaf pair per thread)
-    const uint64_t pool_max = tree_pool_words(max_log, 1);
+    // every region starts on a 64-word (256-byte) boundary: the fold leaves
+    // read their inputs as 8-byte pairs, and a pool size can be odd
+    auto a64 = [](uint64_t w) { return (w + 63) & ~63ull; };
+    const uint64_t pool_max = a64(tree_pool_words(max_log, 1));
+    // fold-leaf trees up to depth 25 (the first FRI layer of a 2^26-point
+    // proof): 4 input columns of 2^(d+1) words, twiddles, 4 output columns
+    const uint32_t fold_max = max_log < 25 ? max_log : 25;
+    const uint64_t nf = 1ull << fold_max;
     Scratch sc;
-    const uint64_t words = 3 * n + pool_max + 64;
+    const uint64_t words = 3 * n + pool_max + 8 * nf + 4 * nf + nf + 64;
     VX_CUDA_TRY(cudaMalloc(&sc.p, words * 4));
     uint32_t *data = (uint32_t *)sc.p, *tab = data + n, *pool = tab + 2 * n;
+    uint32_t *fin = pool + pool_max, *fout = fin + 8 * nf, *ftw = fout + 4 * nf, *falpha = ftw + nf;
     VX_CUDA_TRY(cudaMemset(sc.p, 0, words * 4));
     cudaStream_t st = nullptr;
     cudaError_t err = cudaSuccess;
@@ -151,11 +161,32 @@ extern "C" int vx_autotune(uint32_t max_log, char *report, size_t cap) {
         snprintf(buf, sizeof(buf), "%s\"%u\":[%u,%.4f]", depth == 17 ? "" : ",", depth, bk, best);
         js += buf;
     }
+    js += "},\"fold_leaf_k\":{";
+    // ---- leaf-subtree sizes of fold-leaf (FRI layer) trees ----
+    for (uint32_t depth = 17; depth <= fold_max && err == cudaSuccess; depth++) {
+        float best = 1e30f;
+        uint32_t bk = 0;
+        const uint64_t m = 1ull << depth;
+        LeafFold lf{fin, fin + 2 * m, fin + 4 * m, fin + 6 * m, ftw, falpha,
+                    fout, fout + m, fout + 2 * m, fout + 3 * m, {}};
+        for (uint32_t k = 1; k <= 4; k++) {
+            TreeLevels lv;
+            tree_plan(depth, pool, &lv, k);
+            if ((err = tree_reset(lv, st)) != cudaSuccess) break;
+            float ms = time_ms([&] { return tree_build(lf, lv, ChanStep{nullptr, nullptr, nullptr}, st); }, st, 3, &err);
+            if (ms < best) { best = ms; bk = k; }
+        }
+        tree_knob_set(dev, depth, bk, kLeafFold);
+        char buf[96];
+        snprintf(buf, sizeof(buf), "%s\"%u\":[%u,%.4f]", depth == 17 ? "" : ",", depth, bk, best);
+        js += buf;
+    }
     js += "}}";
     if (err != cudaSuccess) {
         for (uint32_t l = 0; l < 32; l++) {  // back to the defaults
             ntt_knobs_set(dev, l, 0, 0);
-            tree_knob_set(dev, l, 0);
+            tree_knob_set(dev, l, 0, kLeafNarrow);
+            tree_knob_set(dev, l, 0, kLeafFold);
         }
         set_last_error(VX_ERR_CUDA, "vx_autotune: %s", cudaGetErrorString(err));
         return VX_ERR_CUDA;

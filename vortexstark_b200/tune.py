@@ -17,12 +17,13 @@ from . import _lib
 
 NTT_PLAN = 0
 LEAF_K = 1
+FOLD_LEAF_K = 2
 
 
 def autotune(max_log: int = 24) -> dict:
     """Tune transform lengths 13..max_log and tree depths 17..max_log on the
     current device.  Returns {"ntt": {log: [bottom, upper, ms]},
-    "leaf_k": {depth: [k, ms]}} with int keys."""
+    "leaf_k": {depth: [k, ms]}, "fold_leaf_k": {depth: [k, ms]}} with int keys."""
     buf = C.create_string_buffer(8192)
     _lib.check(_lib.lib().vx_autotune(max_log, buf, len(buf)))
     raw = json.loads(buf.value.decode())
@@ -36,8 +37,13 @@ def set_ntt_plan(layers: int, bottom: int = 0, upper: int = 0) -> None:
 
 
 def set_leaf_k(depth: int, k: int = 0) -> None:
-    """2^k leaves per leaf-kernel thread for trees of ``depth`` (1..4; 0 = default)."""
+    """2^k leaves per leaf-kernel thread for narrow-leaf trees of ``depth`` (1..4; 0 = default)."""
     _lib.check(_lib.lib().vx_tune_set(LEAF_K, depth, k, 0))
+
+
+def set_fold_leaf_k(depth: int, k: int = 0) -> None:
+    """The same for fold-leaf (FRI layer) trees."""
+    _lib.check(_lib.lib().vx_tune_set(FOLD_LEAF_K, depth, k, 0))
 
 
 def get(kind: int, layers: int) -> tuple[int, int]:
@@ -59,3 +65,4 @@ def reset(max_log: int = 31) -> None:
     for layers in range(max_log + 1):
         set_ntt_plan(layers)
         set_leaf_k(layers)
+        set_fold_leaf_k(layers)
