@@ -426,8 +426,9 @@ int vx_fri_chain_fetch(vx_fri_chain *h, uint32_t *roots, uint32_t *alphas, uint3
  * (bottom pass of 10..12 layers, upper passes of at most 6..9) of each
  * transform length 13..max_log (shorter ones are a single pass), and the
  * Merkle leaf kernel's subtree size (2^1..2^4 leaves per thread) of each tree
- * depth 17..max_log, separately for narrow leaves (M31 columns) and for fold
- * leaves (FRI layers, depths up to 25), on scratch buffers of that size
+ * depth 17..max_log, separately for narrow leaves (M31 columns) and for wide
+ * leaves (FRI folds, lifted rows; timed with fold leaves, depths up to 25),
+ * on scratch buffers of that size
  * (about 16 * 2^max_log + 52 * 2^min(max_log, 25) bytes, freed before return),
  * and keeps the fastest for later launches on this device.  Every choice
  * computes identical values, so proofs do not change.  Plans are read when
@@ -442,7 +443,8 @@ int vx_autotune(uint32_t max_log, char *report, size_t cap);
  * transforms, a = bottom pass maximum (9..12), b = upper pass maximum
  * (3..9), a = 0 restores the default (12, 9).  kind 1: leaf kernel subtree
  * log for narrow-leaf trees of depth `layers`, a in 1..4, 0 restores the
- * default; kind 2: the same for fold-leaf (FRI layer) trees. */
+ * default; kind 2: the same for wide-leaf trees (FRI layers, lifted rows,
+ * their combinations). */
 int vx_tune_set(uint32_t kind, uint32_t layers, uint32_t a, uint32_t b);
 /* Read the knob that launches on the current device use (b = 0 for kinds 1, 2). */
 int vx_tune_get(uint32_t kind, uint32_t layers, uint32_t *a, uint32_t *b);

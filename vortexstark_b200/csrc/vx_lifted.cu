@@ -476,7 +476,7 @@ extern "C" int vx_lifted_create(uint32_t n_cols, const uint32_t *log_sizes, uint
     uint64_t o_F[kMaxFri];
     for (uint32_t k = 0; k < L.nfri; k++) { o_F[k] = w; w += 4 * align64(1ull << (S - 1 - k)); }
     // leaf-kernel shapes read once: the pools are sized and carved with them
-    const uint32_t kt = tree_leaf_k(S);
+    const uint32_t kt = tree_leaf_k(S, kLeafFold);  // 34-word rows and combinations: wide leaves
     uint32_t kf[kMaxFri];
     for (uint32_t k = 0; k < L.nfri; k++) kf[k] = tree_leaf_k(S - 1 - k, kLeafFold);
     const uint64_t o_t0 = w; w += align64(tree_pool_words(S, kt));

@@ -37,7 +37,7 @@ uint32_t tree_leaf_k(uint32_t depth, uint32_t kind) {
     if (kind >= kLeafKinds) kind = kLeafNarrow;
     if (dev >= 0 && dev < 64 && g_leaf_k_init[dev] && depth < 32 && g_leaf_k[dev][kind][depth])
         return g_leaf_k[dev][kind][depth];
-    // Fold leaves (32 bytes of input and a QM31 fold per leaf): 4 leaves per
+    // Wide leaves (a fold of 32 bytes of input, a lifted row): 4 leaves per
     // thread, so more threads keep their loads in flight (measured on a
     // 2^26-point FRI chain: 6.08 ms against 6.82 ms with 16 per thread).
     if (kind == kLeafFold) return 2u;

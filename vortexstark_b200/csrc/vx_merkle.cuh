@@ -313,8 +313,10 @@ uint64_t tree_plan(uint32_t depth, uint32_t *pool, TreeLevels *lv, uint32_t leaf
 uint64_t tree_pool_words(uint32_t depth, uint32_t leaf_k);
 // Leaf-kernel subtree size (log2 of leaves per thread) for trees of this
 // depth on the current device, and the autotuner's override (1..4; 0 resets),
-// per leaf kind: narrow leaves (columns of M31 words, the quotient, lifted
-// rows) and fold leaves (FRI layers: a QM31 fold of two loaded values).
+// per leaf kind: narrow leaves (a few M31 words: trace columns, the quotient)
+// and wide leaves, whose load is heavy (FRI layers: a QM31 fold of two loaded
+// values; lifted rows of many columns; their combinations).  Wide leaves
+// want small subtrees: each thread's leaves wait on their loads in turn.
 constexpr uint32_t kLeafNarrow = 0, kLeafFold = 1, kLeafKinds = 2;
 uint32_t tree_leaf_k(uint32_t depth, uint32_t kind = kLeafNarrow);
 void tree_knob_set(int dev, uint32_t depth, uint32_t k, uint32_t kind = kLeafNarrow);

@@ -42,7 +42,7 @@ def set_leaf_k(depth: int, k: int = 0) -> None:
 
 
 def set_fold_leaf_k(depth: int, k: int = 0) -> None:
-    """The same for fold-leaf (FRI layer) trees."""
+    """The same for wide-leaf trees (FRI layers, lifted rows, their combinations)."""
     _lib.check(_lib.lib().vx_tune_set(FOLD_LEAF_K, depth, k, 0))
 
 
