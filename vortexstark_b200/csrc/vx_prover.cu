@@ -83,45 +83,80 @@ static void proof_template(const ProofLayout &L, std::vector<uint32_t> &t) {
 // ---------------------------------------------------------------------
 namespace {
 
-// (F(k), F(k+1)) of the sequence F(0)=a, F(1)=b by 2x2 matrix power (air.rs:85-131).
-__device__ void fib_at(uint32_t a, uint32_t b, uint64_t k, uint32_t &fk, uint32_t &fk1) {
-    uint32_t m00 = 1, m01 = 0, m10 = 0, m11 = 1, b00 = 1, b01 = 1, b10 = 1, b11 = 0;
-    while (k) {
-        if (k & 1) {
-            uint32_t t00 = madd(mmul(m00, b00), mmul(m01, b10)), t01 = madd(mmul(m00, b01), mmul(m01, b11));
-            uint32_t t10 = madd(mmul(m10, b00), mmul(m11, b10)), t11 = madd(mmul(m10, b01), mmul(m11, b11));
-            m00 = t00; m01 = t01; m10 = t10; m11 = t11;
+// Chunk seeds by matrix powers, as the reference's parallel trace does
+// (air.rs:85-131).  Standard Fibonacci numbers mod P, built at compile time: fib(k - 1),
+// fib(k), fib(k + 1) for k = 32 t (t < 256) and for k = 2^j (j < 32).
+// With G(k) = a fib(k - 1) + b fib(k), the sequence from (a, b) satisfies
+// G(s + k) = G(s) fib(k - 1) + G(s + 1) fib(k) and
+// G(s + k + 1) = G(s) fib(k) + G(s + 1) fib(k + 1).
+struct FibTab { uint32_t chunk[256][3]; uint32_t pow2[32][3]; };
+constexpr uint32_t cadd_(uint32_t x, uint32_t y) { return (uint32_t)(((uint64_t)x + y) % VX_P); }
+constexpr uint32_t cmul_(uint32_t x, uint32_t y) { return (uint32_t)(((uint64_t)x * y) % VX_P); }
+constexpr FibTab make_fib_tab() {
+    FibTab t{};
+    uint32_t f0 = 1, f1 = 0;  // fib(-1), fib(0)
+    for (uint32_t k = 0; k <= 8192; k++) {   // at step k: f0 = fib(k - 1), f1 = fib(k)
+        if (k % 32 == 0 && k / 32 < 256) {
+            t.chunk[k / 32][0] = f0; t.chunk[k / 32][1] = f1; t.chunk[k / 32][2] = cadd_(f0, f1);
         }
-        uint32_t t00 = madd(mmul(b00, b00), mmul(b01, b10)), t01 = madd(mmul(b00, b01), mmul(b01, b11));
-        uint32_t t10 = madd(mmul(b10, b00), mmul(b11, b10)), t11 = madd(mmul(b10, b01), mmul(b11, b11));
-        b00 = t00; b01 = t01; b10 = t10; b11 = t11;
-        k >>= 1;
-    }
-    fk = madd(mmul(m10, b), mmul(m11, a));
-    fk1 = madd(mmul(m00, b), mmul(m01, a));
-}
-
-// Fibonacci trace t0 = a, t1 = b, t_{i+2} = t_i + t_{i+1} (air.rs:16-25),
-// chunks of 32 rows per thread seeded by fib_at.  Also stamps (a, b) into
-// the proof header.
-__global__ void fib_trace_kernel(uint32_t a, uint32_t b, const uint32_t *ab_dev, uint32_t *out, uint64_t n,
-                                 uint32_t *proof_ab) {
-    uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t C = 32;
-    uint64_t s = t * C;
-    if (ab_dev) { a = ab_dev[0]; b = ab_dev[1]; }
-    if (t == 0) { proof_ab[0] = a; proof_ab[1] = b; }
-    if (s >= n) return;
-    uint32_t f0, f1;
-    fib_at(a, b, s, f0, f1);
-    uint32_t cnt = (uint32_t)((n - s) < C ? (n - s) : C);
-    out[s] = f0;
-    if (cnt > 1) out[s + 1] = f1;
-    for (uint32_t i = 2; i < cnt; i++) {
-        uint32_t f2 = madd(f0, f1);
-        out[s + i] = f2;
+        const uint32_t f2 = cadd_(f0, f1);
         f0 = f1; f1 = f2;
     }
+    // the matrix [[fib(k+1), fib(k)], [fib(k), fib(k-1)]] squared gives 2k
+    uint32_t m = 0, p = 1, q = 1;  // fib(k-1), fib(k), fib(k+1) for k = 1
+    for (uint32_t j = 0; j < 32; j++) {
+        t.pow2[j][0] = m; t.pow2[j][1] = p; t.pow2[j][2] = q;
+        const uint32_t m2 = cadd_(cmul_(p, p), cmul_(m, m)), p2 = cadd_(cmul_(q, p), cmul_(p, m)),
+                       q2 = cadd_(cmul_(q, q), cmul_(p, p));
+        m = m2; p = p2; q = q2;
+    }
+    return t;
+}
+__constant__ FibTab kFib = make_fib_tab();
+
+// (G(s + k), G(s + k + 1)) from (G(s), G(s + 1)) and (fib(k-1), fib(k), fib(k+1)).
+__device__ __forceinline__ void fib_step(uint32_t &g0, uint32_t &g1, const uint32_t f[3]) {
+    const uint32_t n0 = madd(mmul(g0, f[0]), mmul(g1, f[1]));
+    const uint32_t n1 = madd(mmul(g0, f[1]), mmul(g1, f[2]));
+    g0 = n0; g1 = n1;
+}
+
+// Fibonacci trace t0 = a, t1 = b, t_{i+2} = t_i + t_{i+1} (air.rs:16-25).
+// A block of 256 threads writes 8192 rows: thread 0 builds the block's seed
+// (G(base), G(base + 1)) from the powers-of-two table, every thread derives
+// its 32-row chunk's seed with one table step, runs the recurrence into
+// shared memory, and the block writes its rows coalesced.  Also stamps
+// (a, b) into the proof header.
+constexpr uint32_t kTraceRows = 8192;
+__global__ void __launch_bounds__(256) fib_trace_kernel(uint32_t a, uint32_t b, const uint32_t *ab_dev, uint32_t *out,
+                                                        uint64_t n, uint32_t *proof_ab) {
+    __shared__ uint32_t rows[256 * 33];
+    __shared__ uint32_t seed[2];
+    if (ab_dev) { a = ab_dev[0]; b = ab_dev[1]; }
+    if (blockIdx.x == 0 && threadIdx.x == 0) { proof_ab[0] = a; proof_ab[1] = b; }
+    const uint64_t base = (uint64_t)blockIdx.x * kTraceRows;
+    if (threadIdx.x == 0) {
+        uint32_t g0 = a, g1 = b;
+        for (uint32_t j = 13; j < 32 && (base >> j); j++)  // base < 2^31
+            if ((base >> j) & 1ull) fib_step(g0, g1, kFib.pow2[j]);
+        seed[0] = g0; seed[1] = g1;
+    }
+    __syncthreads();
+    const uint32_t t = threadIdx.x;
+    uint32_t f0 = seed[0], f1 = seed[1];
+    fib_step(f0, f1, kFib.chunk[t]);
+    uint32_t *r = rows + 33 * t;
+    r[0] = f0;
+    r[1] = f1;
+#pragma unroll
+    for (uint32_t i = 2; i < 32; i++) {
+        const uint32_t f2 = madd(f0, f1);
+        r[i] = f2;
+        f0 = f1; f1 = f2;
+    }
+    __syncthreads();
+    const uint64_t cnt = (n - base) < kTraceRows ? (n - base) : kTraceRows;
+    for (uint32_t e = t; e < cnt; e += 256) out[base + e] = rows[33 * (e >> 5) + (e & 31u)];
 }
 
 // mix_felts(last layer) (channel.rs:46-59) then n_queries x draw_number(N)
@@ -508,7 +543,7 @@ static int enqueue_stage(vx_prover *p, uint32_t stage, uint32_t a, uint32_t b, c
     switch (stage) {
     case 0:
         VX_CUDA_TRY(cudaMemsetAsync(S.chan, 0, sizeof(DevChannel), st));
-        fib_trace_kernel<<<blocks_for((n + 31) / 32, 256), 256, 0, st>>>(a, b, S.inputs, S.coeffs, n,
+        fib_trace_kernel<<<(unsigned)((n + kTraceRows - 1) / kTraceRows), 256, 0, st>>>(a, b, S.inputs, S.coeffs, n,
                                                                          proof + L.magic + 3);
         *launches += 1;
         break;
