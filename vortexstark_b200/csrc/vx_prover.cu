@@ -191,19 +191,33 @@ __global__ void chan_queries_kernel(DevChannel *ch, const uint32_t *l0, const ui
 
 // ---- fused fold + commitment leaf sources (fri.cu:58-126) ----
 // Circle fold of the quotient into FRI layer 0: output j pairs q[2j], q[2j+1].
+// Both values are alpha_q times an M31 word (c0, c1), so
+//   (f0 + f1) + alpha_f tw (f0 - f1) = alpha_q s + beta d,
+// with s = c0 + c1, d = tw (c0 - c1) in M31 and beta = alpha_f alpha_q
+// formed once per thread: each output word is a dot product of two
+// products, reduced once (the same field values as folding the two QM31s).
 struct LeafCircleFold {
     LeafQuotient q;
     const uint32_t *tw;
     const uint32_t *alpha_ptr;
     uint32_t *o0, *o1, *o2, *o3;
-    qmat am;  // multiplication by the fold challenge
+    uint32_t beta[4];
     __device__ __forceinline__ void init() {
         q.init();
-        am = qmat_of(qm31{{alpha_ptr[0], alpha_ptr[1], alpha_ptr[2], alpha_ptr[3]}});
+        const qm31 b = qmul(qm31{{alpha_ptr[0], alpha_ptr[1], alpha_ptr[2], alpha_ptr[3]}},
+                            qm31{{q.al[0], q.al[1], q.al[2], q.al[3]}});
+#pragma unroll
+        for (int c = 0; c < 4; c++) beta[c] = b.v[c];
     }
     __device__ __forceinline__ uint32_t load(uint64_t j, uint32_t m[16]) const {
-        qm31 f0 = q.value(2 * j), f1 = q.value(2 * j + 1);
-        qm31 r = qadd(qadd(f0, f1), qmul_mat(am, qmulm(qsub(f0, f1), __ldg(tw + j))));
+        const uint64_t i = 2 * j, mk = q.mask;
+        const uint32_t t0 = __ldg(q.eval + i), t1 = __ldg(q.eval + ((i + 1) & mk));
+        const uint32_t t2 = __ldg(q.eval + ((i + 2) & mk)), t3 = __ldg(q.eval + ((i + 3) & mk));
+        const uint32_t c0 = msub(t2, madd(t1, t0)), c1 = msub(t3, madd(t2, t1));
+        const uint32_t s = madd(c0, c1), d = mmul(msub(c0, c1), __ldg(tw + j));
+        qm31 r;
+#pragma unroll
+        for (int c = 0; c < 4; c++) r.v[c] = reduce64((uint64_t)q.al[c] * s + (uint64_t)beta[c] * d);
         o0[j] = r.v[0]; o1[j] = r.v[1]; o2[j] = r.v[2]; o3[j] = r.v[3];
         m[0] = r.v[0]; m[1] = r.v[1]; m[2] = r.v[2]; m[3] = r.v[3];
         return 16u;
