@@ -471,8 +471,19 @@ int vx_ntt_plan(uint32_t total, uint32_t bottom_max, uint32_t upper_max, uint32_
 int vx_prove_fib_noalloc(uint32_t a, uint32_t b, uint32_t log_n, uint32_t blowup_bits, uint32_t n_queries,
                          uint8_t *out, size_t cap, size_t *out_len);
 
-/* Free the slots cached by vx_prove_fib on every device; a size's shared
- * tables are freed with the last slot (of any owner) that uses them. */
+/* Many proofs of one size — replaces ProverPipeline::prove_batch
+ * (prover.rs:2278-2311), which proves its inputs one after another with a
+ * shared cache.  Proves (a[i], b[i]) for i < count into out + i *
+ * *proof_size (cap >= count * vx_proof_size bytes), each proof
+ * byte-identical to vx_prove_fib's.  Two cached slots on two streams keep
+ * two proofs in flight, so one proof's latency-bound FRI tail overlaps the
+ * next one's hashing.  Returns when all proofs are in `out`. */
+int vx_prove_fib_batch(const uint32_t *a, const uint32_t *b, uint32_t count, uint32_t log_n, uint32_t blowup_bits,
+                       uint32_t n_queries, uint8_t *out, size_t cap, size_t *proof_size);
+
+/* Free the slots cached by vx_prove_fib and vx_prove_fib_batch on every
+ * device; a size's shared tables are freed with the last slot (of any
+ * owner) that uses them. */
 void vx_release_all(void);
 
 #ifdef __cplusplus

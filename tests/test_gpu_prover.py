@@ -87,3 +87,33 @@ def test_concurrent_slots_on_streams(oracle):
     torch.cuda.synchronize()
     for c, s, (a, b) in zip(caches, sizes, ins):
         assert c.result_bytes() == oracle.prove(a, b, s)
+
+
+@pytest.mark.parametrize("log_n,count", [(8, 1), (8, 2), (10, 5), (14, 4), (18, 3)])
+def test_prove_batch_matches_single_proofs(oracle, log_n, count):
+    """vx_prove_fib_batch (ProverPipeline::prove_batch, prover.rs:2305) gives the
+    proofs that vx_prove_fib and the oracle give, in input order."""
+    inputs = fib_inputs(900 + log_n, count)
+    got = prover.prove_batch_bytes(inputs, log_n)
+    assert len(got) == count
+    for (a, b), blob in zip(inputs, got):
+        assert blob == prover.prove_bytes(a, b, log_n)
+    for (a, b), blob in list(zip(inputs, got))[:2]:
+        assert blob == oracle.prove(a, b, log_n)
+
+
+def test_prove_batch_arguments():
+    import ctypes as C
+
+    from vortexstark_b200 import _lib
+    assert prover.prove_batch_bytes([], 8) == []
+    size = prover.proof_size(8)
+    a = (C.c_uint32 * 2)(1, 2)
+    b = (C.c_uint32 * 2)(3, 0x7FFFFFFF)  # the second input is not canonical
+    buf = (C.c_uint8 * (2 * size))()
+    n = C.c_size_t()
+    L = _lib.lib()
+    with pytest.raises(_lib.VortexError):
+        _lib.check(L.vx_prove_fib_batch(a, b, 2, 8, 2, 80, buf, 2 * size, C.byref(n)))
+    with pytest.raises(_lib.VortexError):
+        _lib.check(L.vx_prove_fib_batch(a, a, 2, 8, 2, 80, buf, 2 * size - 1, C.byref(n)))

@@ -730,11 +730,117 @@ extern "C" int vx_prove_fib(uint32_t a, uint32_t b, uint32_t log_n, uint32_t blo
     return VX_OK;
 }
 
+// ---- batch: ProverPipeline::prove_batch (prover.rs:2278-2311) ----
+// Two slots of one size on two non-blocking streams keep two proofs in
+// flight: one proof's latency-bound FRI tail overlaps the next one's trace,
+// LDE and hashing.  Each slot's proof bytes and status word come back
+// through its own pinned buffer while the other slot proves.
+namespace {
+struct BatchCtx {
+    vx_prover *slot[2] = {nullptr, nullptr};
+    cudaStream_t st[2] = {nullptr, nullptr};
+    uint8_t *pinned[2] = {nullptr, nullptr};
+    cudaEvent_t done[2] = {nullptr, nullptr};
+};
+std::map<std::tuple<int, uint32_t, uint32_t, uint32_t>, BatchCtx> g_batch;
+
+void batch_free(BatchCtx &c) {
+    for (int k = 0; k < 2; k++) {
+        if (c.done[k]) cudaEventDestroy(c.done[k]);
+        if (c.pinned[k]) cudaFreeHost(c.pinned[k]);
+        if (c.st[k]) cudaStreamDestroy(c.st[k]);
+        if (c.slot[k]) vx_prover_destroy(c.slot[k]);
+    }
+    c = BatchCtx{};
+}
+
+int batch_ctx(int dev, uint32_t log_n, uint32_t blowup_bits, uint32_t n_queries, size_t bytes, BatchCtx **out) {
+    auto key = std::make_tuple(dev, log_n, blowup_bits, n_queries);
+    auto it = g_batch.find(key);
+    if (it != g_batch.end()) { *out = &it->second; return VX_OK; }
+    BatchCtx c;
+    int rc = VX_OK;
+    for (int k = 0; k < 2 && rc == VX_OK; k++) {
+        rc = vx_prover_create(log_n, blowup_bits, n_queries, &c.slot[k]);
+        if (rc == VX_OK && (cudaStreamCreateWithFlags(&c.st[k], cudaStreamNonBlocking) != cudaSuccess ||
+                            cudaHostAlloc((void **)&c.pinned[k], bytes + 16, cudaHostAllocDefault) != cudaSuccess ||
+                            cudaEventCreateWithFlags(&c.done[k], cudaEventDisableTiming) != cudaSuccess)) {
+            cudaGetLastError();
+            set_last_error(VX_ERR_OOM, "vx_prove_fib_batch: stream, pinned buffer or event creation failed");
+            rc = VX_ERR_OOM;
+        }
+    }
+    if (rc != VX_OK) { batch_free(c); return rc; }
+    *out = &(g_batch[key] = c);
+    return VX_OK;
+}
+}  // namespace
+
+extern "C" int vx_prove_fib_batch(const uint32_t *a, const uint32_t *b, uint32_t count, uint32_t log_n,
+                                  uint32_t blowup_bits, uint32_t n_queries, uint8_t *out, size_t cap,
+                                  size_t *proof_size) {
+    VX_CHECK_ARG(a != nullptr && b != nullptr && out != nullptr && proof_size != nullptr,
+                 "vx_prove_fib_batch: null argument");
+    const size_t need = vx_proof_size(log_n, blowup_bits, n_queries);
+    VX_CHECK_ARG(need != 0, "vx_prove_fib_batch: unsupported size log_n=%u blowup_bits=%u", log_n, blowup_bits);
+    VX_CHECK_ARG(cap / need >= count, "vx_prove_fib_batch: output capacity %zu < %u proofs of %zu bytes", cap, count,
+                 need);
+    for (uint32_t i = 0; i < count; i++)
+        VX_CHECK_ARG(a[i] < VX_P && b[i] < VX_P, "vx_prove_fib_batch: input %u is not canonical M31", i);
+    *proof_size = need;
+    if (count == 0) return VX_OK;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(g_slot_mu);
+    BatchCtx *c = nullptr;
+    int rc = batch_ctx(dev, log_n, blowup_bits, n_queries, need, &c);
+    if (rc) return rc;
+    // collect proof i (slot i % 2): wait for its stream, copy out, check its status word
+    auto collect = [&](uint32_t i) -> int {
+        const int k = (int)(i & 1u);
+        VX_CUDA_TRY(cudaEventSynchronize(c->done[k]));
+        uint32_t err = 0;
+        memcpy(&err, c->pinned[k] + need, 4);
+        if (err) {
+            set_last_error(VX_ERR_DEVICE, "vx_prove_fib_batch: proof %u: transcript rejection sampling exceeded its bound",
+                           i);
+            return VX_ERR_DEVICE;
+        }
+        memcpy(out + (size_t)i * need, c->pinned[k], need);
+        return VX_OK;
+    };
+    uint32_t launched = 0, collected = 0;
+    for (uint32_t i = 0; i < count && rc == VX_OK; i++) {
+        const int k = (int)(i & 1u);
+        if (i >= 2) {
+            rc = collect(i - 2);
+            collected = i - 1;
+            if (rc) break;
+        }
+        vx_prover *p = c->slot[k];
+        rc = vx_prover_prove_async(p, a[i], b[i], c->st[k]);
+        if (rc) break;
+        VX_CUDA_TRY(cudaMemcpyAsync(c->pinned[k], p->s.proof, need, cudaMemcpyDeviceToHost, c->st[k]));
+        VX_CUDA_TRY(cudaMemcpyAsync(c->pinned[k] + need, &p->s.chan->err, 4, cudaMemcpyDeviceToHost, c->st[k]));
+        VX_CUDA_TRY(cudaEventRecord(c->done[k], c->st[k]));
+        launched = i + 1;
+    }
+    // drain what is still in flight, even after an error, so no copy lands later
+    for (uint32_t i = collected; i < launched; i++) {
+        const int r2 = collect(i);
+        if (rc == VX_OK) rc = r2;
+    }
+    return rc;
+}
+
 extern "C" void vx_release_all(void) {
-    // the cached slots of vx_prove_fib; each size's tables go with their last slot
+    // the cached slots of vx_prove_fib and vx_prove_fib_batch; each size's
+    // tables go with their last slot
     std::lock_guard<std::mutex> lk(g_slot_mu);
     for (auto &kv : g_slots) vx_prover_destroy(kv.second);
     g_slots.clear();
+    for (auto &kv : g_batch) batch_free(kv.second);
+    g_batch.clear();
 }
 
 // ---------------------------------------------------------------------

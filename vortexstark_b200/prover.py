@@ -42,6 +42,26 @@ def prove_bytes(a: int, b: int, log_n: int, blowup_bits: int = BLOWUP_BITS, n_qu
     return bytes(memoryview(buf)[: n.value])
 
 
+def prove_batch_bytes(inputs, log_n: int, blowup_bits: int = BLOWUP_BITS, n_queries: int = N_QUERIES,
+                      out: bytearray | None = None) -> list[bytes]:
+    """ProverPipeline::prove_batch (prover.rs:2305-2311) through the C ABI
+    (vx_prove_fib_batch): the proofs of [(a, b), ...], two in flight."""
+    pairs = list(inputs)
+    for a, b in pairs:
+        _check_inputs(a, b, log_n, blowup_bits)
+    size = proof_size(log_n, blowup_bits, n_queries)
+    n = len(pairs)
+    buf = out if out is not None and len(out) >= n * size else bytearray(max(n, 1) * size)
+    av = (C.c_uint32 * max(n, 1))(*[p[0] for p in pairs])
+    bv = (C.c_uint32 * max(n, 1))(*[p[1] for p in pairs])
+    got = C.c_size_t()
+    _lib.check(_lib.lib().vx_prove_fib_batch(av, bv, n, log_n, blowup_bits, n_queries,
+                                              C.addressof((C.c_uint8 * len(buf)).from_buffer(buf)), len(buf),
+                                              C.byref(got)))
+    mv = memoryview(buf)
+    return [bytes(mv[i * size:(i + 1) * size]) for i in range(n)]
+
+
 def prove(a: int, b: int, log_n: int) -> StarkProof:
     """prover.rs:221 — prove the Fibonacci AIR with public inputs (a, b)."""
     return deserialize_proof(prove_bytes(a, b, log_n))
