@@ -609,6 +609,25 @@ def blake2s_probe_rate(stream) -> float:
     return 148 * 8 * 256 * iters / (pa.elapsed_time(pb) / 1e3)
 
 
+def max_over_ranks(values, dist, device="cpu"):
+    """Each value's maximum over the ranks (a replica job is as slow as its
+    slowest GPU); the values themselves when there is one rank."""
+    if dist is None:
+        return list(values)
+    import torch
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.cpu()]
+
+
+def rank_inputs(rank: int, count: int):
+    """Public inputs of one rank's proofs: a replica per GPU, each its own seeded stream."""
+    from vortexstark_b200.workload import fib_inputs
+
+    return fib_inputs(SEED + rank, count)
+
+
 def run_reference(args, rank: int):
     """CPU oracle arm: each step one proof of the workload (or a bounded
     sample of it), all host threads."""
@@ -626,7 +645,7 @@ def run_reference(args, rank: int):
     t0 = time.perf_counter()
     O.prove(a, b, 20)
     t20 = time.perf_counter() - t0
-    per = t20 * (1 << (args.log_n - 20)) * (args.log_n + 2) / 22.0
+    per = t20 * 2.0 ** (args.log_n - 20) * (args.log_n + 2) / 22.0
     full = per * args.steps <= 240.0
     k = args.log_n if full else args.log_n - 2
     scale = 1.0 if full else (1 << (args.log_n - k)) * (args.log_n + 2) / (k + 2)
@@ -722,7 +741,7 @@ def main():
     cache = prover.ProverCache(log_n)
     cache2 = prover.ProverCache(log_n)  # a second slot: two proofs in flight
     size = cache.size
-    ins = fib_inputs(SEED + rank, args.steps + args.warmup)
+    ins = rank_inputs(rank, args.steps + args.warmup)
     stream = torch.cuda.Stream()
     stream2 = torch.cuda.Stream()
     s = stream.cuda_stream
@@ -846,11 +865,8 @@ def main():
     stages_ms = {name: statistics.median([st_ev[r][k].elapsed_time(st_ev[r][k + 1]) for r in range(reps)])
                  for k, name in enumerate(stage_names)}
 
-    # max over ranks
-    if dist is not None:
-        t = torch.tensor([dev_ms, t_all, dev_ms_one], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_ms, t_all, dev_ms_one = float(t[0]), float(t[1]), float(t[2])
+    # the job's times are its slowest rank's
+    dev_ms, t_all, dev_ms_one = max_over_ranks([dev_ms, t_all, dev_ms_one], dist, "cuda")
 
     steps = args.steps
     value = world * steps / (dev_ms / 1e3)
