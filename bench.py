@@ -685,6 +685,9 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched lifted commitment")
     ap.add_argument("--no-micro", action="store_true", help="skip the NTT / iNTT microbench (2^20, 2^24, 2^28)")
     ap.add_argument("--no-tune", action="store_true", help="keep the built-in NTT plans and leaf-kernel shapes")
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="run only the standalone kernel microbench (Merkle, FRI folds, bit reversals) and print it")
+    ap.add_argument("--kernel-log", type=int, default=26, help="log2 size of the standalone kernel microbench")
     ap.add_argument("--batched-only", action="store_true",
                     help="run only the batched lifted commitment and print its object")
     args = ap.parse_args()
@@ -721,6 +724,14 @@ def main():
                  "ntt_plan": {k: v[:2] for k, v in tuned["ntt"].items()},
                  "leaf_k": {k: v[0] for k, v in tuned["leaf_k"].items()},
                  "fold_leaf_k": {k: v[0] for k, v in tuned["fold_leaf_k"].items()}}
+
+    if args.kernels_only:
+        peak, _ = _peaks()
+        probe = blake2s_probe_rate(torch.cuda.Stream())
+        res = kernel_microbench(peak, probe, log_n=args.kernel_log, cpu=not args.no_cpu_baseline)
+        if rank == 0:
+            print(json.dumps({"kernel_microbench": res}), flush=True)
+        return
 
     if args.batched_only:
         peak, _ = _peaks()
