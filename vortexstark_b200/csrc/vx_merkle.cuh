@@ -42,8 +42,13 @@ struct LeafSoA4 {
 struct LeafCols {
     const uint32_t *const *cols;
     uint32_t n_cols;
-    __device__ __forceinline__ void init() {}
+    const uint32_t *c0;  // the first column pointer, read once by init()
+    __device__ __forceinline__ void init() { c0 = n_cols ? cols[0] : nullptr; }
     __device__ __forceinline__ uint32_t load(uint64_t i, uint32_t m[16]) const {
+        if (n_cols == 1) {  // one column: no pointer reads per leaf
+            m[0] = __ldg(c0 + i);
+            return 4u;
+        }
         uint32_t n = n_cols > 16u ? 16u : n_cols;
 #pragma unroll
         for (uint32_t c = 0; c < 16; c++) if (c < n) m[c] = cols[c][i];
