@@ -194,6 +194,34 @@ void cuda_bit_reverse_qm31(const uint32_t *in, uint32_t *out, uint32_t n, uint32
 /* replaces cuda_accumulate_lift, accumulate_lift.cu:35-44: col[i] +=
  * curr[((i >> (log_ratio + 1)) << 1) | (i & 1)] for i < col_n */
 void cuda_accumulate_lift(uint32_t *col, const uint32_t *curr, uint32_t col_n, uint32_t log_ratio);
+/* replaces cuda_bit_reverse_qm31_forge (ffi.rs:1004-1019): the same as
+ * cuda_bit_reverse_qm31 */
+void cuda_bit_reverse_qm31_forge(const uint32_t *in, uint32_t *out, uint32_t n, uint32_t log_n);
+/* replaces cuda_gather_u32, gather.cu:44-53: dst[i] = src[idx[i]], i < n
+ * (ColumnOps decommitment, column.rs) */
+void cuda_gather_u32(const uint32_t *src, const uint32_t *idx, uint32_t *dst, uint32_t n);
+/* replaces cuda_gather_u256, gather.cu:55-64: dst[8i .. 8i+8) = src[8 idx[i] .. +8) */
+void cuda_gather_u256(const uint32_t *src, const uint32_t *idx, uint32_t *dst, uint32_t n);
+/* replace cuda_gather_u32_forge / cuda_gather_u256_forge (ffi.rs:986-1002,
+ * gather_forge.cu): the same with src_len words of source; an element whose
+ * source lies outside it is not written */
+void cuda_gather_u32_forge(const uint32_t *src, const uint32_t *idx, uint32_t *dst, uint32_t n, uint32_t src_len);
+void cuda_gather_u256_forge(const uint32_t *src, const uint32_t *idx, uint32_t *dst, uint32_t n, uint32_t src_len);
+/* replaces cuda_barycentric_eval, barycentric_eval.cu:44-110: out[4b .. 4b+4)
+ * = sum of evals[i] * weights[i] (M31 times QM31, weights AoS) over the i
+ * of block b of a grid-stride loop of n_blocks x 256 threads (the caller
+ * adds the n_blocks partial sums); synchronises the device. */
+void cuda_barycentric_eval(const uint32_t *evals, const uint32_t *weights, uint32_t n, uint32_t *out,
+                           uint32_t n_blocks);
+/* replaces cuda_eval_at_point, circle_ntt.cu:429-468 (PolyOps::eval_at_point,
+ * poly_ops.rs:382-443): folds n = 2^k M31 coefficients with the k QM31
+ * folding factors (AoS, factor l for level l, level 0 splitting the top
+ * index bit: v[t] + f_l v[t + n/2^(l+1)]) into one QM31, written to the
+ * HOST array h_result[4].  d_scratch1 holds at least 2n words (the
+ * reference's n/2 QM31); d_scratch2 is not used.  Synchronous.  n = 1
+ * gives the coefficient; n not a power of two is rejected. */
+void cuda_eval_at_point(const uint32_t *d_coeffs, const uint32_t *d_folding_factors, uint32_t *h_result, uint32_t n,
+                        uint32_t *d_scratch1, uint32_t *d_scratch2);
 /* replaces cuda_pack_leaves, pack_leaves.cu:44-52: output[c*16 + p][i] =
  * input[c][16 i + p]; both pointer arrays are DEVICE arrays (4 and 64
  * entries), N a multiple of 16 */

@@ -22,7 +22,8 @@ ARCH="-gencode arch=compute_100a,code=sm_100a"
 DEFS="-DFORGE_NTT=1 -DFORGE_NTT_BATCH=1 -DFORGE_FRI=1 -DFORGE_PERMUTE=1"
 SRCS="circle_ntt circle_ntt_layer_forge circle_ntt_batch_forge twiddles batch_inverse constraint blake2s \
 merkle_hash_leaves_forge fri fri_fold_line_forge fri_fold_circle_forge permute permute_forge \
-merkle_leaves_lifted bit_reverse_wide accumulate_lift fields circle_ntt_stwo circle_ntt_stwo_batch pack_leaves grind grind_m31_output"
+merkle_leaves_lifted bit_reverse_wide accumulate_lift fields circle_ntt_stwo circle_ntt_stwo_batch pack_leaves grind grind_m31_output \
+barycentric_eval gather"
 pids=()
 for s in $SRCS; do
   obj="$OUT/obj/$s.o"

@@ -68,6 +68,8 @@ def lib():
         L.vxo_accumulate_lift.argtypes = [U32P, U32P, C.c_uint64, C.c_uint32]
         L.vxo_pack_leaves.argtypes = [C.POINTER(U32P), C.POINTER(U32P), C.c_uint64]
         L.vxo_fri_chain.argtypes = [C.POINTER(U32P), C.c_uint32, U32P, U32P, U32P, U32P]
+        L.vxo_eval_at_point.argtypes = [U32P, U32P, C.c_uint32, U32P]
+        L.vxo_barycentric_partials.argtypes = [U32P, U32P, C.c_uint32, C.c_uint32, U32P]
         L.vxo_stwo_fold_circle_twiddles.argtypes = [C.c_uint32, U32P]
         L.vxo_lifted_size.argtypes = [C.c_uint32, U32P, C.c_uint32, C.c_uint32]
         L.vxo_lifted_size.restype = C.c_size_t
@@ -289,6 +291,24 @@ def fri_chain(src: np.ndarray, state_words):
     last = np.zeros((2, 4), np.uint32)
     lib().vxo_fri_chain(ins, L, _p(st), _p(roots), _p(alphas), _p(last))
     return roots, alphas, last
+
+
+def eval_at_point(coeffs: np.ndarray, factors: np.ndarray) -> np.ndarray:
+    """Fold 2^k M31 coefficients with k QM31 factors (shape [k, 4])."""
+    c = np.ascontiguousarray(coeffs, dtype=np.uint32)
+    f = np.ascontiguousarray(factors, dtype=np.uint32).reshape(-1)
+    k = int(len(c)).bit_length() - 1
+    out = np.zeros(4, np.uint32)
+    lib().vxo_eval_at_point(_p(c), _p(f), k, _p(out))
+    return out
+
+
+def barycentric_partials(evals: np.ndarray, weights: np.ndarray, n_blocks: int) -> np.ndarray:
+    e = np.ascontiguousarray(evals, dtype=np.uint32)
+    w = np.ascontiguousarray(weights, dtype=np.uint32).reshape(-1)
+    out = np.zeros((n_blocks, 4), np.uint32)
+    lib().vxo_barycentric_partials(_p(e), _p(w), len(e), n_blocks, _p(out))
+    return out
 
 
 def batch_inverse(x: np.ndarray) -> np.ndarray:

@@ -1193,3 +1193,38 @@ void vxo_fri_chain(const uint32_t *const src[4], uint32_t log_size, const uint32
     for (int c = 0; c < 4; c++) { free(cur[c]); free(nxt[c]); }
     free(tw);
 }
+
+/* ------------------------------------------------------------------ */
+/* PolyOps on the device path of the stwo backend                      */
+/* ------------------------------------------------------------------ */
+/* eval_at_point by folding, level by level (circle_ntt.cu:186-231,
+ * 429-468): level 0 combines v[t] + f_0 v[t + n/2] with the coefficients as
+ * QM31 of one M31 word; level l uses factor l on the half-length result. */
+void vxo_eval_at_point(const uint32_t *coeffs, const uint32_t *factors, uint32_t log_n, uint32_t out[4]) {
+    const uint64_t n = 1ull << log_n;
+    qm *v = (qm *)malloc(sizeof(qm) * (n ? n : 1));
+    for (uint64_t i = 0; i < n; i++) { v[i].v[0] = coeffs[i]; v[i].v[1] = v[i].v[2] = v[i].v[3] = 0; }
+    uint64_t cur = n;
+    for (uint32_t l = 0; l < log_n; l++) {
+        qm f; memcpy(f.v, factors + 4 * l, 16);
+        const uint64_t half = cur / 2;
+        for (uint64_t t = 0; t < half; t++) v[t] = q_add(v[t], q_mul(v[t + half], f));
+        cur = half;
+    }
+    memcpy(out, v[0].v, 16);
+    free(v);
+}
+/* barycentric_eval_kernel partial sums (barycentric_eval.cu:44-94): block b of
+ * a grid-stride loop over n_blocks x 256 threads. */
+void vxo_barycentric_partials(const uint32_t *evals, const uint32_t *weights, uint32_t n, uint32_t n_blocks,
+                              uint32_t *out) {
+    memset(out, 0, 16ull * n_blocks);
+    const uint64_t stride = 256ull * n_blocks;
+    for (uint64_t i = 0; i < n; i++) {
+        const uint64_t b = (i % stride) / 256;
+        qm w; memcpy(w.v, weights + 4 * i, 16);
+        qm acc; memcpy(acc.v, out + 4 * b, 16);
+        acc = q_add(acc, q_mulm(w, evals[i]));
+        memcpy(out + 4 * b, acc.v, 16);
+    }
+}

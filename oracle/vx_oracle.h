@@ -104,6 +104,12 @@ void vxo_fold_circle_into_line(uint32_t *const dst[4], const uint32_t *const src
 void vxo_fri_chain(const uint32_t *const src[4], uint32_t log_size, const uint32_t state[8], uint32_t *roots,
                    uint32_t *alphas, uint32_t last[8]);
 
+/* PolyOps::eval_at_point by folding (circle_ntt.cu:429-468) and the
+ * barycentric evaluation's per-block partial sums (barycentric_eval.cu). */
+void vxo_eval_at_point(const uint32_t *coeffs, const uint32_t *factors, uint32_t log_n, uint32_t out[4]);
+void vxo_barycentric_partials(const uint32_t *evals, const uint32_t *weights, uint32_t n, uint32_t n_blocks,
+                              uint32_t *out);
+
 /* ---- channel (channel.rs:15-185) ---- */
 typedef struct { uint8_t state[32]; uint32_t n_draws; } vxo_channel;
 void vxo_channel_init(vxo_channel *ch);

@@ -217,3 +217,106 @@ def test_commit_lifted_graph_and_uploads(oracle):
         assert com.column_ptr(0) != 0 and probe.numel() == len(cols[0])
     assert com.launches() > 0 and com.device_bytes() > 0
     com.close()
+
+
+def _qm(rng, n):
+    return rng.integers(0, P, (n, 4), dtype=np.uint32)
+
+
+@pytest.mark.parametrize("log_n", [0, 1, 3, 10, 11, 12, 16, 20])
+def test_eval_at_point_matches_oracle_and_reference(oracle, log_n):
+    """cuda_eval_at_point (PolyOps::eval_at_point, poly_ops.rs:382-443)."""
+    import ctypes as C
+    rng = np.random.default_rng(40 + log_n)
+    n = 1 << log_n
+    coeffs = rng.integers(0, P, n, dtype=np.uint32)
+    factors = _qm(rng, max(log_n, 1))
+    want = oracle.eval_at_point(coeffs, factors[:log_n])
+    d_c, d_f = to_dev(coeffs), to_dev(factors.reshape(-1))
+    s1, s2 = empty(2 * n + 8), empty(2 * n + 8)
+    res = (C.c_uint32 * 4)()
+    _lib.clear_error()
+    _lib.lib().cuda_eval_at_point(d_c.data_ptr(), d_f.data_ptr(), res, n, s1.data_ptr(), s2.data_ptr())
+    _lib.raise_if_error()
+    assert list(res) == want.tolist()
+    if oracle.ref_available() and log_n >= 1:  # the reference's launcher needs n >= 2
+        R = oracle.ref_lib()
+        R.cuda_eval_at_point.argtypes = [C.c_void_p] * 3 + [C.c_uint32, C.c_void_p, C.c_void_p]
+        ref = (C.c_uint32 * 4)()
+        R.cuda_eval_at_point(d_c.data_ptr(), d_f.data_ptr(), ref, n, s1.data_ptr(), s2.data_ptr())
+        assert list(ref) == want.tolist()
+
+
+def test_eval_at_point_rejects_non_power_of_two():
+    import ctypes as C
+    d = empty(8)
+    res = (C.c_uint32 * 4)()
+    _lib.clear_error()
+    _lib.lib().cuda_eval_at_point(d.data_ptr(), d.data_ptr(), res, 6, d.data_ptr(), d.data_ptr())
+    with pytest.raises(_lib.VortexError):
+        _lib.raise_if_error()
+
+
+@pytest.mark.parametrize("n,n_blocks", [(1, 1), (255, 1), (1000, 3), (1 << 16, 64), (1 << 20, 256), (12345, 256)])
+def test_barycentric_partials_match_oracle_and_reference(oracle, n, n_blocks):
+    """cuda_barycentric_eval (poly_ops.rs:449-497): the per-block partial sums."""
+    import ctypes as C
+    rng = np.random.default_rng(n + n_blocks)
+    evals = rng.integers(0, P, n, dtype=np.uint32)
+    weights = _qm(rng, n)
+    want = oracle.barycentric_partials(evals, weights, n_blocks)
+    d_e, d_w, out = to_dev(evals), to_dev(weights.reshape(-1)), empty(4 * n_blocks)
+    _lib.clear_error()
+    _lib.lib().cuda_barycentric_eval(d_e.data_ptr(), d_w.data_ptr(), n, out.data_ptr(), n_blocks)
+    _lib.raise_if_error()
+    assert np.array_equal(to_host(out, 4 * n_blocks).reshape(-1, 4), want)
+    if oracle.ref_available():
+        R = oracle.ref_lib()
+        R.cuda_barycentric_eval.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32]
+        out2 = empty(4 * n_blocks)
+        R.cuda_barycentric_eval(d_e.data_ptr(), d_w.data_ptr(), n, out2.data_ptr(), n_blocks)
+        assert np.array_equal(to_host(out2, 4 * n_blocks).reshape(-1, 4), want)
+
+
+def test_gathers_and_forge_aliases(oracle):
+    """cuda_gather_u32 / _u256 (gather.cu) and their bounded _forge forms;
+    cuda_bit_reverse_qm31_forge == cuda_bit_reverse_qm31."""
+    import ctypes as C
+    L = _lib.lib()
+    rng = np.random.default_rng(9)
+    src = rng.integers(0, 1 << 32, 5000, dtype=np.uint64).astype(np.uint32)
+    idx = rng.integers(0, 5000, 777, dtype=np.uint32)
+    d_src, d_idx = to_dev(src), to_dev(idx)
+    out = empty(777)
+    L.cuda_gather_u32(d_src.data_ptr(), d_idx.data_ptr(), out.data_ptr(), 777)
+    assert np.array_equal(to_host(out, 777), src[idx])
+    idx8 = rng.integers(0, 5000 // 8, 300, dtype=np.uint32)
+    d_idx8 = to_dev(idx8)
+    out8 = empty(8 * 300)
+    L.cuda_gather_u256(d_src.data_ptr(), d_idx8.data_ptr(), out8.data_ptr(), 300)
+    want8 = src[: (5000 // 8) * 8].reshape(-1, 8)[idx8].reshape(-1)
+    assert np.array_equal(to_host(out8, 8 * 300), want8)
+    # bounded forms: in-range the same, out-of-range elements left as they were
+    bad = idx.copy()
+    bad[::5] = 6000
+    d_bad = to_dev(bad)
+    outf = to_dev(np.full(777, 0xABCD, np.uint32))
+    L.cuda_gather_u32_forge(d_src.data_ptr(), d_bad.data_ptr(), outf.data_ptr(), 777, 5000)
+    got = to_host(outf, 777)
+    ok = bad < 5000
+    assert np.array_equal(got[ok], src[bad[ok]]) and (got[~ok] == 0xABCD).all()
+    outf8 = empty(8 * 300)
+    L.cuda_gather_u256_forge(d_src.data_ptr(), d_idx8.data_ptr(), outf8.data_ptr(), 300, 5000)
+    assert np.array_equal(to_host(outf8, 8 * 300), want8)
+    if oracle.ref_available():
+        R = oracle.ref_lib()
+        R.cuda_gather_u32.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]
+        out_r = empty(777)
+        R.cuda_gather_u32(d_src.data_ptr(), d_idx.data_ptr(), out_r.data_ptr(), 777)
+        assert np.array_equal(to_host(out_r, 777), src[idx])
+    q = rng.integers(0, P, 4 * 1024, dtype=np.uint32)
+    a, b = empty(4 * 1024), empty(4 * 1024)
+    dq = to_dev(q)
+    L.cuda_bit_reverse_qm31(dq.data_ptr(), a.data_ptr(), 1024, 10)
+    L.cuda_bit_reverse_qm31_forge(dq.data_ptr(), b.data_ptr(), 1024, 10)
+    assert np.array_equal(to_host(a), to_host(b))

@@ -214,3 +214,24 @@ def test_lifted_shapes_rejected(oracle):
     with pytest.raises(ValueError):
         oracle.commit_lifted(_cols(4, [5, 4]), 2, 8)
     assert parse_lifted(oracle.commit_lifted(_cols(4, [4, 5]), 1, 8)).lifting_log == 6
+
+
+def test_eval_at_point_fold_is_the_weighted_sum():
+    """The level-by-level fold equals sum_i c[i] prod(f_(k-1-b) for the set bits b of i)."""
+    import numpy as np
+
+    from oracle import oracle as O
+    P = (1 << 31) - 1
+    rng = np.random.default_rng(3)
+    k = 5
+    c = rng.integers(0, P, 1 << k, dtype=np.uint32)
+    f = rng.integers(0, P, (k, 4), dtype=np.uint32)
+    acc = np.zeros(4, np.uint32)
+    for i in range(1 << k):
+        w = np.array([1, 0, 0, 0], np.uint32)
+        for b in range(k):
+            if (i >> b) & 1:
+                w = O.qm31_mul(w, f[k - 1 - b])
+        term = np.array([(int(x) * int(c[i])) % P for x in w], np.uint32)
+        acc = np.array([(int(x) + int(y)) % P for x, y in zip(acc, term)], np.uint32)
+    assert np.array_equal(O.eval_at_point(c, f), acc)

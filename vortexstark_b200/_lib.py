@@ -74,6 +74,13 @@ _SIGS = {
     "cuda_bit_reverse_qm31": [vp, vp, u32, u32],
     "cuda_accumulate_lift": [vp, vp, u32, u32],
     "cuda_pack_leaves": [vp, vp, u32],
+    "cuda_bit_reverse_qm31_forge": [vp, vp, u32, u32],
+    "cuda_gather_u32": [vp, vp, vp, u32],
+    "cuda_gather_u256": [vp, vp, vp, u32],
+    "cuda_gather_u32_forge": [vp, vp, vp, u32, u32],
+    "cuda_gather_u256_forge": [vp, vp, vp, u32, u32],
+    "cuda_barycentric_eval": [vp, vp, u32, vp, u32],
+    "cuda_eval_at_point": [vp, vp, vp, u32, vp, vp],
     # vx_ API
     "vx_last_error": ([], C.c_char_p),
     "vx_version": ([], C.c_int),

@@ -142,6 +142,147 @@ __global__ void __launch_bounds__(256) pack_leaves_kernel(const uint32_t *const 
     }
 }
 
+// ---- evaluation of a circle polynomial at a QM31 point by folding ----
+// The reference folds level by level (circle_ntt.cu:186-231, 429-468):
+// level l combines v[t] + f_l v[t + half], l = 0 at the top index bit.  The
+// result is linear in the coefficients: sum_i c[i] w(i), w(i) the product of
+// f_(log_n - 1 - b) over the set bits b of i, so any grouping gives the same
+// field value.  Here a block folds a contiguous chunk of 2^11 coefficients
+// (8 per thread in registers, then 8 levels in shared memory), scales the
+// chunk's value by the factors of its high index bits, and a second kernel
+// adds the chunk values.
+constexpr uint32_t kEvalChunkLog = 11, kEvalThreads = 256;
+__device__ __forceinline__ qm31 qscale(qm31 f, uint32_t m) { return qmulm(f, m); }
+
+__global__ void __launch_bounds__(kEvalThreads) eval_chunk_kernel(const uint32_t *__restrict__ coeffs,
+                                                                  const uint32_t *__restrict__ factors,
+                                                                  uint32_t log_n, uint32_t *__restrict__ partial) {
+    __shared__ uint32_t fs[4 * 32];
+    __shared__ qm31 s[kEvalThreads];
+    const uint32_t t = threadIdx.x;
+    if (t < 4 * log_n) fs[t] = factors[t];
+    __syncthreads();
+    auto fac = [&](uint32_t bit) {  // factor of index bit `bit`
+        const uint32_t l = log_n - 1 - bit;
+        return qm31{{fs[4 * l], fs[4 * l + 1], fs[4 * l + 2], fs[4 * l + 3]}};
+    };
+    const uint64_t base = ((uint64_t)blockIdx.x << kEvalChunkLog) + 8ull * t;
+    uint32_t c[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) c[j] = coeffs[base + j];
+    // index bits 2, 1, 0 of the thread's 8 coefficients
+    const qm31 f2 = fac(2), f1 = fac(1), f0 = fac(0);
+    qm31 u[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const qm31 b = qscale(f2, c[j + 4]);
+        u[j] = {{madd(c[j], b.v[0]), b.v[1], b.v[2], b.v[3]}};
+    }
+    const qmat m1 = qmat_of(f1), m0 = qmat_of(f0);
+    const qm31 w0 = qadd(u[0], qmul_mat(m1, u[2])), w1 = qadd(u[1], qmul_mat(m1, u[3]));
+    s[t] = qadd(w0, qmul_mat(m0, w1));
+    __syncthreads();
+    // index bits 3 .. 10: thread bits 0 .. 7, highest first
+    for (uint32_t k = 8; k-- > 0;) {
+        const uint32_t half = 1u << k;
+        if (t < half) s[t] = qadd(s[t], qmul_mat(qmat_of(fac(k + 3)), s[t + half]));
+        __syncthreads();
+    }
+    if (t == 0) {
+        qm31 r = s[0];
+        const uint64_t chunk = blockIdx.x;
+        for (uint32_t b = kEvalChunkLog; b < log_n; b++)
+            if ((chunk >> (b - kEvalChunkLog)) & 1ull) r = qmul(r, fac(b));
+#pragma unroll
+        for (int w = 0; w < 4; w++) partial[4ull * blockIdx.x + w] = r.v[w];
+    }
+}
+
+// Sum of `count` QM31 values (chunk values), or for n < 2^11 the direct sum
+// of c[i] w(i); one block, the total to out[0..4).
+__global__ void __launch_bounds__(kEvalThreads) eval_sum_kernel(const uint32_t *__restrict__ vals, uint64_t count,
+                                                                const uint32_t *__restrict__ coeffs,
+                                                                const uint32_t *__restrict__ factors, uint32_t log_n,
+                                                                uint32_t *__restrict__ out) {
+    __shared__ qm31 s[kEvalThreads];
+    const uint32_t t = threadIdx.x;
+    qm31 acc{{0u, 0u, 0u, 0u}};
+    if (coeffs) {  // small polynomial: weight each coefficient directly
+        for (uint64_t i = t; i < (1ull << log_n); i += kEvalThreads) {
+            qm31 w{{1u, 0u, 0u, 0u}};
+            for (uint32_t b = 0; b < log_n; b++)
+                if ((i >> b) & 1ull) {
+                    const uint32_t l = log_n - 1 - b;
+                    w = qmul(w, qm31{{factors[4 * l], factors[4 * l + 1], factors[4 * l + 2], factors[4 * l + 3]}});
+                }
+            acc = qadd(acc, qmulm(w, coeffs[i]));
+        }
+    } else {
+        for (uint64_t i = t; i < count; i += kEvalThreads)
+            acc = qadd(acc, qm31{{vals[4 * i], vals[4 * i + 1], vals[4 * i + 2], vals[4 * i + 3]}});
+    }
+    s[t] = acc;
+    __syncthreads();
+    for (uint32_t half = kEvalThreads / 2; half > 0; half >>= 1) {
+        if (t < half) s[t] = qadd(s[t], s[t + half]);
+        __syncthreads();
+    }
+    if (t < 4) out[t] = s[0].v[t];
+}
+
+// ---- barycentric evaluation partial sums (barycentric_eval.cu:52-94) ----
+// Block b accumulates evals[i] * weights[i] (M31 times QM31, weights AoS)
+// over the i that a grid-stride loop of n_blocks x 256 threads gives it, so
+// the partial sums are the reference's.
+__global__ void __launch_bounds__(256) barycentric_kernel(const uint32_t *__restrict__ evals,
+                                                          const uint32_t *__restrict__ weights, uint32_t n,
+                                                          uint32_t *__restrict__ out) {
+    __shared__ qm31 s[8];
+    const uint32_t stride = gridDim.x * blockDim.x;
+    qm31 acc{{0u, 0u, 0u, 0u}};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint32_t e = __ldg(evals + i);
+        const uint64_t b = 4ull * i;
+        const qm31 w{{__ldg(weights + b), __ldg(weights + b + 1), __ldg(weights + b + 2), __ldg(weights + b + 3)}};
+        acc = qadd(acc, qmulm(w, e));
+    }
+#pragma unroll
+    for (int m = 16; m > 0; m >>= 1) {
+        qm31 o;
+#pragma unroll
+        for (int c = 0; c < 4; c++) o.v[c] = __shfl_xor_sync(0xffffffffu, acc.v[c], m);
+        acc = qadd(acc, o);
+    }
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    if (lane == 0) s[warp] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        qm31 r = s[0];
+        for (uint32_t w = 1; w < (blockDim.x + 31) / 32; w++) r = qadd(r, s[w]);
+#pragma unroll
+        for (int c = 0; c < 4; c++) out[4 * blockIdx.x + c] = r.v[c];
+    }
+}
+
+// ---- gathers (gather.cu): dst[i] = src[idx[i]], or 8-word elements ----
+// The bounded forms skip an element whose source lies outside src_len words.
+__global__ void gather_u32_kernel(const uint32_t *__restrict__ src, const uint32_t *__restrict__ idx,
+                                  uint32_t *__restrict__ dst, uint32_t n, uint64_t src_len) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t j = idx[i];
+    if (j < src_len) dst[i] = src[j];
+}
+__global__ void gather_u256_kernel(const uint32_t *__restrict__ src, const uint32_t *__restrict__ idx,
+                                   uint32_t *__restrict__ dst, uint32_t n, uint64_t src_len) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t j = 8ull * idx[i];
+    if (j + 8 > src_len) return;
+#pragma unroll
+    for (int w = 0; w < 8; w++) dst[8ull * i + w] = src[j + w];
+}
+
 }  // namespace
 }  // namespace vx
 
@@ -221,6 +362,65 @@ void cuda_pack_leaves(const uint32_t *const *input_col_ptrs, uint32_t *const *ou
     const uint64_t n_out = n / 16u;
     pack_leaves_kernel<<<dim3(blocks_for(n_out, 32), 4), 256>>>(input_col_ptrs, output_col_ptrs, n_out);
     VX_LAUNCH_CHECK();
+}
+
+void cuda_bit_reverse_qm31_forge(const uint32_t *in, uint32_t *out, uint32_t n, uint32_t log_n) {
+    cuda_bit_reverse_qm31(in, out, n, log_n);
+}
+
+void cuda_gather_u32(const uint32_t *src, const uint32_t *idx, uint32_t *dst, uint32_t n) {
+    if (n == 0) return;
+    gather_u32_kernel<<<blocks_for(n, 256), 256>>>(src, idx, dst, n, ~0ull);
+    VX_LAUNCH_CHECK();
+}
+void cuda_gather_u32_forge(const uint32_t *src, const uint32_t *idx, uint32_t *dst, uint32_t n, uint32_t src_len) {
+    if (n == 0) return;
+    gather_u32_kernel<<<blocks_for(n, 256), 256>>>(src, idx, dst, n, src_len);
+    VX_LAUNCH_CHECK();
+}
+void cuda_gather_u256(const uint32_t *src, const uint32_t *idx, uint32_t *dst, uint32_t n) {
+    if (n == 0) return;
+    gather_u256_kernel<<<blocks_for(n, 256), 256>>>(src, idx, dst, n, ~0ull);
+    VX_LAUNCH_CHECK();
+}
+void cuda_gather_u256_forge(const uint32_t *src, const uint32_t *idx, uint32_t *dst, uint32_t n, uint32_t src_len) {
+    if (n == 0) return;
+    gather_u256_kernel<<<blocks_for(n, 256), 256>>>(src, idx, dst, n, src_len);
+    VX_LAUNCH_CHECK();
+}
+
+void cuda_barycentric_eval(const uint32_t *evals, const uint32_t *weights, uint32_t n, uint32_t *out,
+                           uint32_t n_blocks) {
+    if (n_blocks == 0) return;
+    barycentric_kernel<<<n_blocks, 256>>>(evals, weights, n, out);
+    VX_LAUNCH_CHECK();
+    cudaDeviceSynchronize();  // the reference's launcher returns with the sums in place
+}
+
+void cuda_eval_at_point(const uint32_t *d_coeffs, const uint32_t *d_folding_factors, uint32_t *h_result, uint32_t n,
+                        uint32_t *d_scratch1, uint32_t *d_scratch2) {
+    (void)d_scratch2;
+    if (n == 0 || (n & (n - 1u))) {
+        set_last_error(VX_ERR_ARG, "cuda_eval_at_point: n = %u is not a power of two", n);
+        return;
+    }
+    const uint32_t log_n = 31u - __builtin_clz(n);
+    if (log_n == 0) {  // a constant: the coefficient itself
+        uint32_t c = 0;
+        if (cudaMemcpy(&c, d_coeffs, 4, cudaMemcpyDeviceToHost) != cudaSuccess) { VX_LAUNCH_CHECK(); return; }
+        h_result[0] = c; h_result[1] = h_result[2] = h_result[3] = 0u;
+        return;
+    }
+    if (log_n < kEvalChunkLog) {
+        eval_sum_kernel<<<1, kEvalThreads>>>(nullptr, 0, d_coeffs, d_folding_factors, log_n, d_scratch1);
+    } else {
+        const uint64_t chunks = 1ull << (log_n - kEvalChunkLog);
+        eval_chunk_kernel<<<(unsigned)chunks, kEvalThreads>>>(d_coeffs, d_folding_factors, log_n, d_scratch1);
+        eval_sum_kernel<<<1, kEvalThreads>>>(d_scratch1, chunks, nullptr, nullptr, 0, d_scratch1 + 4 * chunks);
+        d_scratch1 += 4 * chunks;
+    }
+    VX_LAUNCH_CHECK();
+    if (cudaMemcpy(h_result, d_scratch1, 16, cudaMemcpyDeviceToHost) != cudaSuccess) VX_LAUNCH_CHECK();
 }
 
 }  // extern "C"
