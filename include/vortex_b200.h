@@ -503,9 +503,11 @@ int vx_prove_fib_noalloc(uint32_t a, uint32_t b, uint32_t log_n, uint32_t blowup
  * (prover.rs:2278-2311), which proves its inputs one after another with a
  * shared cache.  Proves (a[i], b[i]) for i < count into out + i *
  * *proof_size (cap >= count * vx_proof_size bytes), each proof
- * byte-identical to vx_prove_fib's.  Two cached slots on two streams keep
- * two proofs in flight, so one proof's latency-bound FRI tail overlaps the
- * next one's hashing.  Returns when all proofs are in `out`. */
+ * byte-identical to vx_prove_fib's.  Up to four cached slots on their own
+ * streams keep that many proofs in flight, so one proof's latency-bound FRI
+ * tail overlaps the next ones' hashing; a slot after the first is added only
+ * while it fits in half of the free device memory.  Returns when all proofs
+ * are in `out`. */
 int vx_prove_fib_batch(const uint32_t *a, const uint32_t *b, uint32_t count, uint32_t log_n, uint32_t blowup_bits,
                        uint32_t n_queries, uint8_t *out, size_t cap, size_t *proof_size);
 

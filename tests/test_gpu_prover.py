@@ -89,7 +89,7 @@ def test_concurrent_slots_on_streams(oracle):
         assert c.result_bytes() == oracle.prove(a, b, s)
 
 
-@pytest.mark.parametrize("log_n,count", [(8, 1), (8, 2), (10, 5), (14, 4), (18, 3)])
+@pytest.mark.parametrize("log_n,count", [(8, 1), (8, 2), (10, 5), (12, 11), (14, 4), (18, 3)])
 def test_prove_batch_matches_single_proofs(oracle, log_n, count):
     """vx_prove_fib_batch (ProverPipeline::prove_batch, prover.rs:2305) gives the
     proofs that vx_prove_fib and the oracle give, in input order."""
@@ -100,6 +100,15 @@ def test_prove_batch_matches_single_proofs(oracle, log_n, count):
         assert blob == prover.prove_bytes(a, b, log_n)
     for (a, b), blob in list(zip(inputs, got))[:2]:
         assert blob == oracle.prove(a, b, log_n)
+
+
+def test_prove_batch_slots_grow_between_calls():
+    """A size first batched with one proof, then with more: the cached context
+    grows to more slots in flight and every proof stays byte-identical."""
+    for count in (1, 3, 9):
+        inputs = fib_inputs(1700 + count, count)
+        got = prover.prove_batch_bytes(inputs, 9)
+        assert [blob == prover.prove_bytes(a, b, 9) for (a, b), blob in zip(inputs, got)] == [True] * count
 
 
 def test_prove_batch_arguments():
