@@ -10,11 +10,14 @@
 //
 // The full search visits nonces (hi << 32) | low, low < 2^20, hi = 0, 1, ...
 // and returns the smallest accepted one, the order stwo's SimdBackend and the
-// reference's loop use.  Every thread walks its share of a range in
-// increasing order and stops once its next candidate exceeds the best nonce
-// found so far, so the result is exactly the minimum of the range whatever
-// the scheduling.  Launches are bounded (a fixed range each); the host checks
-// the result between launches.
+// reference's loop use.  Warps take chunks of candidates in increasing order
+// from a counter and stop at a chunk that starts beyond the best nonce found
+// so far; no chunk is left half done, so the result is exactly the minimum
+// of the range whatever the scheduling.  (A fixed grid-stride split wastes
+// work here: the warp scheduler lets some warps run far ahead of the one
+// that holds the answer.)  Launches are bounded (a fixed range each); the
+// host checks the result between launches.  The reference-ABI launchers,
+// which have no counter word, keep a stateless grid-stride loop.
 #include <mutex>
 
 #include "vx_blake2s.cuh"
@@ -41,61 +44,109 @@ __device__ __forceinline__ uint32_t mod_p(uint32_t h) {
 }
 
 // Candidate w of a launch is nonce base + ((w >> lowbits) << 32) + (w & lowmask)
-// (lowbits >= 63: base + w).  count candidates, visited in increasing order.
-// The digest comes by value, or from device memory when dptr is not null.
+// (lowbits >= 63: base + w).  count candidates.  With `next` (a zeroed
+// counter) warps take kWarpChunk consecutive candidates at a time; without
+// it each thread walks w = its index + j * (grid threads), j = 0, 1, ...
+// Both visit a thread's candidates in increasing order.  The digest comes by
+// value, or from device memory when dptr is not null.
+constexpr uint32_t kPerLane = 4, kWarpChunk = 32 * kPerLane;
+
+template <bool M31OUT>
+__device__ __forceinline__ void grind_one(const Digest8 &d, unsigned long long *result, uint32_t pow_bits,
+                                          uint64_t nonce, uint32_t one) {
+    uint32_t m[16];
+#pragma unroll
+    for (int i = 0; i < 8; i++) m[i] = d.w[i];
+    m[8] = (uint32_t)nonce;
+    m[9] = (uint32_t)(nonce >> 32);
+#pragma unroll
+    for (int i = 10; i < 16; i++) m[i] = 0u;
+    uint32_t h[8];
+    blake2s_block(h, m, 40u, one);  // one == 1: Blake2s pipe balance
+    uint32_t h0 = h[0], h1 = h[1], h2 = h[2], h3 = h[3];
+    if (M31OUT) { h0 = mod_p(h0); h1 = mod_p(h1); h2 = mod_p(h2); h3 = mod_p(h3); }
+    if (tz128(h0, h1, h2, h3) >= pow_bits) atomicMin(result, (unsigned long long)nonce);
+}
+
 template <bool M31OUT>
 __global__ void __launch_bounds__(256) grind_kernel(Digest8 d, const uint32_t *dptr, unsigned long long *result,
-                                                    uint32_t pow_bits, uint64_t base, uint64_t count,
-                                                    uint32_t lowbits, uint32_t one) {
+                                                    unsigned long long *next, uint32_t pow_bits, uint64_t base,
+                                                    uint64_t count, uint32_t lowbits, uint32_t one) {
     if (dptr) {
 #pragma unroll
         for (int i = 0; i < 8; i++) d.w[i] = __ldg(dptr + i);
     }
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     const uint64_t lowmask = lowbits >= 63 ? ~0ull : ((1ull << lowbits) - 1ull);
+    auto nonce_of = [&](uint64_t w) { return lowbits >= 63 ? base + w : base + ((w >> lowbits) << 32) + (w & lowmask); };
+    if (next) {
+        const uint32_t lane = threadIdx.x & 31u;
+        while (true) {
+            // lane 0 takes the chunk and reads the best nonce; both are
+            // broadcast, so the whole warp leaves the loop together
+            unsigned long long c0 = 0, best = 0;
+            if (lane == 0) {
+                c0 = atomicAdd(next, (unsigned long long)kWarpChunk);
+                best = __ldcv(result);
+            }
+            c0 = __shfl_sync(0xFFFFFFFFu, c0, 0);
+            best = __shfl_sync(0xFFFFFFFFu, best, 0);
+            if (c0 >= count || nonce_of(c0) > best) return;
+#pragma unroll 1
+            for (uint32_t r = 0; r < kPerLane; r++) {
+                const uint64_t w = c0 + 32u * r + lane;
+                if (w < count) grind_one<M31OUT>(d, result, pow_bits, nonce_of(w), one);
+            }
+        }
+    }
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < count; w += stride) {
-        const uint64_t nonce =
-            lowbits >= 63 ? base + w : base + ((w >> lowbits) << 32) + (w & lowmask);
+        const uint64_t nonce = nonce_of(w);
         if (nonce > __ldcv(result)) return;  // a smaller nonce is already accepted
-        uint32_t m[16];
-#pragma unroll
-        for (int i = 0; i < 8; i++) m[i] = d.w[i];
-        m[8] = (uint32_t)nonce;
-        m[9] = (uint32_t)(nonce >> 32);
-#pragma unroll
-        for (int i = 10; i < 16; i++) m[i] = 0u;
-        uint32_t h[8];
-        blake2s_block(h, m, 40u, one);  // one == 1: Blake2s pipe balance
-        uint32_t h0 = h[0], h1 = h[1], h2 = h[2], h3 = h[3];
-        if (M31OUT) { h0 = mod_p(h0); h1 = mod_p(h1); h2 = mod_p(h2); h3 = mod_p(h3); }
-        if (tz128(h0, h1, h2, h3) >= pow_bits) atomicMin(result, (unsigned long long)nonce);
+        grind_one<M31OUT>(d, result, pow_bits, nonce, one);
     }
 }
 
-unsigned grind_blocks() {
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 148;
+// Blocks of 256 threads: every resident block with the chunk counter; two
+// per SM for the grid-stride loop, which measured fastest there when the
+// answer comes early (the fewer warps per SM, the less they drift apart).
+unsigned grind_blocks(bool m31, bool dynamic) {
+    static int cached[64][2];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) {
+        cudaGetLastError();
+        sms = 148;
     }
-    return (unsigned)sms * 8u;  // 8 blocks of 256 threads per SM
+    if (!dynamic) return (unsigned)sms * 2u;
+    int *c = (dev >= 0 && dev < 64) ? &cached[dev][m31 ? 1 : 0] : nullptr;
+    if (c && *c) return (unsigned)*c;
+    int per_sm = 0;
+    cudaError_t e = m31 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grind_kernel<true>, 256, 0)
+                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grind_kernel<false>, 256, 0);
+    if (e != cudaSuccess || per_sm <= 0) {
+        cudaGetLastError();
+        per_sm = 4;
+    }
+    if (c) *c = sms * per_sm;
+    return (unsigned)(sms * per_sm);
 }
 
 // digest_words: 8 host words, or nullptr with dptr the device digest.
+// next: a zeroed chunk counter (dynamic chunks), or null (grid-stride loop).
 cudaError_t grind_launch(bool m31, const uint32_t *digest_words, const uint32_t *dptr, unsigned long long *result,
-                         uint32_t pow_bits, uint64_t base, uint64_t count, uint32_t lowbits, cudaStream_t st) {
+                         unsigned long long *next, uint32_t pow_bits, uint64_t base, uint64_t count, uint32_t lowbits,
+                         cudaStream_t st) {
     Digest8 d{};
     if (digest_words)
         for (int i = 0; i < 8; i++) d.w[i] = digest_words[i];
     uint64_t need = (count + 255) / 256;
-    unsigned blocks = grind_blocks();
+    unsigned blocks = grind_blocks(m31, next != nullptr);
     if (need < blocks) blocks = (unsigned)(need ? need : 1);
     if (m31)
-        grind_kernel<true><<<blocks, 256, 0, st>>>(d, dptr, result, pow_bits, base, count, lowbits, 1u);
+        grind_kernel<true><<<blocks, 256, 0, st>>>(d, dptr, result, next, pow_bits, base, count, lowbits, 1u);
     else
-        grind_kernel<false><<<blocks, 256, 0, st>>>(d, dptr, result, pow_bits, base, count, lowbits, 1u);
+        grind_kernel<false><<<blocks, 256, 0, st>>>(d, dptr, result, next, pow_bits, base, count, lowbits, 1u);
     return cudaGetLastError();
 }
 
@@ -115,8 +166,8 @@ extern "C" {
 static void grind_abi(bool m31, const uint32_t *prefixed_digest, uint64_t *result, uint32_t pow_bits,
                       uint64_t batch_offset, uint32_t n_threads, const char *who) {
     if (n_threads == 0) return;
-    cudaError_t e = grind_launch(m31, nullptr, prefixed_digest, (unsigned long long *)result, pow_bits, batch_offset,
-                                 n_threads, 63u, 0);
+    cudaError_t e = grind_launch(m31, nullptr, prefixed_digest, (unsigned long long *)result, nullptr, pow_bits,
+                                 batch_offset, n_threads, 63u, 0);
     if (e != cudaSuccess) set_last_error(VX_ERR_CUDA, "%s: %s", who, cudaGetErrorString(e));
 }
 
@@ -148,15 +199,16 @@ extern "C" int vx_grind_pow(const uint32_t prefixed_digest[8], uint32_t pow_bits
     VX_CUDA_TRY(cudaGetDevice(&dev));
     VX_CHECK_ARG(dev >= 0 && dev < 64, "vx_grind_pow: device %d out of range", dev);
     std::lock_guard<std::mutex> lk(g_grind_mu);
-    if (!g_grind_res[dev]) VX_CUDA_TRY(cudaMalloc(&g_grind_res[dev], sizeof(unsigned long long)));
-    unsigned long long *res = g_grind_res[dev];
+    if (!g_grind_res[dev]) VX_CUDA_TRY(cudaMalloc(&g_grind_res[dev], 2 * sizeof(unsigned long long)));
+    unsigned long long *res = g_grind_res[dev];  // [0] best nonce, [1] chunk counter
     cudaStream_t st = (cudaStream_t)stream;
     constexpr uint32_t kLowBits = 20, kHiPerLaunch = 64;
     for (uint32_t hi = 0; hi < max_batches; hi += kHiPerLaunch) {
         const uint32_t nh = max_batches - hi < kHiPerLaunch ? max_batches - hi : kHiPerLaunch;
         VX_CUDA_TRY(cudaMemsetAsync(res, 0xFF, sizeof(unsigned long long), st));
-        VX_CUDA_TRY(grind_launch(m31_output != 0, prefixed_digest, nullptr, res, pow_bits, (uint64_t)hi << 32,
-                                 (uint64_t)nh << kLowBits, kLowBits, st));
+        VX_CUDA_TRY(cudaMemsetAsync(res + 1, 0, sizeof(unsigned long long), st));
+        VX_CUDA_TRY(grind_launch(m31_output != 0, prefixed_digest, nullptr, res, res + 1, pow_bits,
+                                 (uint64_t)hi << 32, (uint64_t)nh << kLowBits, kLowBits, st));
         unsigned long long found = ~0ull;
         VX_CUDA_TRY(cudaMemcpyAsync(&found, res, sizeof(found), cudaMemcpyDeviceToHost, st));
         VX_CUDA_TRY(cudaStreamSynchronize(st));
