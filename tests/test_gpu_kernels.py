@@ -353,10 +353,5 @@ def test_fri_chain_matches_oracle(oracle, L):
         assert np.array_equal(np.array(alphas, np.uint32), want_alphas)
         assert np.array_equal(np.array(roots, np.uint32), want_roots)
         assert np.array_equal(np.array(last, np.uint32), want_last)
-    # the challenge-drawing init kernel, then every layer of at most 2^10
-    # values in one tail launch; larger layers take their own tree launches
-    if L <= 11:
-        assert ch.launches() == 2
-    else:
-        assert ch.launches() >= 2 + (L - 11)
+    assert ch.launches() >= L
     ch.close()

@@ -13,7 +13,6 @@
 
 #include "vx_common.cuh"
 #include "vx_fri.cuh"
-#include "vx_fri_tail.cuh"
 #include "vx_merkle.cuh"
 #include "vx_twiddles.cuh"
 
@@ -133,17 +132,16 @@ extern "C" int vx_fri_chain_commit_async(vx_fri_chain *h, const uint32_t *const 
     chain_init_kernel<<<1, 32, 0, st>>>(h->chan, s8, h->alphas);
     VX_CUDA_TRY(cudaGetLastError());
     uint32_t launches = 1;
-    FoldLayer fl[32];
     for (uint32_t k = 0; k < h->nl; k++) {
         const uint32_t *const *in = k == 0 ? host_cols : (const uint32_t *const *)h->F[k - 1];
-        FoldLayer &f = fl[k];
-        for (int c = 0; c < 4; c++) { f.in[c] = in[c]; f.out[c] = h->F[k][c]; }
-        f.tw = k == 0 ? h->tw_circle : h->tw_line[h->L - k];
-        f.alpha = h->alphas + 4 * k;
-        f.lv = h->lv[k];
-        f.cs = ChanStep{h->chan, h->roots + 8 * k, k + 1 < h->nl ? h->alphas + 4 * (k + 1) : nullptr};
+        const uint32_t *tw = k == 0 ? h->tw_circle : h->tw_line[h->L - k];
+        LeafFold lf{in[0], in[1], in[2], in[3], tw, h->alphas + 4 * k,
+                    h->F[k][0], h->F[k][1], h->F[k][2], h->F[k][3], {}};
+        VX_CUDA_TRY(tree_build(lf, h->lv[k],
+                               ChanStep{h->chan, h->roots + 8 * k, k + 1 < h->nl ? h->alphas + 4 * (k + 1) : nullptr},
+                               st));
+        launches += tree_launches(h->lv[k]);
     }
-    VX_CUDA_TRY(fold_layers(fl, h->nl, st, &launches));
     h->launches = launches;
     return VX_OK;
 }

@@ -25,7 +25,6 @@
 #include "vx_common.cuh"
 #include "vx_field.cuh"
 #include "vx_fri.cuh"
-#include "vx_fri_tail.cuh"
 #include "vx_merkle.cuh"
 #include "vx_ntt.cuh"
 #include "vx_prover.cuh"
@@ -353,20 +352,19 @@ int lift_stage(vx_lifted *h, uint32_t stage, cudaStream_t st, uint32_t *launches
         *launches += tree_launches(h->flv[0]);
         break;
     }
-    case 4: {  // line folds
-        FoldLayer fl[32];
+    case 4:  // line folds
         for (uint32_t k = 1; k < L.nfri; k++) {
             const uint32_t lsrc = S - k;
-            FoldLayer &f = fl[k - 1];
-            for (int c = 0; c < 4; c++) { f.in[c] = h->F[k - 1][c]; f.out[c] = h->F[k][c]; }
-            f.tw = h->fold_line + h->fold_line_off[lsrc];
-            f.alpha = h->alpha_f + 4 * k;
-            f.lv = h->flv[k];
-            f.cs = ChanStep{h->chan, proof + L.froots + 8 * k, k + 1 < L.nfri ? h->alpha_f + 4 * (k + 1) : nullptr};
+            LeafFold lf{h->F[k - 1][0], h->F[k - 1][1], h->F[k - 1][2], h->F[k - 1][3],
+                        h->fold_line + h->fold_line_off[lsrc], h->alpha_f + 4 * k,
+                        h->F[k][0], h->F[k][1], h->F[k][2], h->F[k][3], {}};
+            VX_CUDA_TRY(tree_build(lf, h->flv[k],
+                                   ChanStep{h->chan, proof + L.froots + 8 * k,
+                                            k + 1 < L.nfri ? h->alpha_f + 4 * (k + 1) : nullptr},
+                                   st));
+            *launches += tree_launches(h->flv[k]);
         }
-        VX_CUDA_TRY(fold_layers(fl, L.nfri > 0 ? L.nfri - 1 : 0, st, launches));
         break;
-    }
     case 5: {
         const uint32_t kl = L.nfri - 1;
         lift_queries_kernel<<<1, 128, 0, st>>>(h->chan, h->F[kl][0], h->F[kl][1], h->F[kl][2], h->F[kl][3],

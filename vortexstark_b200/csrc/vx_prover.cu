@@ -19,7 +19,6 @@
 #include "vx_common.cuh"
 #include "vx_field.cuh"
 #include "vx_fri.cuh"
-#include "vx_fri_tail.cuh"
 #include "vx_merkle.cuh"
 #include "vx_ntt.cuh"
 #include "vx_prover.cuh"
@@ -591,20 +590,19 @@ static int enqueue_stage(vx_prover *p, uint32_t stage, uint32_t a, uint32_t b, c
         *launches += tree_launches(S.fri_lv[0]);
         break;
     }
-    case 6: {
-        FoldLayer fl[32];
+    case 6:
         for (uint32_t k = 1; k < L.nfri; k++) {
-            const uint32_t lsrc = le - k;  // log size of the layer being folded
-            FoldLayer &f = fl[k - 1];
-            for (int c = 0; c < 4; c++) { f.in[c] = S.fri[k - 1][c]; f.out[c] = S.fri[k][c]; }
-            f.tw = T.fold_line + T.fold_line_off[lsrc];
-            f.alpha = S.alpha_f + 4 * k;
-            f.lv = S.fri_lv[k];
-            f.cs = ChanStep{S.chan, proof + L.froots + 8 * k, k + 1 < L.nfri ? S.alpha_f + 4 * (k + 1) : nullptr};
+            uint32_t lsrc = le - k;  // log size of the layer being folded
+            LeafLineFold lf{S.fri[k - 1][0], S.fri[k - 1][1], S.fri[k - 1][2], S.fri[k - 1][3],
+                            T.fold_line + T.fold_line_off[lsrc], S.alpha_f + 4 * k,
+                            S.fri[k][0], S.fri[k][1], S.fri[k][2], S.fri[k][3], {}};
+            VX_CUDA_TRY(tree_build(lf, S.fri_lv[k],
+                                   ChanStep{S.chan, proof + L.froots + 8 * k,
+                                            k + 1 < L.nfri ? S.alpha_f + 4 * (k + 1) : nullptr},
+                                   st));
+            *launches += tree_launches(S.fri_lv[k]);
         }
-        VX_CUDA_TRY(fold_layers(fl, L.nfri > 0 ? L.nfri - 1 : 0, st, launches));
         break;
-    }
     case 7: {
         uint32_t kl = L.nfri - 1;
         chan_queries_kernel<<<1, 128, 0, st>>>(S.chan, S.fri[kl][0], S.fri[kl][1], S.fri[kl][2], S.fri[kl][3],
