@@ -929,10 +929,16 @@ def main():
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the six LDE launches of "
                                            "one log_n=24 proof, full size, one-pass metrics (plan 10 + 7 + 7); the "
                                            "bottom pass reads its twiddles, as large as the data",
-                         "algorithmic_bytes": lde_bytes, "time_ms": lde_t * 1e3},
+                         "algorithmic_bytes": lde_bytes, "time_ms": lde_t * 1e3,
+                         "note": "the proof's HBM-class kernel. It is issue-bound on the integer ALU pipe "
+                                 "(ncu: its bottom pass at ~89% of the ALU-pipe ceiling, DRAM 17-36%), so its "
+                                 "HBM fraction is low by construction. The dominant kernels, the Blake2s leaf "
+                                 "subtrees (~94% of a proof), are neither HBM- nor tensor-bound: see roofline_alu"},
             "roofline_alu": {"bound": "int-alu (Blake2s)", "kernel": f"trace commitment (2^{log_n + 2} leaves)",
                              "achieved": merkle_rate, "peak": probe_rate, "unit": "compressions/s",
-                             "frac": merkle_rate / probe_rate, "time_ms": tcommit_t * 1e3},
+                             "frac": merkle_rate / probe_rate, "time_ms": tcommit_t * 1e3,
+                             "peak_source": "measured in this run: a register-only chain of the same Blake2s "
+                                            "compression on every SM (vx_probe_blake2s)"},
             "stages_ms": stages_ms,
             "stage_rooflines": stage_roofline_table(stages_ms, log_n, peak, probe_rate),
             "gpu_launches": launches_per_proof * steps,
