@@ -7,7 +7,7 @@
 # forge-fri, forge-permute: build.rs:214-244), and links them with
 # ref_driver.cu (the prove_lean_inner orchestration restated over those
 # launchers) and the C oracle's host transcript into one shared library.
-# The .so is git-ignored and travels to the GPU box with the working tree.
+# The .so is git-ignored and travels with the working tree.
 set -euo pipefail
 REF=${VX_REFERENCE_ROOT:-/root/reference}
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"

@@ -1,4 +1,4 @@
-// ref_driver.cu — TEST INFRASTRUCTURE ONLY (checker, never shipped).
+// ref_driver.cu — TEST INFRASTRUCTURE ONLY (oracle side, never shipped).
 //
 // Drives the reference's own CUDA launchers, compiled from the reference's
 // sources by oracle/build_ref.sh into oracle/_ref/libvxref.so, through the

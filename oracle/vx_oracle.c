@@ -1,6 +1,6 @@
 /*
  * vx_oracle.c — CPU restatement of the VortexSTARK Fibonacci commitment
- * path.  TEST INFRASTRUCTURE ONLY (the checker and the CPU baseline); the
+ * path.  TEST INFRASTRUCTURE ONLY (the oracle and the CPU baseline); the
  * product library never links or calls it.
  *
  * Each function follows the reference file:line cited in vx_oracle.h.

@@ -1,7 +1,7 @@
 /*
  * vx_oracle.h — CPU restatement of the VortexSTARK Fibonacci commitment path.
  *
- * TEST INFRASTRUCTURE ONLY.  This library is the checker: the tests, the
+ * TEST INFRASTRUCTURE ONLY.  This library is the oracle: the tests, the
  * smoke entry and the CPU-baseline leg of the benchmark load it to produce
  * expected outputs.  The product path (vortexstark_b200) never calls it.
  *

@@ -105,7 +105,7 @@ def test_workload_streams_are_seeded():
 
 
 def test_package_imports_no_oracle():
-    """The product package never reaches into oracle/ (the checker)."""
+    """The product package never reaches into oracle/ (the oracle)."""
     root = os.path.dirname(vortexstark_b200.__file__)
     for dirpath, _, files in os.walk(root):
         for f in files:
