@@ -423,7 +423,8 @@ def kernel_microbench(peak_gbs: float, probe_rate: float, log_n: int = 26, reps:
             R = O.ref_lib()
             for name in ("cuda_merkle_tiled_generic", "cuda_merkle_hash_nodes", "cuda_merkle_reduce_to_root",
                          "cuda_fold_line_soa", "cuda_fold_circle_into_line_soa", "cuda_bit_reverse_qm31",
-                         "cuda_bit_reverse_m31", "cuda_permute_hc_to_canonic_brt"):
+                         "cuda_bit_reverse_m31", "cuda_permute_hc_to_canonic_brt", "cuda_eval_at_point",
+                         "cuda_barycentric_eval"):
                 getattr(R, name).argtypes = _lib._SIGS[name]
             libs["reference_kernels"] = R
     except Exception:
@@ -548,6 +549,48 @@ def kernel_microbench(peak_gbs: float, probe_rate: float, log_n: int = 26, reps:
                                                   "frac": 32 * n / (ms / 1e3) / 1e9 / peak_gbs}
     out["bit_reverse"] = br
     del qa, qb
+    torch.cuda.empty_cache()
+
+    # ---- stwo PolyOps: eval_at_point over 2^log_n coefficients (4 bytes each), barycentric_eval over
+    # 2^(log_n-2) points (an M31 value and a QM31 weight: 20 bytes each), 256 blocks as poly_ops.rs launches ----
+    from oracle import oracle as O_
+
+    coeffs = torch.from_numpy(m31_array(SEED + 5, n).view("int32")).cuda()
+    factors = torch.from_numpy(rng.integers(0, 0x7FFFFFFF, 4 * log_n, dtype=np.uint32).view(np.int32)).cuda()
+    s1 = torch.empty(2 * n, dtype=torch.int32, device="cuda")
+    s2 = torch.empty(n, dtype=torch.int32, device="cuda")
+    nb = n >> 2
+    weights = torch.from_numpy(rng.integers(0, 0x7FFFFFFF, 4 * nb, dtype=np.uint32).view(np.int32)).cuda()
+    n_blocks = min((nb + 255) // 256, 256)
+    part = torch.empty(4 * n_blocks, dtype=torch.int32, device="cuda")
+    res = (C.c_uint32 * 4)()
+    so, vals, parts = {}, {}, {}
+    for name, Lx in libs.items():
+        ms = _time_ms(lambda Lx=Lx: Lx.cuda_eval_at_point(coeffs.data_ptr(), factors.data_ptr(), res, n,
+                                                          s1.data_ptr(), s2.data_ptr()), ds, reps)
+        vals[name] = tuple(res)
+        so[f"eval_at_point_2^{log_n}_{name}"] = {"ms": ms, "gbs": 4 * n / (ms / 1e3) / 1e9,
+                                                 "frac": 4 * n / (ms / 1e3) / 1e9 / peak_gbs}
+        ms = _time_ms(lambda Lx=Lx: Lx.cuda_barycentric_eval(coeffs.data_ptr(), weights.data_ptr(), nb,
+                                                             part.data_ptr(), n_blocks), ds, reps)
+        parts[name] = bytes(part.cpu().numpy().tobytes())
+        so[f"barycentric_2^{log_n - 2}_{name}"] = {"ms": ms, "gbs": 20 * nb / (ms / 1e3) / 1e9,
+                                                   "frac": 20 * nb / (ms / 1e3) / 1e9 / peak_gbs}
+    so["values_equal"] = len(set(vals.values())) == 1 and len(set(parts.values())) == 1
+    if cpu:
+        hc = coeffs.cpu().numpy().view(np.uint32)
+        hf = factors.cpu().numpy().view(np.uint32).reshape(log_n, 4)
+        t0 = time.perf_counter()
+        ov = O_.eval_at_point(hc, hf)
+        so["eval_at_point_cpu_baseline"] = {"ms": 1e3 * (time.perf_counter() - t0), "cores": 1, "kind": "port",
+                                            "equal": tuple(int(x) for x in ov) == vals["vortex"]}
+        hw = weights.cpu().numpy().view(np.uint32).reshape(nb, 4)
+        t0 = time.perf_counter()
+        op = O_.barycentric_partials(hc[:nb], hw, n_blocks)
+        so["barycentric_cpu_baseline"] = {"ms": 1e3 * (time.perf_counter() - t0), "cores": 1, "kind": "port",
+                                          "equal": op.tobytes() == parts["vortex"]}
+    out["stwo_poly_ops"] = so
+    del coeffs, factors, s1, s2, weights, part
     torch.cuda.empty_cache()
     return out
 

@@ -320,3 +320,27 @@ def test_gathers_and_forge_aliases(oracle):
     L.cuda_bit_reverse_qm31(dq.data_ptr(), a.data_ptr(), 1024, 10)
     L.cuda_bit_reverse_qm31_forge(dq.data_ptr(), b.data_ptr(), 1024, 10)
     assert np.array_equal(to_host(a), to_host(b))
+
+
+def test_eval_and_barycentric_unaligned_inputs(oracle):
+    """The scalar-load forms: coefficients and weights one word off 16-byte alignment."""
+    import ctypes as C
+    rng = np.random.default_rng(77)
+    n = 1 << 13
+    coeffs = rng.integers(0, P, n + 1, dtype=np.uint32)
+    factors = _qm(rng, 13)
+    d_c, d_f = to_dev(coeffs), to_dev(factors.reshape(-1))
+    s1 = empty(2 * n + 8)
+    res = (C.c_uint32 * 4)()
+    _lib.clear_error()
+    _lib.lib().cuda_eval_at_point(d_c.data_ptr() + 4, d_f.data_ptr(), res, n, s1.data_ptr(), s1.data_ptr())
+    _lib.raise_if_error()
+    assert list(res) == oracle.eval_at_point(coeffs[1:], factors).tolist()
+    m = 5000
+    evals = rng.integers(0, P, m, dtype=np.uint32)
+    weights = rng.integers(0, P, 4 * m + 1, dtype=np.uint32)
+    d_e, d_w, out = to_dev(evals), to_dev(weights), empty(4 * 7)
+    _lib.lib().cuda_barycentric_eval(d_e.data_ptr(), d_w.data_ptr() + 4, m, out.data_ptr(), 7)
+    _lib.raise_if_error()
+    want = oracle.barycentric_partials(evals, weights[1:].reshape(m, 4), 7)
+    assert np.array_equal(to_host(out, 28).reshape(-1, 4), want)

@@ -154,6 +154,7 @@ __global__ void __launch_bounds__(256) pack_leaves_kernel(const uint32_t *const 
 constexpr uint32_t kEvalChunkLog = 11, kEvalThreads = 256;
 __device__ __forceinline__ qm31 qscale(qm31 f, uint32_t m) { return qmulm(f, m); }
 
+template <bool VEC>  // VEC: coeffs 16-byte aligned, two 16-byte loads per thread
 __global__ void __launch_bounds__(kEvalThreads) eval_chunk_kernel(const uint32_t *__restrict__ coeffs,
                                                                   const uint32_t *__restrict__ factors,
                                                                   uint32_t log_n, uint32_t *__restrict__ partial) {
@@ -168,8 +169,13 @@ __global__ void __launch_bounds__(kEvalThreads) eval_chunk_kernel(const uint32_t
     };
     const uint64_t base = ((uint64_t)blockIdx.x << kEvalChunkLog) + 8ull * t;
     uint32_t c[8];
+    if (VEC) {
+        const uint4 q0 = __ldg((const uint4 *)(coeffs + base)), q1 = __ldg((const uint4 *)(coeffs + base) + 1);
+        c[0] = q0.x; c[1] = q0.y; c[2] = q0.z; c[3] = q0.w; c[4] = q1.x; c[5] = q1.y; c[6] = q1.z; c[7] = q1.w;
+    } else {
 #pragma unroll
-    for (int j = 0; j < 8; j++) c[j] = coeffs[base + j];
+        for (int j = 0; j < 8; j++) c[j] = __ldg(coeffs + base + j);
+    }
     // index bits 2, 1, 0 of the thread's 8 coefficients
     const qm31 f2 = fac(2), f1 = fac(1), f0 = fac(0);
     qm31 u[4];
@@ -234,18 +240,41 @@ __global__ void __launch_bounds__(kEvalThreads) eval_sum_kernel(const uint32_t *
 // Block b accumulates evals[i] * weights[i] (M31 times QM31, weights AoS)
 // over the i that a grid-stride loop of n_blocks x 256 threads gives it, so
 // the partial sums are the reference's.
+// Each thread keeps kBaryInFlight of its elements in flight per step (the launch has
+// only n_blocks <= 256 blocks of 256 threads); it still accumulates exactly
+// the elements i = its index + k * (grid threads), so each block's sum is the
+// reference's.  VEC: weights 16-byte aligned, one 16-byte load per weight.
+constexpr int kBaryInFlight = 8;
+template <bool VEC>
+__device__ __forceinline__ qm31 bary_weight(const uint32_t *__restrict__ weights, uint64_t i) {
+    if (VEC) {
+        const uint4 q = __ldg((const uint4 *)weights + i);
+        return qm31{{q.x, q.y, q.z, q.w}};
+    }
+    const uint64_t b = 4ull * i;
+    return qm31{{__ldg(weights + b), __ldg(weights + b + 1), __ldg(weights + b + 2), __ldg(weights + b + 3)}};
+}
+
+template <bool VEC>
 __global__ void __launch_bounds__(256) barycentric_kernel(const uint32_t *__restrict__ evals,
                                                           const uint32_t *__restrict__ weights, uint32_t n,
                                                           uint32_t *__restrict__ out) {
     __shared__ qm31 s[8];
-    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     qm31 acc{{0u, 0u, 0u, 0u}};
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const uint32_t e = __ldg(evals + i);
-        const uint64_t b = 4ull * i;
-        const qm31 w{{__ldg(weights + b), __ldg(weights + b + 1), __ldg(weights + b + 2), __ldg(weights + b + 3)}};
-        acc = qadd(acc, qmulm(w, e));
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; i + (kBaryInFlight - 1) * stride < n; i += kBaryInFlight * stride) {
+        uint32_t e[kBaryInFlight];
+        qm31 w[kBaryInFlight];
+#pragma unroll
+        for (int k = 0; k < kBaryInFlight; k++) {
+            e[k] = __ldg(evals + i + k * stride);
+            w[k] = bary_weight<VEC>(weights, i + k * stride);
+        }
+#pragma unroll
+        for (int k = 0; k < kBaryInFlight; k++) acc = qadd(acc, qmulm(w[k], e[k]));
     }
+    for (; i < n; i += stride) acc = qadd(acc, qmulm(bary_weight<VEC>(weights, i), __ldg(evals + i)));
 #pragma unroll
     for (int m = 16; m > 0; m >>= 1) {
         qm31 o;
@@ -392,7 +421,10 @@ void cuda_gather_u256_forge(const uint32_t *src, const uint32_t *idx, uint32_t *
 void cuda_barycentric_eval(const uint32_t *evals, const uint32_t *weights, uint32_t n, uint32_t *out,
                            uint32_t n_blocks) {
     if (n_blocks == 0) return;
-    barycentric_kernel<<<n_blocks, 256>>>(evals, weights, n, out);
+    if (((uintptr_t)weights & 15u) == 0)
+        barycentric_kernel<true><<<n_blocks, 256>>>(evals, weights, n, out);
+    else
+        barycentric_kernel<false><<<n_blocks, 256>>>(evals, weights, n, out);
     VX_LAUNCH_CHECK();
     cudaDeviceSynchronize();  // the reference's launcher returns with the sums in place
 }
@@ -415,7 +447,10 @@ void cuda_eval_at_point(const uint32_t *d_coeffs, const uint32_t *d_folding_fact
         eval_sum_kernel<<<1, kEvalThreads>>>(nullptr, 0, d_coeffs, d_folding_factors, log_n, d_scratch1);
     } else {
         const uint64_t chunks = 1ull << (log_n - kEvalChunkLog);
-        eval_chunk_kernel<<<(unsigned)chunks, kEvalThreads>>>(d_coeffs, d_folding_factors, log_n, d_scratch1);
+        if (((uintptr_t)d_coeffs & 15u) == 0)
+            eval_chunk_kernel<true><<<(unsigned)chunks, kEvalThreads>>>(d_coeffs, d_folding_factors, log_n, d_scratch1);
+        else
+            eval_chunk_kernel<false><<<(unsigned)chunks, kEvalThreads>>>(d_coeffs, d_folding_factors, log_n, d_scratch1);
         eval_sum_kernel<<<1, kEvalThreads>>>(d_scratch1, chunks, nullptr, nullptr, 0, d_scratch1 + 4 * chunks);
         d_scratch1 += 4 * chunks;
     }
