@@ -424,7 +424,8 @@ def kernel_microbench(peak_gbs: float, probe_rate: float, log_n: int = 26, reps:
             for name in ("cuda_merkle_tiled_generic", "cuda_merkle_hash_nodes", "cuda_merkle_reduce_to_root",
                          "cuda_fold_line_soa", "cuda_fold_circle_into_line_soa", "cuda_bit_reverse_qm31",
                          "cuda_bit_reverse_m31", "cuda_permute_hc_to_canonic_brt", "cuda_eval_at_point",
-                         "cuda_barycentric_eval"):
+                         "cuda_barycentric_eval", "cuda_compute_coset_points", "cuda_extract_and_squash",
+                         "cuda_batch_inverse_m31"):
                 getattr(R, name).argtypes = _lib._SIGS[name]
             libs["reference_kernels"] = R
     except Exception:
@@ -591,6 +592,40 @@ def kernel_microbench(peak_gbs: float, probe_rate: float, log_n: int = 26, reps:
                                           "equal": op.tobytes() == parts["vortex"]}
     out["stwo_poly_ops"] = so
     del coeffs, factors, s1, s2, weights, part
+    torch.cuda.empty_cache()
+
+    # ---- twiddle tables of half_coset(log_n), forward and inverse, by the reference's call sequence
+    # (circle.rs:454-550: coset points, one extract-and-squash per line layer, batch inverses) ----
+    from vortexstark_b200.circle import Coset
+
+    co = Coset.half_coset(log_n)
+    xs, ys = (torch.empty(n, dtype=torch.int32, device="cuda") for _ in range(2))
+    line, iline = (torch.empty(n - 1, dtype=torch.int32, device="cuda") for _ in range(2))
+    icirc = torch.empty(n // 2, dtype=torch.int32, device="cuda")
+    sq = [torch.empty(n >> (j + 1), dtype=torch.int32, device="cuda") for j in range(log_n - 1)]
+    tw, tables = {}, {}
+    for name, Lx in libs.items():
+        def build(Lx=Lx):
+            Lx.cuda_compute_coset_points(co.initial.x, co.initial.y, co.step.x, co.step.y, xs.data_ptr(),
+                                         ys.data_ptr(), n)
+            cur, m, off = xs, n, 0
+            for j in range(log_n - 1):
+                Lx.cuda_extract_and_squash(cur.data_ptr(), line.data_ptr() + 4 * off, sq[j].data_ptr(), m // 2)
+                off += m // 2
+                cur, m = sq[j], m // 2
+            Lx.cuda_batch_inverse_m31(line.data_ptr(), iline.data_ptr(), n - 1)
+            Lx.cuda_batch_inverse_m31(ys.data_ptr(), icirc.data_ptr(), n // 2)
+        ms = _time_ms(build, ds, reps)
+        tables[name] = hash(bytes(line.cpu().numpy().tobytes()) + bytes(iline.cpu().numpy().tobytes())
+                            + bytes(icirc.cpu().numpy().tobytes()))
+        # bytes: coset points 8n written; the line layers 16n (each reads its points, writes its twiddles and
+        # the squashed points); the batch inverses 12n (read and write n - 1 + n/2 words)
+        tb = 36 * n
+        tw[name] = {"ms": ms, "gbs": tb / (ms / 1e3) / 1e9, "frac": tb / (ms / 1e3) / 1e9 / peak_gbs}
+    tw["bytes"] = 36 * n
+    tw["tables_equal"] = len(set(tables.values())) == 1
+    out["twiddle_tables"] = tw
+    del xs, ys, line, iline, icirc, sq
     torch.cuda.empty_cache()
     return out
 

@@ -129,6 +129,19 @@ def test_batch_inverse(oracle, L):
     assert np.array_equal(to_host(o, len(x)), oracle.batch_inverse(x))
 
 
+@pytest.mark.parametrize("n", [1, 63, 64, 65, 4095, 4096, 4097, 8192 + 64, (1 << 20) + 3])
+def test_batch_inverse_sizes_and_in_place(oracle, L, n):
+    """Chunk (64) and block (4096) boundaries, zeros in first and other slots, in place."""
+    x = m31_array(90 + n % 1000, n)
+    x[::97] = 0
+    want = oracle.batch_inverse(x)
+    d, o = to_dev(x), empty(n)
+    L.cuda_batch_inverse_m31(d.data_ptr(), o.data_ptr(), n)
+    assert np.array_equal(to_host(o, n), want)
+    L.cuda_batch_inverse_m31(d.data_ptr(), d.data_ptr(), n)
+    assert np.array_equal(to_host(d, n), want)
+
+
 @pytest.mark.parametrize("kind,ey", [("half_coset", 1), ("half_odds", 0), ("subgroup", 1), ("half_coset", 0)])
 @pytest.mark.parametrize("k", [2, 7, 15])
 def test_fold_twiddles(oracle, kind, ey, k):

@@ -40,16 +40,18 @@ inline uint32_t log2_exact(uint64_t n) {
 
 // ---- twiddle helpers for arbitrary (initial, step) points ----
 // p_j = initial * step^j, 16 consecutive points per thread (twiddles.cu:80-105).
+// Thread t of T writes points t, t + T, t + 2T, ... (about 16 each), stepping
+// by step^T, so a warp's stores are consecutive words.
 __global__ void coset_points_kernel(cpoint init, cpoint step, uint32_t *xs, uint32_t *ys, uint64_t n) {
-    uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    uint64_t j0 = t * 16ull;
-    if (j0 >= n) return;
-    cpoint p = pmul(init, ppow(step, j0));
-    uint64_t j1 = j0 + 16ull < n ? j0 + 16ull : n;
-    for (uint64_t j = j0; j < j1; j++) {
+    const uint64_t T = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const cpoint stride_step = ppow(step, T);
+    cpoint p = pmul(init, ppow(step, t));
+    for (uint64_t j = t; j < n; j += T) {
         xs[j] = p.x;
         ys[j] = p.y;
-        p = pmul(p, step);
+        p = pmul(p, stride_step);
     }
 }
 

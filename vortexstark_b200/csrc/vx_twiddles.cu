@@ -60,29 +60,51 @@ __global__ void stwo_fold_circle_kernel(GenTables g, uint32_t log, uint32_t *out
 }
 
 // One thread per aligned chunk of 64, mirroring batch_inverse.cu:8-41
-// exactly, including the zero-first-slot behaviour.  Safe in place.
-__global__ void batch_inverse_kernel(const uint32_t *in, uint32_t *out, uint64_t n) {
-    uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    uint64_t s = c * 64ull;
-    if (s >= n) return;
-    uint32_t cnt = (uint32_t)((n - s) < 64ull ? (n - s) : 64ull);
-    uint32_t pre[64];
-    uint32_t acc = in[s];
-    pre[0] = acc;
-    for (uint32_t i = 1; i < cnt; i++) {
-        uint32_t v = in[s + i];
-        acc = v ? mmul(acc, v) : acc;
-        pre[i] = acc;
+// exactly, including the zero-first-slot behaviour: prefix products that
+// skip zeros, one inversion, then the backward pass.  A block of 64 threads
+// stages its 64 chunks (4096 words) through shared memory, so global loads
+// and stores are coalesced; chunk c's word i sits at 65 c + i, so the
+// threads' per-chunk walks hit distinct banks.  The outputs overwrite the
+// prefix slots (slot i is last read at step i + 1 of the backward pass).
+// Every load of a block precedes its stores, and blocks own disjoint
+// ranges, so it is safe in place.
+constexpr uint32_t kBiChunk = 64, kBiThreads = 64, kBiWords = kBiChunk * kBiThreads;
+
+__global__ void __launch_bounds__(kBiThreads) batch_inverse_kernel(const uint32_t *in, uint32_t *out, uint64_t n) {
+    __shared__ uint32_t xv[kBiWords + kBiThreads], pre[kBiWords + kBiThreads];
+    const uint32_t t = threadIdx.x;
+    const uint64_t base = (uint64_t)blockIdx.x * kBiWords;
+    for (uint32_t e = t; e < kBiWords; e += kBiThreads) {
+        const uint64_t g = base + e;
+        xv[e + e / kBiChunk] = g < n ? in[g] : 0u;
     }
-    uint32_t first = in[s];
-    uint32_t inv = minv(acc);
-    for (uint32_t i = cnt - 1; i > 0; i--) {
-        uint32_t v = in[s + i];
-        if (!v) { out[s + i] = 0u; continue; }
-        out[s + i] = mmul(inv, pre[i - 1]);
-        inv = mmul(inv, v);
+    __syncthreads();
+    const uint64_t s = base + (uint64_t)t * kBiChunk;
+    if (s < n) {
+        const uint32_t cnt = (uint32_t)((n - s) < kBiChunk ? (n - s) : kBiChunk);
+        uint32_t *x = xv + t * (kBiChunk + 1), *pr = pre + t * (kBiChunk + 1);
+        uint32_t acc = x[0];
+        pr[0] = acc;
+        for (uint32_t i = 1; i < cnt; i++) {
+            const uint32_t v = x[i];
+            acc = v ? mmul(acc, v) : acc;
+            pr[i] = acc;
+        }
+        const uint32_t first = x[0];
+        uint32_t inv = minv(acc);
+        for (uint32_t i = cnt - 1; i > 0; i--) {
+            const uint32_t v = x[i];
+            if (!v) { pr[i] = 0u; continue; }
+            pr[i] = mmul(inv, pr[i - 1]);
+            inv = mmul(inv, v);
+        }
+        pr[0] = first ? inv : 0u;
     }
-    out[s] = first ? inv : 0u;
+    __syncthreads();
+    for (uint32_t e = t; e < kBiWords; e += kBiThreads) {
+        const uint64_t g = base + e;
+        if (g < n) out[g] = pre[e + e / kBiChunk];
+    }
 }
 
 }  // namespace
@@ -114,8 +136,7 @@ cudaError_t gen_tables_get(GenTables *out) {
 
 cudaError_t batch_inverse(const uint32_t *in, uint32_t *out, uint64_t n, cudaStream_t stream) {
     if (!n) return cudaSuccess;
-    uint64_t chunks = (n + 63) / 64;
-    batch_inverse_kernel<<<blocks_for(chunks, 128), 128, 0, stream>>>(in, out, n);
+    batch_inverse_kernel<<<(unsigned)((n + kBiWords - 1) / kBiWords), kBiThreads, 0, stream>>>(in, out, n);
     return cudaGetLastError();
 }
 
