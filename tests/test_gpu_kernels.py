@@ -190,7 +190,7 @@ def _tree_levels(oracle, cols):
     return levels
 
 
-@pytest.mark.parametrize("ncols", [1, 4, 7, 16, 20])
+@pytest.mark.parametrize("ncols", [1, 2, 4, 7, 8, 16, 20])
 def test_merkle_leaves_nodes(oracle, L, ncols):
     n = 256
     cols = [m31_array(100 * ncols + i, n) for i in range(ncols)]
@@ -231,6 +231,18 @@ def test_merkle_soa4_variants(oracle, L):
     sub2 = empty(16)
     L.cuda_merkle_tiled_generic(_ptrs(d).data_ptr(), sub2.data_ptr(), 4, n)
     assert np.array_equal(to_host(sub2).reshape(-1, 8), lv[10])
+
+
+@pytest.mark.parametrize("ncols", [1, 2, 3, 8])
+def test_merkle_tiled_generic_column_counts(oracle, L, ncols):
+    """1024-leaf subtree roots for the compile-time column counts and the generic fallback (3)."""
+    n = 4096
+    cols = [m31_array(300 + 10 * ncols + i, n) for i in range(ncols)]
+    d = [to_dev(c) for c in cols]
+    lv = _tree_levels(oracle, cols)
+    sub = empty(8 * (n // 1024))
+    L.cuda_merkle_tiled_generic(_ptrs(d).data_ptr(), sub.data_ptr(), ncols, n)
+    assert np.array_equal(to_host(sub).reshape(-1, 8), lv[10])
 
 
 @pytest.mark.parametrize("log_n,ncols", [(12, 1), (16, 4), (20, 1)])

@@ -55,6 +55,23 @@ struct LeafCols {
         return 4u * n;
     }
 };
+// The same with the column count fixed at compile time: the message words
+// past the N loaded ones are known zeros, whose additions the compression
+// drops (a one-column leaf then costs what LeafM31's does).
+template <uint32_t N>
+struct LeafColsN {
+    const uint32_t *const *cols;
+    const uint32_t *p[N];  // the column pointers, read once by init()
+    __device__ __forceinline__ void init() {
+#pragma unroll
+        for (uint32_t c = 0; c < N; c++) p[c] = cols[c];
+    }
+    __device__ __forceinline__ uint32_t load(uint64_t i, uint32_t m[16]) const {
+#pragma unroll
+        for (uint32_t c = 0; c < N; c++) m[c] = __ldg(p[c] + i);
+        return 4u * N;
+    }
+};
 // Up to 16 columns passed by value (host-side pointer list); t = 4 * n.
 struct LeafColsV {
     const uint32_t *col[16];
@@ -151,11 +168,11 @@ struct LeafLifted {
     }
 };
 
-// Fold a subtree of 2^kl leaves starting at `base` into its root.
-template <class Src>
+// Fold a subtree of 2^kl leaves (kl <= KMAX) starting at `base` into its root.
+template <class Src, uint32_t KMAX = 5>
 __device__ __forceinline__ void subtree_root(const Src &src, uint64_t base, uint32_t kl, uint32_t root[8],
                                              uint32_t one = 1u) {
-    uint32_t stk[5][8];
+    uint32_t stk[KMAX][8];
     uint32_t sp = 0;
     const uint32_t K = 1u << kl;
     for (uint32_t j = 0; j < K; j++) {
