@@ -425,7 +425,7 @@ def kernel_microbench(peak_gbs: float, probe_rate: float, log_n: int = 26, reps:
                          "cuda_fold_line_soa", "cuda_fold_circle_into_line_soa", "cuda_bit_reverse_qm31",
                          "cuda_bit_reverse_m31", "cuda_permute_hc_to_canonic_brt", "cuda_eval_at_point",
                          "cuda_barycentric_eval", "cuda_compute_coset_points", "cuda_extract_and_squash",
-                         "cuda_batch_inverse_m31"):
+                         "cuda_batch_inverse_m31", "cuda_fibonacci_quotient"):
                 getattr(R, name).argtypes = _lib._SIGS[name]
             libs["reference_kernels"] = R
     except Exception:
@@ -550,6 +550,21 @@ def kernel_microbench(peak_gbs: float, probe_rate: float, log_n: int = 26, reps:
                                                   "frac": 32 * n / (ms / 1e3) / 1e9 / peak_gbs}
     out["bit_reverse"] = br
     del qa, qb
+    torch.cuda.empty_cache()
+
+    # ---- Fibonacci quotient over a 2^log_n-point evaluation (reads 4 B, writes 4 x 4 B per point) ----
+    tr = torch.from_numpy(m31_array(SEED + 6, n).view("int32")).cuda()
+    qo = [torch.empty(n, dtype=torch.int32, device="cuda") for _ in range(4)]
+    qa = (C.c_uint32 * 4)(*[int(x) for x in rng.integers(0, 0x7FFFFFFF, 4)])
+    qt, qs = {}, {}
+    for name, Lx in libs.items():
+        ms = _time_ms(lambda Lx=Lx: Lx.cuda_fibonacci_quotient(tr.data_ptr(), *[q.data_ptr() for q in qo], qa, n),
+                      ds, reps)
+        qs[name] = hash(b"".join(bytes(q.cpu().numpy().tobytes()) for q in qo))
+        qt[name] = {"ms": ms, "gbs": 20 * n / (ms / 1e3) / 1e9, "frac": 20 * n / (ms / 1e3) / 1e9 / peak_gbs}
+    qt["values_equal"] = len(set(qs.values())) == 1
+    out["fibonacci_quotient"] = qt
+    del tr, qo
     torch.cuda.empty_cache()
 
     # ---- stwo PolyOps: eval_at_point over 2^log_n coefficients (4 bytes each), barycentric_eval over

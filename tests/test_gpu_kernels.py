@@ -173,6 +173,34 @@ def test_zero_pad_and_quotient(oracle, L):
         assert np.array_equal(to_host(qc[c], 512), want[c][N - 512:])
 
 
+def test_quotient_chunk_unaligned(oracle, L):
+    """A chunk whose offset and length are not multiples of 4 (the scalar form), ending at the wrap."""
+    N = 1000
+    ev = m31_array(61, N)
+    alpha = (9, 10, 11, 12)
+    dev = to_dev(ev)
+    want = oracle.fibonacci_quotient(ev, alpha)
+    for off, cnt in ((3, 10), (N - 7, 7), (0, 999)):
+        q = [empty(cnt) for _ in range(4)]
+        L.cuda_fibonacci_quotient_chunk(dev.data_ptr(), *[c.data_ptr() for c in q], (C.c_uint32 * 4)(*alpha), off,
+                                        cnt, N)
+        for c in range(4):
+            assert np.array_equal(to_host(q[c], cnt), want[c][off:off + cnt])
+
+
+@pytest.mark.parametrize("N", [1, 2, 3, 5])
+def test_quotient_tiny_domains(oracle, L, N):
+    """(i + 1) mod N and (i + 2) mod N where i + 2 can pass 2N."""
+    ev = m31_array(40 + N, N)
+    alpha = (5, 6, 7, 8)
+    dev = to_dev(ev)
+    q = [empty(N) for _ in range(4)]
+    L.cuda_fibonacci_quotient(dev.data_ptr(), *[c.data_ptr() for c in q], (C.c_uint32 * 4)(*alpha), N)
+    want = oracle.fibonacci_quotient(ev, alpha)
+    for c in range(4):
+        assert np.array_equal(to_host(q[c], N), want[c])
+
+
 def _ptrs(ts):
     import torch
     return torch.tensor([t.data_ptr() for t in ts], dtype=torch.int64, device="cuda")

@@ -80,15 +80,53 @@ __global__ void zero_pad_kernel(const uint32_t *src, uint32_t *dst, uint64_t src
     dst[i] = i < src_n ? src[i] : 0u;
 }
 
+__device__ __forceinline__ void quotient_one(const uint32_t *tr, uint32_t *o0, uint32_t *o1, uint32_t *o2,
+                                             uint32_t *o3, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                             uint64_t li, uint64_t i, uint64_t global_n) {
+    // (i + 1) mod N and (i + 2) mod N for i < N by one conditional subtraction
+    // each; N < 3 (where i + 2 can pass 2N) keeps the division
+    uint64_t i1 = i + 1, i2 = i + 2;
+    if (global_n > 2) {
+        if (i1 >= global_n) i1 -= global_n;
+        if (i2 >= global_n) i2 -= global_n;
+    } else {
+        i1 %= global_n;
+        i2 %= global_n;
+    }
+    const uint32_t c = msub(tr[i2], madd(tr[i1], tr[i]));
+    o0[li] = mmul(a0, c); o1[li] = mmul(a1, c); o2[li] = mmul(a2, c); o3[li] = mmul(a3, c);
+}
+
+// VEC: four consecutive points per thread with 16-byte loads and stores
+// (the host checks 16-byte alignment of every array, offset and chunk
+// multiples of 4 and N > 2); the last group before the wrap-around takes the
+// scalar form.
+template <bool VEC>
 __global__ void quotient_kernel(const uint32_t *tr, uint32_t *o0, uint32_t *o1, uint32_t *o2, uint32_t *o3,
                                 uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint64_t offset, uint64_t chunk,
                                 uint64_t global_n) {
-    uint64_t li = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (!VEC) {
+        if (t < chunk) quotient_one(tr, o0, o1, o2, o3, a0, a1, a2, a3, t, offset + t, global_n);
+        return;
+    }
+    const uint64_t li = 4 * t;
     if (li >= chunk) return;
-    uint64_t i = offset + li;
-    uint32_t t0 = tr[i], t1 = tr[(i + 1) % global_n], t2 = tr[(i + 2) % global_n];
-    uint32_t c = msub(t2, madd(t1, t0));
-    o0[li] = mmul(a0, c); o1[li] = mmul(a1, c); o2[li] = mmul(a2, c); o3[li] = mmul(a3, c);
+    const uint64_t i = offset + li;
+    if (i + 5 >= global_n) {
+        for (uint32_t k = 0; k < 4; k++) quotient_one(tr, o0, o1, o2, o3, a0, a1, a2, a3, li + k, i + k, global_n);
+        return;
+    }
+    const uint4 x = *(const uint4 *)(tr + i);
+    const uint2 y = *(const uint2 *)(tr + i + 4);
+    const uint32_t v[6] = {x.x, x.y, x.z, x.w, y.x, y.y};
+    uint32_t c[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) c[k] = msub(v[k + 2], madd(v[k + 1], v[k]));
+    *(uint4 *)(o0 + li) = make_uint4(mmul(a0, c[0]), mmul(a0, c[1]), mmul(a0, c[2]), mmul(a0, c[3]));
+    *(uint4 *)(o1 + li) = make_uint4(mmul(a1, c[0]), mmul(a1, c[1]), mmul(a1, c[2]), mmul(a1, c[3]));
+    *(uint4 *)(o2 + li) = make_uint4(mmul(a2, c[0]), mmul(a2, c[1]), mmul(a2, c[2]), mmul(a2, c[3]));
+    *(uint4 *)(o3 + li) = make_uint4(mmul(a3, c[0]), mmul(a3, c[1]), mmul(a3, c[2]), mmul(a3, c[3]));
 }
 
 // ---- bit reverse / permute ----
@@ -628,8 +666,16 @@ void cuda_zero_pad(const uint32_t *src, uint32_t *dst, uint32_t src_n, uint32_t 
 void cuda_fibonacci_quotient_chunk_stream(const uint32_t *tr, uint32_t *o0, uint32_t *o1, uint32_t *o2, uint32_t *o3,
                                           const uint32_t *al, uint32_t offset, uint32_t chunk_n, uint32_t global_n,
                                           void *stream) {
-    quotient_kernel<<<blocks_for(chunk_n, 256), 256, 0, (cudaStream_t)stream>>>(tr, o0, o1, o2, o3, al[0], al[1], al[2],
-                                                                               al[3], offset, chunk_n, global_n);
+    if (chunk_n == 0) return;
+    const cudaStream_t st = (cudaStream_t)stream;
+    const bool vec = ((((uintptr_t)tr | (uintptr_t)o0 | (uintptr_t)o1 | (uintptr_t)o2 | (uintptr_t)o3) & 15u) == 0) &&
+                     offset % 4u == 0 && chunk_n % 4u == 0 && global_n > 2;
+    if (vec)
+        quotient_kernel<true><<<blocks_for(chunk_n / 4u, 256), 256, 0, st>>>(tr, o0, o1, o2, o3, al[0], al[1], al[2],
+                                                                           al[3], offset, chunk_n, global_n);
+    else
+        quotient_kernel<false><<<blocks_for(chunk_n, 256), 256, 0, st>>>(tr, o0, o1, o2, o3, al[0], al[1], al[2],
+                                                                        al[3], offset, chunk_n, global_n);
     VX_LAUNCH_CHECK();
 }
 
