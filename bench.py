@@ -552,6 +552,19 @@ def kernel_microbench(peak_gbs: float, probe_rate: float, log_n: int = 26, reps:
     del qa, qb
     torch.cuda.empty_cache()
 
+    # ---- zero-pad of 2^(log_n-2) coefficients into a 2^log_n-point buffer (prover.rs:308) ----
+    zs = torch.from_numpy(m31_array(SEED + 7, n >> 2).view("int32")).cuda()
+    zd = torch.empty(n, dtype=torch.int32, device="cuda")
+    zp = {}
+    for name, Lx in libs.items():
+        Lx.cuda_zero_pad.argtypes = _lib._SIGS["cuda_zero_pad"]
+        ms = _time_ms(lambda Lx=Lx: Lx.cuda_zero_pad(zs.data_ptr(), zd.data_ptr(), n >> 2, n), ds, reps)
+        zb = 4 * (n >> 2) + 4 * n  # read the coefficients, write the buffer
+        zp[name] = {"ms": ms, "gbs": zb / (ms / 1e3) / 1e9, "frac": zb / (ms / 1e3) / 1e9 / peak_gbs}
+    out["zero_pad"] = zp
+    del zs, zd
+    torch.cuda.empty_cache()
+
     # ---- Fibonacci quotient over a 2^log_n-point evaluation (reads 4 B, writes 4 x 4 B per point) ----
     tr = torch.from_numpy(m31_array(SEED + 6, n).view("int32")).cuda()
     qo = [torch.empty(n, dtype=torch.int32, device="cuda") for _ in range(4)]

@@ -173,6 +173,16 @@ def test_zero_pad_and_quotient(oracle, L):
         assert np.array_equal(to_host(qc[c], 512), want[c][N - 512:])
 
 
+@pytest.mark.parametrize("n,N,shift", [(1, 1, 0), (5, 13, 0), (1024, 4096, 0), (1001, 4099, 0), (6, 11, 1)])
+def test_zero_pad_sizes(L, n, N, shift):
+    """Ragged lengths, a straddling group, and an unaligned (word-offset) source and destination."""
+    x = m31_array(70 + n, n + shift)
+    s, d = to_dev(x), to_dev(np.full(N + shift, 0xDEAD, np.uint32))
+    L.cuda_zero_pad(s.data_ptr() + 4 * shift, d.data_ptr() + 4 * shift, n, N)
+    got = to_host(d, N + shift)[shift:]
+    assert np.array_equal(got[:n], x[shift:shift + n]) and not got[n:].any()
+
+
 def test_quotient_chunk_unaligned(oracle, L):
     """A chunk whose offset and length are not multiples of 4 (the scalar form), ending at the wrap."""
     N = 1000

@@ -74,10 +74,24 @@ __global__ void fold_sources_generic_kernel(cpoint init, cpoint step, uint32_t *
 }
 
 // ---- glue (constraint.cu) ----
+// VEC: four words per thread with 16-byte accesses (both arrays 16-byte
+// aligned); a group that straddles src_n or dst_n goes word by word.
+template <bool VEC>
 __global__ void zero_pad_kernel(const uint32_t *src, uint32_t *dst, uint64_t src_n, uint64_t dst_n) {
-    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (!VEC) {
+        if (t < dst_n) dst[t] = t < src_n ? src[t] : 0u;
+        return;
+    }
+    const uint64_t i = 4 * t;
     if (i >= dst_n) return;
-    dst[i] = i < src_n ? src[i] : 0u;
+    if (i + 4 <= dst_n && i + 4 <= src_n) {
+        *(uint4 *)(dst + i) = *(const uint4 *)(src + i);
+    } else if (i + 4 <= dst_n && i >= src_n) {
+        *(uint4 *)(dst + i) = make_uint4(0u, 0u, 0u, 0u);
+    } else {
+        for (uint64_t j = i; j < i + 4 && j < dst_n; j++) dst[j] = j < src_n ? src[j] : 0u;
+    }
 }
 
 __device__ __forceinline__ void quotient_one(const uint32_t *tr, uint32_t *o0, uint32_t *o1, uint32_t *o2,
@@ -659,7 +673,10 @@ void cuda_compute_fold_twiddle_sources(uint32_t ix, uint32_t iy, uint32_t sx, ui
 
 // ---------------- glue ----------------
 void cuda_zero_pad(const uint32_t *src, uint32_t *dst, uint32_t src_n, uint32_t dst_n) {
-    zero_pad_kernel<<<blocks_for(dst_n, 256), 256>>>(src, dst, src_n, dst_n);
+    if ((((uintptr_t)src | (uintptr_t)dst) & 15u) == 0)
+        zero_pad_kernel<true><<<blocks_for(((uint64_t)dst_n + 3) / 4, 256), 256>>>(src, dst, src_n, dst_n);
+    else
+        zero_pad_kernel<false><<<blocks_for(dst_n, 256), 256>>>(src, dst, src_n, dst_n);
     VX_LAUNCH_CHECK();
 }
 
