@@ -425,7 +425,9 @@ def kernel_microbench(peak_gbs: float, probe_rate: float, log_n: int = 26, reps:
                          "cuda_fold_line_soa", "cuda_fold_circle_into_line_soa", "cuda_bit_reverse_qm31",
                          "cuda_bit_reverse_m31", "cuda_permute_hc_to_canonic_brt", "cuda_eval_at_point",
                          "cuda_barycentric_eval", "cuda_compute_coset_points", "cuda_extract_and_squash",
-                         "cuda_batch_inverse_m31", "cuda_fibonacci_quotient"):
+                         "cuda_batch_inverse_m31", "cuda_fibonacci_quotient", "cuda_stwo_ntt_evaluate",
+                         "cuda_stwo_ntt_interpolate", "cuda_stwo_ntt_batch_evaluate",
+                         "cuda_stwo_ntt_batch_interpolate"):
                 getattr(R, name).argtypes = _lib._SIGS[name]
             libs["reference_kernels"] = R
     except Exception:
@@ -550,6 +552,38 @@ def kernel_microbench(peak_gbs: float, probe_rate: float, log_n: int = 26, reps:
                                                   "frac": 32 * n / (ms / 1e3) / 1e9 / peak_gbs}
     out["bit_reverse"] = br
     del qa, qb
+    torch.cuda.empty_cache()
+
+    # ---- stwo NTT (PolyOps::evaluate_polynomials / interpolate, poly_ops.rs): one column of 2^(log_n-2) and a
+    # batch of 16 columns of 2^(log_n-6), tables in stwo's layout built on the device; 8 B per element ----
+    sn = {}
+    for tag, lg, ncol in (("single", log_n - 2, 1), ("batch16", log_n - 6, 16)):
+        m = 1 << lg
+        tw = torch.empty(m // 2, dtype=torch.int32, device="cuda")
+        itw = torch.empty(m // 2, dtype=torch.int32, device="cuda")
+        _lib.check(_lib.lib().vx_stwo_twiddles(lg, 0, tw.data_ptr(), None))
+        _lib.check(_lib.lib().vx_stwo_twiddles(lg, 1, itw.data_ptr(), None))
+        cols = [torch.from_numpy(m31_array(SEED + 8 + c, m).view("int32")).cuda() for c in range(ncol)]
+        ptrs = (C.c_void_p * ncol)(*[c.data_ptr() for c in cols])
+        outs = {}
+        for name, Lx in libs.items():
+            if ncol == 1:
+                ev = lambda Lx=Lx: Lx.cuda_stwo_ntt_evaluate(cols[0].data_ptr(), tw.data_ptr(), m)
+                it = lambda Lx=Lx: Lx.cuda_stwo_ntt_interpolate(cols[0].data_ptr(), itw.data_ptr(), m)
+            else:
+                ev = lambda Lx=Lx: Lx.cuda_stwo_ntt_batch_evaluate(ptrs, tw.data_ptr(), m, ncol)
+                it = lambda Lx=Lx: Lx.cuda_stwo_ntt_batch_interpolate(ptrs, itw.data_ptr(), m, ncol)
+            ev()
+            outs[name] = hash(b"".join(bytes(c.cpu().numpy().tobytes()) for c in cols))
+            it()
+            b = 8 * m * ncol
+            for op, fn in (("evaluate", ev), ("interpolate", it)):
+                ms = _time_ms(fn, ds, reps)
+                sn[f"{tag}_2^{lg}_{op}_{name}"] = {"ms": ms, "gbs": b / (ms / 1e3) / 1e9,
+                                                   "frac": b / (ms / 1e3) / 1e9 / peak_gbs}
+        sn[f"{tag}_values_equal"] = len(set(outs.values())) == 1
+        del cols, tw, itw
+    out["stwo_ntt"] = sn
     torch.cuda.empty_cache()
 
     # ---- zero-pad of 2^(log_n-2) coefficients into a 2^log_n-point buffer (prover.rs:308) ----
