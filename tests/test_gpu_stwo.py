@@ -223,7 +223,7 @@ def _qm(rng, n):
     return rng.integers(0, P, (n, 4), dtype=np.uint32)
 
 
-@pytest.mark.parametrize("log_n", [0, 1, 3, 10, 11, 12, 16, 20])
+@pytest.mark.parametrize("log_n", [0, 1, 3, 10, 11, 12, 13, 16, 20, 21, 22, 23])
 def test_eval_at_point_matches_oracle_and_reference(oracle, log_n):
     """cuda_eval_at_point (PolyOps::eval_at_point, poly_ops.rs:382-443)."""
     import ctypes as C
@@ -330,10 +330,14 @@ def test_eval_and_barycentric_unaligned_inputs(oracle):
     coeffs = rng.integers(0, P, n + 1, dtype=np.uint32)
     factors = _qm(rng, 13)
     d_c, d_f = to_dev(coeffs), to_dev(factors.reshape(-1))
-    s1 = empty(2 * n + 8)
+    s1, s2 = empty(2 * n + 8), empty(2 * n + 8)
     res = (C.c_uint32 * 4)()
     _lib.clear_error()
-    _lib.lib().cuda_eval_at_point(d_c.data_ptr() + 4, d_f.data_ptr(), res, n, s1.data_ptr(), s1.data_ptr())
+    _lib.lib().cuda_eval_at_point(d_c.data_ptr() + 4, d_f.data_ptr(), res, n, s1.data_ptr(), s2.data_ptr())
+    _lib.raise_if_error()
+    assert list(res) == oracle.eval_at_point(coeffs[1:], factors).tolist()
+    # an unaligned first scratch buffer takes the chunk fold
+    _lib.lib().cuda_eval_at_point(d_c.data_ptr() + 4, d_f.data_ptr(), res, n, s1.data_ptr() + 4, s2.data_ptr())
     _lib.raise_if_error()
     assert list(res) == oracle.eval_at_point(coeffs[1:], factors).tolist()
     m = 5000

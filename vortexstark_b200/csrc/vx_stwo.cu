@@ -204,6 +204,88 @@ __global__ void __launch_bounds__(kEvalThreads) eval_chunk_kernel(const uint32_t
     }
 }
 
+// Table-driven form for log_n >= 12.  With i = hi 2^11 + lo,
+//   value = sum_hi W(hi) sum_lo c[i] w(lo),
+// w(lo) the product of the factors of lo's set bits (bits 0..10) and W(hi)
+// that of hi's (bits 11..), W(hi) = T1[hi mod 2^m1] T2[hi >> m1].  One block
+// builds w, T1 and T2 by doubling; persistent blocks hold w in shared memory,
+// take 2048-coefficient chunks, multiply-accumulate in 64 bits and scale each
+// chunk sum by W(hi); a last launch adds the block sums.
+constexpr uint32_t kEvTabLog = 11, kEvTabThreads = 1024, kEvAccThreads = 256;
+
+// Block 0 builds w (index bits 0..10), block 1 T1 (bits 11..11+m1-1),
+// block 2 T2 (the rest), each by doubling in shared memory, then writes it.
+__global__ void __launch_bounds__(kEvTabThreads) eval_tables_kernel(const uint32_t *__restrict__ factors,
+                                                                    uint32_t log_n, uint32_t m1, uint32_t m2,
+                                                                    uint32_t *wlo, uint32_t *t1, uint32_t *t2) {
+    __shared__ qm31 tab[1u << kEvTabLog];
+    const uint32_t t = threadIdx.x;
+    const uint32_t b0 = blockIdx.x == 0 ? 0u : blockIdx.x == 1 ? kEvTabLog : kEvTabLog + m1;
+    const uint32_t k = blockIdx.x == 0 ? kEvTabLog : blockIdx.x == 1 ? m1 : m2;
+    uint32_t *out = blockIdx.x == 0 ? wlo : blockIdx.x == 1 ? t1 : t2;
+    if (t == 0) tab[0] = qm31{{1u, 0u, 0u, 0u}};
+    __syncthreads();
+    for (uint32_t j = 0; j < k; j++) {
+        const uint32_t l = log_n - 1 - (b0 + j);  // the factor of index bit b0 + j
+        const qm31 f{{factors[4 * l], factors[4 * l + 1], factors[4 * l + 2], factors[4 * l + 3]}};
+        for (uint32_t x = t; x < (1u << j); x += kEvTabThreads) tab[x + (1u << j)] = qmul(tab[x], f);
+        __syncthreads();
+    }
+    for (uint32_t x = t; x < (1u << k); x += kEvTabThreads)
+        for (int c = 0; c < 4; c++) out[4 * x + c] = tab[x].v[c];
+}
+
+__global__ void __launch_bounds__(kEvAccThreads) eval_accum_kernel(const uint32_t *__restrict__ coeffs,
+                                                                   const uint32_t *__restrict__ wlo,
+                                                                   const uint32_t *__restrict__ t1,
+                                                                   const uint32_t *__restrict__ t2, uint32_t m1,
+                                                                   uint64_t chunks, uint32_t *__restrict__ partial) {
+    __shared__ uint4 w[1u << kEvTabLog];
+    __shared__ qm31 red[kEvAccThreads / 32];
+    const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+    for (uint32_t x = t; x < (1u << kEvTabLog); x += kEvAccThreads) w[x] = __ldg((const uint4 *)wlo + x);
+    __syncthreads();
+    qm31 bacc{{0u, 0u, 0u, 0u}};
+    for (uint64_t hi = blockIdx.x; hi < chunks; hi += gridDim.x) {
+        const uint32_t *cp = coeffs + (hi << kEvTabLog);
+        uint32_t c[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) c[j] = __ldg(cp + t + kEvAccThreads * j);
+        // products < 2^62: four of them, or a reduced value and four, stay below 2^64
+        uint64_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            if (j == 4) { a0 = reduce64(a0); a1 = reduce64(a1); a2 = reduce64(a2); a3 = reduce64(a3); }
+            const uint4 q = w[t + kEvAccThreads * j];
+            a0 += (uint64_t)c[j] * q.x; a1 += (uint64_t)c[j] * q.y;
+            a2 += (uint64_t)c[j] * q.z; a3 += (uint64_t)c[j] * q.w;
+        }
+        qm31 v{{reduce64(a0), reduce64(a1), reduce64(a2), reduce64(a3)}};
+#pragma unroll
+        for (int m = 16; m > 0; m >>= 1) {
+            qm31 o;
+#pragma unroll
+            for (int k = 0; k < 4; k++) o.v[k] = __shfl_xor_sync(0xFFFFFFFFu, v.v[k], m);
+            v = qadd(v, o);
+        }
+        if (lane == 0) red[warp] = v;
+        __syncthreads();
+        if (t == 0) {
+            qm31 sum = red[0];
+            for (uint32_t k = 1; k < kEvAccThreads / 32; k++) sum = qadd(sum, red[k]);
+            const uint64_t i1 = hi & ((1ull << m1) - 1ull), i2 = hi >> m1;
+            const qm31 W = qmul(qm31{{t1[4 * i1], t1[4 * i1 + 1], t1[4 * i1 + 2], t1[4 * i1 + 3]}},
+                                qm31{{t2[4 * i2], t2[4 * i2 + 1], t2[4 * i2 + 2], t2[4 * i2 + 3]}});
+            bacc = qadd(bacc, qmul(sum, W));
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) partial[4ull * blockIdx.x + k] = bacc.v[k];
+    }
+}
+
 // Sum of `count` QM31 values (chunk values), or for n < 2^11 the direct sum
 // of c[i] w(i); one block, the total to out[0..4).
 __global__ void __launch_bounds__(kEvalThreads) eval_sum_kernel(const uint32_t *__restrict__ vals, uint64_t count,
@@ -429,9 +511,13 @@ void cuda_barycentric_eval(const uint32_t *evals, const uint32_t *weights, uint3
     cudaDeviceSynchronize();  // the reference's launcher returns with the sums in place
 }
 
+// Scratch as poly_ops.rs allocates it (2n words each).  log_n >= 12 with a
+// 16-byte-aligned d_scratch1: the low-bit table (2^13 words) in d_scratch1,
+// the high-bit tables and block sums (at most 12 n / 2^11 + 4 words) in
+// d_scratch2.  Smaller or unaligned: the chunk fold, which uses at most
+// 4 n / 2^11 + 4 words of d_scratch1.
 void cuda_eval_at_point(const uint32_t *d_coeffs, const uint32_t *d_folding_factors, uint32_t *h_result, uint32_t n,
                         uint32_t *d_scratch1, uint32_t *d_scratch2) {
-    (void)d_scratch2;
     if (n == 0 || (n & (n - 1u))) {
         set_last_error(VX_ERR_ARG, "cuda_eval_at_point: n = %u is not a power of two", n);
         return;
@@ -445,6 +531,21 @@ void cuda_eval_at_point(const uint32_t *d_coeffs, const uint32_t *d_folding_fact
     }
     if (log_n < kEvalChunkLog) {
         eval_sum_kernel<<<1, kEvalThreads>>>(nullptr, 0, d_coeffs, d_folding_factors, log_n, d_scratch1);
+    } else if (log_n > kEvTabLog && ((uintptr_t)d_scratch1 & 15u) == 0 && d_scratch2 != nullptr) {
+        const uint32_t H = log_n - kEvTabLog, m1 = H < 10u ? H : 10u, m2 = H - m1;
+        uint32_t *wlo = d_scratch1, *t1 = d_scratch2, *t2 = t1 + (4u << m1), *part = t2 + (4u << m2);
+        const uint64_t chunks = 1ull << H;
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) {
+            cudaGetLastError();
+            sms = 148;
+        }
+        const unsigned grid = (unsigned)(chunks < (uint64_t)sms * 6u ? chunks : (uint64_t)sms * 6u);
+        eval_tables_kernel<<<3, kEvTabThreads>>>(d_folding_factors, log_n, m1, m2, wlo, t1, t2);
+        eval_accum_kernel<<<grid, kEvAccThreads>>>(d_coeffs, wlo, t1, t2, m1, chunks, part);
+        eval_sum_kernel<<<1, kEvalThreads>>>(part, grid, nullptr, nullptr, 0, part + 4ull * grid);
+        d_scratch1 = part + 4ull * grid;  // where the value lands
     } else {
         const uint64_t chunks = 1ull << (log_n - kEvalChunkLog);
         if (((uintptr_t)d_coeffs & 15u) == 0)
