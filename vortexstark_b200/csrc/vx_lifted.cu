@@ -523,7 +523,7 @@ extern "C" int vx_lifted_create(uint32_t n_cols, const uint32_t *log_sizes, uint
         for (uint32_t j = 0; j < h->gcnt[g]; j++) {
             const uint32_t c = h->gfirst[g] + j, le = h->glog[g] + B;
             h->cols.col[c] = h->lde[g] + ((uint64_t)j << le);
-            h->cols.shift[c] = le == S ? 0u : S - le + 1u;
+            h->cols.shift[c] = S - le + 1u;  // 1 when le == S: the row is then the index itself
         }
     // constant tables and words
     GenTables gt;

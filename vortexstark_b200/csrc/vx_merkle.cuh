@@ -144,13 +144,13 @@ __device__ __forceinline__ void leaf_digest(const Src &src, uint64_t i, uint32_t
 constexpr uint32_t kMaxLiftCols = 64;
 struct LeafLifted {
     const uint32_t *col[kMaxLiftCols];
-    uint32_t shift[kMaxLiftCols];  // S - L + 1, or 0 when L = S
+    uint32_t shift[kMaxLiftCols];  // S - L + 1 (1 when L = S, where the formula gives the index itself)
     uint32_t n_cols;
     __device__ __forceinline__ void init() {}
+    // Row of column c for tree index idx < 2^S <= 2^31 (32-bit arithmetic).
     __device__ __forceinline__ uint32_t word(uint32_t c, uint64_t idx) const {
-        const uint32_t sh = shift[c];
-        const uint64_t row = sh ? (((idx >> sh) << 1) | (idx & 1ull)) : idx;
-        return __ldg(col[c] + row);
+        const uint32_t i = (uint32_t)idx, sh = shift[c];
+        return __ldg(col[c] + (((i >> sh) << 1) | (i & 1u)));
     }
     __device__ __forceinline__ void digest(uint64_t idx, uint32_t h[8], uint32_t one = 1u) const {
         blake2s_init(h);
