@@ -123,13 +123,19 @@ struct LeafCombine {
     __device__ __forceinline__ uint32_t load(uint64_t i, uint32_t m[16]) const {
         uint64_t s0 = 0, s1 = 0, s2 = 0, s3 = 0;
         const uint32_t nc = cols.n_cols;
-        for (uint32_t c = 0; c < nc; c++) {
+        auto mac = [&](uint32_t c) {
             const uint32_t v = cols.word(c, i);
             const uint4 p = __ldg((const uint4 *)pw + c);
             s0 += (uint64_t)p.x * v; s1 += (uint64_t)p.y * v;
             s2 += (uint64_t)p.z * v; s3 += (uint64_t)p.w * v;
-            if (c % 3u == 2u) { s0 = fold64(s0); s1 = fold64(s1); s2 = fold64(s2); s3 = fold64(s3); }
+        };
+        // three products (< 2^62 each) on a folded sum (< 2^34) stay below 2^64
+        uint32_t c = 0;
+        for (; c + 3u <= nc; c += 3u) {
+            mac(c); mac(c + 1u); mac(c + 2u);
+            s0 = fold64(s0); s1 = fold64(s1); s2 = fold64(s2); s3 = fold64(s3);
         }
+        for (; c < nc; c++) mac(c);  // at most two more
         s0 = fold64(s0); s1 = fold64(s1); s2 = fold64(s2); s3 = fold64(s3);
         const uint32_t a0 = reduce34(s0), a1 = reduce34(s1), a2 = reduce34(s2), a3 = reduce34(s3);
         o0[i] = a0; o1[i] = a1; o2[i] = a2; o3[i] = a3;
