@@ -147,10 +147,11 @@ __global__ void __launch_bounds__(256) pack_leaves_kernel(const uint32_t *const 
 // level l combines v[t] + f_l v[t + half], l = 0 at the top index bit.  The
 // result is linear in the coefficients: sum_i c[i] w(i), w(i) the product of
 // f_(log_n - 1 - b) over the set bits b of i, so any grouping gives the same
-// field value.  Here a block folds a contiguous chunk of 2^11 coefficients
+// field value.  For n = 2^11 (and when the first scratch buffer is not
+// 16-byte aligned) a block folds a contiguous chunk of 2^11 coefficients
 // (8 per thread in registers, then 8 levels in shared memory), scales the
 // chunk's value by the factors of its high index bits, and a second kernel
-// adds the chunk values.
+// adds the chunk values.  Larger n take the table-driven form below.
 constexpr uint32_t kEvalChunkLog = 11, kEvalThreads = 256;
 __device__ __forceinline__ qm31 qscale(qm31 f, uint32_t m) { return qmulm(f, m); }
 
