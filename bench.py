@@ -300,9 +300,11 @@ def ntt_microbench(peak_gbs: float, sizes=(20, 24, 28), reps: int = 5):
     calls; the reference's own kernels compiled for sm_100a are timed the same
     way when they are built.  Algorithmic bytes: 8 per element (one read, one
     write)."""
+    import ctypes as C
+
     import torch
 
-    from vortexstark_b200 import ntt
+    from vortexstark_b200 import _lib, ntt
     from vortexstark_b200.circle import Coset
     from vortexstark_b200.workload import m31_array
 
@@ -335,6 +337,54 @@ def ntt_microbench(peak_gbs: float, sizes=(20, 24, 28), reps: int = 5):
         out[f"2^{k}"] = res
         del d, cache
         torch.cuda.empty_cache()
+    # batched (ntt.rs:191-281 as the reference's default `forge-ntt-batch` build calls it: the _forge
+    # symbols with a host array of column pointers): the batched commitment's largest size group,
+    # 10 columns of 2^22
+    k, ncol = 22, 10
+    n = 1 << k
+    cache = ntt.TwiddleCache(Coset.half_coset(k))
+    cols = [torch.from_numpy(m31_array(SEED + 50 + c, n).view("int32")).cuda() for c in range(ncol)]
+    ptrs = (C.c_void_p * ncol)(*[c.data_ptr() for c in cols])
+    host_u32 = lambda v: (C.c_uint32 * max(len(v), 1))(*v)
+    libs = {"vortex": _lib.lib()}
+    try:
+        from oracle import oracle as O
+
+        if O.ref_available():
+            R = O.ref_lib()
+            for name in ("cuda_circle_ntt_evaluate_batch_forge", "cuda_circle_ntt_interpolate_batch_forge"):
+                getattr(R, name).argtypes = _lib._SIGS[name]
+            libs["reference_kernels"] = R
+    except Exception:
+        pass
+    res, outs = {}, {}
+    for name, Lx in libs.items():
+        def ev(Lx=Lx):
+            Lx.cuda_circle_ntt_evaluate_batch_forge(ptrs, cache.d_twiddles.data_ptr(),
+                                              cache.d_circle_twids.data_ptr(), host_u32(cache.layer_offsets),
+                                              host_u32(cache.layer_sizes), k - 1, n, ncol)
+
+        def it(Lx=Lx):
+            Lx.cuda_circle_ntt_interpolate_batch_forge(ptrs, cache.d_itwiddles.data_ptr(),
+                                                 cache.d_circle_itwids.data_ptr(), host_u32(cache.layer_offsets),
+                                                 host_u32(cache.layer_sizes), k - 1, n, ncol)
+        ev()
+        outs[name] = hash(b"".join(bytes(c.cpu().numpy().tobytes()) for c in cols))
+        it()
+        for op, fn in (("evaluate", ev), ("interpolate", it)):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(ds)
+            for _ in range(reps):
+                fn()
+            e1.record(ds)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            res[f"{op}_{name}"] = {"ms": ms, "gbs": 8 * n * ncol / (ms / 1e3) / 1e9,
+                                   "frac": 8 * n * ncol / (ms / 1e3) / 1e9 / peak_gbs}
+    res["values_equal"] = len(set(outs.values())) == 1
+    out[f"batch_{ncol}x2^{k}"] = res
+    del cols, ptrs, cache
+    torch.cuda.empty_cache()
     return out
 
 

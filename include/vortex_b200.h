@@ -58,6 +58,22 @@ void cuda_circle_ntt_interpolate_batch(uint32_t **d_columns, const uint32_t *d_i
                                        const uint32_t *d_circle_itwids, const uint32_t *h_layer_offsets,
                                        const uint32_t *h_layer_sizes, uint32_t n_line_layers, uint32_t n,
                                        uint32_t n_cols);
+/* replaces cuda_circle_ntt_evaluate_batch_forge / _interpolate_batch_forge, circle_ntt_batch_forge.cu:26-185
+ * (ntt.rs:191-281 with the default `forge-ntt-batch` feature): the same transforms with col_ptrs a HOST
+ * array of device column pointers; synchronous */
+void cuda_circle_ntt_evaluate_batch_forge(uint32_t *const *col_ptrs, const uint32_t *d_twiddles,
+                                          const uint32_t *d_circle_twids, const uint32_t *h_layer_offsets,
+                                          const uint32_t *h_layer_sizes, uint32_t n_line_layers, uint32_t n,
+                                          uint32_t n_cols);
+void cuda_circle_ntt_interpolate_batch_forge(uint32_t *const *col_ptrs, const uint32_t *d_itwiddles,
+                                             const uint32_t *d_circle_itwids, const uint32_t *h_layer_offsets,
+                                             const uint32_t *h_layer_sizes, uint32_t n_line_layers, uint32_t n,
+                                             uint32_t n_cols);
+/* replaces cuda_circle_ntt_layer_forge (ffi.rs:395-398): the layer of cuda_circle_ntt_layer */
+void cuda_circle_ntt_layer_forge(uint32_t *d_data, const uint32_t *d_twiddles, uint32_t layer_idx, uint32_t n,
+                                 int forward);
+/* replaces cuda_batch_inverse_m31_forge, batch_inverse_forge.cu:1-20: the chunk-of-64 batch inverse */
+void cuda_batch_inverse_m31_forge(const uint32_t *input, uint32_t *output, uint32_t n);
 /* replaces cuda_circle_ntt_layer, circle_ntt.cu:408-420 */
 void cuda_circle_ntt_layer(uint32_t *d_data, const uint32_t *d_twiddles, uint32_t layer_idx, uint32_t n, int forward);
 /* replaces cuda_bit_reverse_m31, circle_ntt.cu:422-427 */

@@ -418,3 +418,37 @@ def test_fri_chain_matches_oracle(oracle, L):
         assert np.array_equal(np.array(last, np.uint32), want_last)
     assert ch.launches() >= L
     ch.close()
+
+
+def test_forge_forms_match_plain(oracle, L):
+    """The forge-feature symbols of ntt.rs / blake2s_m31.rs: batched NTT with a host pointer array, the
+    single layer and the batch inverse give the plain forms' words."""
+    from vortexstark_b200 import ntt
+    from vortexstark_b200.circle import Coset
+    k, ncol = 12, 3
+    n = 1 << k
+    cache = ntt.TwiddleCache(Coset.half_coset(k))
+    cols = [m31_array(500 + c, n) for c in range(ncol)]
+    d1, d2 = [to_dev(c) for c in cols], [to_dev(c) for c in cols]
+    ntt.evaluate_batch(d1, cache)
+    hp = (C.c_void_p * ncol)(*[d.data_ptr() for d in d2])
+    off = (C.c_uint32 * len(cache.layer_offsets))(*cache.layer_offsets)
+    sz = (C.c_uint32 * len(cache.layer_sizes))(*cache.layer_sizes)
+    L.cuda_circle_ntt_evaluate_batch_forge(hp, cache.d_twiddles.data_ptr(), cache.d_circle_twids.data_ptr(), off, sz,
+                                           k - 1, n, ncol)
+    for a, b in zip(d1, d2):
+        assert np.array_equal(to_host(a, n), to_host(b, n))
+    L.cuda_circle_ntt_interpolate_batch_forge(hp, cache.d_itwiddles.data_ptr(), cache.d_circle_itwids.data_ptr(), off,
+                                              sz, k - 1, n, ncol)
+    for c, b in zip(cols, d2):
+        assert np.array_equal(to_host(b, n), c)
+    x1, x2 = to_dev(cols[0]), to_dev(cols[0])
+    tw = cache.d_twiddles.data_ptr() + 4 * cache.layer_offsets[2]
+    L.cuda_circle_ntt_layer(x1.data_ptr(), tw, 3, n, 1)
+    L.cuda_circle_ntt_layer_forge(x2.data_ptr(), tw, 3, n, 1)
+    assert np.array_equal(to_host(x1, n), to_host(x2, n))
+    z = m31_array(77, 1000)
+    z[::50] = 0
+    dz, oz = to_dev(z), empty(1000)
+    L.cuda_batch_inverse_m31_forge(dz.data_ptr(), oz.data_ptr(), 1000)
+    assert np.array_equal(to_host(oz, 1000), oracle.batch_inverse(z))

@@ -27,6 +27,10 @@ _SIGS = {
     "cuda_circle_ntt_interpolate": [vp, vp, vp, vp, vp, u32, u32],
     "cuda_circle_ntt_evaluate_batch": [vp, vp, vp, vp, vp, u32, u32, u32],
     "cuda_circle_ntt_interpolate_batch": [vp, vp, vp, vp, vp, u32, u32, u32],
+    "cuda_circle_ntt_evaluate_batch_forge": [vp, vp, vp, vp, vp, u32, u32, u32],
+    "cuda_circle_ntt_interpolate_batch_forge": [vp, vp, vp, vp, vp, u32, u32, u32],
+    "cuda_circle_ntt_layer_forge": [vp, vp, u32, u32, C.c_int],
+    "cuda_batch_inverse_m31_forge": [vp, vp, u32],
     "cuda_circle_ntt_layer": [vp, vp, u32, u32, C.c_int],
     "cuda_bit_reverse_m31": [vp, u32],
     "cuda_permute_hc_to_canonic_brt": [vp, vp, u32, u32],

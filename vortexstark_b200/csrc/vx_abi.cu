@@ -10,6 +10,8 @@
 #include <cstring>
 #include <string>
 
+#include <mutex>
+
 #include "vx_common.cuh"
 #include "vx_field.cuh"
 #include "vx_merkle.cuh"
@@ -598,9 +600,76 @@ void cuda_circle_ntt_interpolate_batch(uint32_t **cols, const uint32_t *itw, con
     cudaDeviceSynchronize();
 }
 
+// The forge-feature forms (ntt.rs:191-281 with `forge-ntt-batch`, on by
+// default in the reference's Cargo features): the same transforms, with
+// the column pointers as a HOST array (circle_ntt_batch_forge.cu:26-39
+// copies them to the device per call).  They go to a per-device device
+// array kept across calls; the call is synchronous, so the lock covers its
+// use.
+namespace {
+std::mutex g_forge_cols_mu;
+uint32_t **g_forge_cols[64] = {nullptr};
+uint32_t g_forge_cols_cap[64] = {0};
+
+int forge_batch(bool fwd, uint32_t *const *col_ptrs, const uint32_t *tw, const uint32_t *ctw, const uint32_t *h_off,
+                const uint32_t *h_sizes, uint32_t n_line, uint32_t n, uint32_t n_cols, const char *who) {
+    if (n_cols == 0) return VX_OK;
+    if (col_ptrs == nullptr) {
+        set_last_error(VX_ERR_ARG, "%s: null column pointer array", who);
+        return VX_ERR_ARG;
+    }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) {
+        set_last_error(VX_ERR_ARG, "%s: device %d out of range", who, dev);
+        return VX_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lk(g_forge_cols_mu);
+    if (g_forge_cols_cap[dev] < n_cols) {
+        if (g_forge_cols[dev]) cudaFree(g_forge_cols[dev]);
+        g_forge_cols[dev] = nullptr;
+        g_forge_cols_cap[dev] = 0;
+        if (cudaMalloc(&g_forge_cols[dev], sizeof(uint32_t *) * n_cols) != cudaSuccess) {
+            cudaGetLastError();
+            set_last_error(VX_ERR_OOM, "%s: cannot allocate the column pointer array", who);
+            return VX_ERR_OOM;
+        }
+        g_forge_cols_cap[dev] = n_cols;
+    }
+    if (cudaMemcpy(g_forge_cols[dev], col_ptrs, sizeof(uint32_t *) * n_cols, cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaGetLastError();
+        set_last_error(VX_ERR_CUDA, "%s: pointer upload failed", who);
+        return VX_ERR_CUDA;
+    }
+    if (fwd)
+        cuda_circle_ntt_evaluate_batch(g_forge_cols[dev], tw, ctw, h_off, h_sizes, n_line, n, n_cols);
+    else
+        cuda_circle_ntt_interpolate_batch(g_forge_cols[dev], tw, ctw, h_off, h_sizes, n_line, n, n_cols);
+    return VX_OK;
+}
+}  // namespace
+
+void cuda_circle_ntt_evaluate_batch_forge(uint32_t *const *col_ptrs, const uint32_t *tw, const uint32_t *ctw,
+                                          const uint32_t *h_off, const uint32_t *h_sizes, uint32_t n_line, uint32_t n,
+                                          uint32_t n_cols) {
+    forge_batch(true, col_ptrs, tw, ctw, h_off, h_sizes, n_line, n, n_cols, "cuda_circle_ntt_evaluate_batch_forge");
+}
+
+void cuda_circle_ntt_interpolate_batch_forge(uint32_t *const *col_ptrs, const uint32_t *itw, const uint32_t *ictw,
+                                             const uint32_t *h_off, const uint32_t *h_sizes, uint32_t n_line,
+                                             uint32_t n, uint32_t n_cols) {
+    forge_batch(false, col_ptrs, itw, ictw, h_off, h_sizes, n_line, n, n_cols,
+                "cuda_circle_ntt_interpolate_batch_forge");
+}
+
 void cuda_circle_ntt_layer(uint32_t *d, const uint32_t *tw, uint32_t layer_idx, uint32_t n, int forward) {
     ntt_single_layer(d, tw, layer_idx, log2_exact(n), forward != 0, 0);
     VX_LAUNCH_CHECK();
+}
+
+// circle_ntt_layer_forge (blake2s_m31.rs): the same layer.
+void cuda_circle_ntt_layer_forge(uint32_t *d, const uint32_t *tw, uint32_t layer_idx, uint32_t n, int forward) {
+    cuda_circle_ntt_layer(d, tw, layer_idx, n, forward);
 }
 
 void cuda_bit_reverse_m31(uint32_t *data, uint32_t log_n) {
@@ -652,6 +721,9 @@ void cuda_batch_inverse_m31(const uint32_t *in, uint32_t *out, uint32_t n) {
     cudaError_t e = batch_inverse(in, out, n, 0);
     if (e != cudaSuccess) set_last_error(VX_ERR_CUDA, "cuda_batch_inverse_m31: %s", cudaGetErrorString(e));
 }
+
+// batch_inverse_forge.cu:1-20: the same chunk-of-64 prefix-product inverse.
+void cuda_batch_inverse_m31_forge(const uint32_t *in, uint32_t *out, uint32_t n) { cuda_batch_inverse_m31(in, out, n); }
 
 void cuda_batch_inverse_m31_stream(const uint32_t *in, uint32_t *out, uint32_t n, void *stream) {
     cudaError_t e = batch_inverse(in, out, n, (cudaStream_t)stream);
