@@ -34,6 +34,8 @@ def lib():
         L = C.CDLL(_LIB_PATH)
         L.vxo_prove.argtypes = [C.c_uint32] * 5 + [C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(C.c_size_t)]
         L.vxo_prove.restype = C.c_int
+        L.vxo_prove_lean.argtypes = [C.c_uint32] * 5 + [C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(C.c_size_t)]
+        L.vxo_prove_lean.restype = C.c_int
         L.vxo_verify.argtypes = [C.POINTER(C.c_uint8), C.c_size_t, C.c_uint32, C.c_uint32, C.c_char_p, C.c_size_t]
         L.vxo_verify.restype = C.c_int
         L.vxo_proof_size.argtypes = [C.c_uint32] * 3
@@ -129,6 +131,22 @@ def prove(a: int, b: int, log_n: int, blowup_bits: int = 2, n_queries: int = 80)
     rc = L.vxo_prove(a, b, log_n, blowup_bits, n_queries, C.byref(out), C.byref(n))
     if rc:
         raise ValueError(f"oracle prove rejected its arguments (rc={rc})")
+    try:
+        return C.string_at(out, n.value)
+    finally:
+        L.vxo_free(out)
+
+
+def prove_lean(a: int, b: int, log_n: int, blowup_bits: int = 2, n_queries: int = 80) -> bytes:
+    """The same bytes as ``prove`` in bounded host memory (for 2^30- and
+    2^31-point proofs): the quotient is recomputed where it is read and
+    trees keep their levels from height 8 up."""
+    L = lib()
+    out = C.POINTER(C.c_uint8)()
+    n = C.c_size_t()
+    rc = L.vxo_prove_lean(a, b, log_n, blowup_bits, n_queries, C.byref(out), C.byref(n))
+    if rc:
+        raise ValueError(f"oracle prove_lean failed (rc={rc})")
     try:
         return C.string_at(out, n.value)
     finally:

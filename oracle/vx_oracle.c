@@ -644,6 +644,220 @@ static int prove_impl(uint32_t a, uint32_t b, uint32_t log_n, uint32_t B, uint32
 int vxo_prove(uint32_t a, uint32_t b, uint32_t log_n, uint32_t B, uint32_t nq, uint8_t **out, size_t *out_len) {
     return prove_impl(a, b, log_n, B, nq, out, out_len, NULL);
 }
+
+/* ------------------------------------------------------------------ */
+/* the same proof in bounded host memory (for 2^30- and 2^31-point     */
+/* proofs): prover.rs:264-619 computes the same values; only what is    */
+/* kept in memory differs.                                              */
+/*  - The quotient q = alpha (t[i+2] - t[i+1] - t[i]) is never stored:  */
+/*    its leaves, its circle fold and its openings recompute it from    */
+/*    the evaluation (constraint.cu:10-64; prover.rs:1522-1530 does the */
+/*    same on the host).                                                */
+/*  - A tree keeps its levels from height K up; an authentication path */
+/*    re-hashes the 2^K-leaf subtree of its leaf (merkle.rs:455-497     */
+/*    reads the same siblings from a full tree).                        */
+/* At log_n = 30 / blowup 1 the peak is the evaluation (8 GiB), the FRI */
+/* layers (32 GiB) and the fold twiddles (4 GiB).                       */
+/* ------------------------------------------------------------------ */
+enum { LSRC_TRACE = 0, LSRC_QUOT = 1, LSRC_COLS4 = 2 };
+typedef struct {
+    int kind;
+    const uint32_t *t;        /* trace evaluation (TRACE, QUOT) */
+    uint64_t n;               /* leaves */
+    uint32_t alpha[4];        /* QUOT */
+    const uint32_t *c[4];     /* COLS4 */
+} lsrc;
+
+static inline uint32_t quot_c(const uint32_t *t, uint64_t n, uint64_t i) {
+    return m_sub(t[(i + 2) % n], m_add(t[(i + 1) % n], t[i]));
+}
+static inline uint32_t lsrc_words(const lsrc *s, uint64_t i, uint32_t w[4]) {
+    switch (s->kind) {
+    case LSRC_TRACE: w[0] = s->t[i]; return 1;
+    case LSRC_QUOT: {
+        uint32_t c = quot_c(s->t, s->n, i);
+        for (int k = 0; k < 4; k++) w[k] = m_mul(s->alpha[k], c);
+        return 4;
+    }
+    default:
+        for (int k = 0; k < 4; k++) w[k] = s->c[k][i];
+        return 4;
+    }
+}
+
+typedef struct { uint32_t log_n, K; uint32_t **levels; lsrc src; } ltree;
+
+/* 2^K leaves of subtree j hashed and reduced in place; levels (if non-NULL)
+ * receives every level of the subtree, leaves first (2^(K+1) - 1 hashes). */
+static void lsub(const lsrc *s, uint32_t K, uint64_t j, uint32_t *levels, uint32_t out[8]) {
+    uint64_t m = 1ull << K;
+    uint32_t *buf = levels ? levels : (uint32_t *)malloc(m * 32);
+    for (uint64_t i = 0; i < m; i++) {
+        uint32_t w[4];
+        uint32_t nw = lsrc_words(s, (j << K) + i, w);
+        hash_words16(w, nw, buf + 8 * i);
+    }
+    uint32_t *dn = buf;
+    for (uint32_t l = 1; l <= K; l++) {
+        uint64_t cnt = m >> l;
+        uint32_t *up = levels ? dn + 8 * (cnt * 2) : buf;
+        for (uint64_t i = 0; i < cnt; i++) vxo_hash_pair(dn + 16 * i, dn + 16 * i + 8, up + 8 * i);
+        dn = up;
+    }
+    memcpy(out, dn, 32);
+    if (!levels) free(buf);
+}
+
+static void ltree_build(ltree *t, const lsrc *s, uint32_t log_n) {
+    t->log_n = log_n;
+    t->K = log_n < 8 ? log_n : 8;
+    t->src = *s;
+    t->levels = (uint32_t **)calloc(log_n + 1, sizeof(uint32_t *));
+    uint64_t nk = 1ull << (log_n - t->K);
+    uint32_t *lk = (uint32_t *)malloc(nk * 32);
+    #pragma omp parallel for schedule(static)
+    for (int64_t j = 0; j < (int64_t)nk; j++) lsub(&t->src, t->K, (uint64_t)j, NULL, lk + 8 * j);
+    t->levels[t->K] = lk;
+    for (uint32_t l = t->K + 1; l <= log_n; l++) {
+        uint64_t m = 1ull << (log_n - l);
+        uint32_t *up = (uint32_t *)malloc(m * 32), *dn = t->levels[l - 1];
+        #pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < (int64_t)m; i++) vxo_hash_pair(dn + 16 * i, dn + 16 * i + 8, up + 8 * i);
+        t->levels[l] = up;
+    }
+}
+static void ltree_free(ltree *t) {
+    if (!t->levels) return;
+    for (uint32_t l = t->K; l <= t->log_n; l++) free(t->levels[l]);
+    free(t->levels); t->levels = NULL;
+}
+static void ltree_path(const ltree *t, uint64_t idx, uint32_t *out) {
+    uint32_t K = t->K;
+    uint64_t m = 1ull << K;
+    uint32_t *sub = (uint32_t *)malloc((2 * m) * 32), root[8];
+    lsub(&t->src, K, idx >> K, sub, root);
+    uint64_t off = 0, cnt = m, li = idx & (m - 1);
+    for (uint32_t l = 0; l < K; l++) {
+        memcpy(out + 8 * l, sub + 8 * (off + (li ^ 1)), 32);
+        off += cnt; cnt >>= 1; li >>= 1;
+    }
+    uint64_t hi = idx >> K;
+    for (uint32_t l = K; l < t->log_n; l++) {
+        memcpy(out + 8 * l, t->levels[l] + 8 * (hi ^ 1), 32);
+        hi >>= 1;
+    }
+    free(sub);
+}
+static void write_ldecom(wbuf *w, const ltree *t, const uint64_t *idx, uint32_t nq) {
+    uint32_t v[4];
+    wr(w, nq);
+    for (int s = 0; s < 2; s++)
+        for (uint32_t q = 0; q < nq; q++) {
+            uint32_t nw = lsrc_words(&t->src, idx[q] ^ (uint64_t)s, v);
+            wrs(w, v, nw);
+        }
+    uint32_t *path = (uint32_t *)malloc(((size_t)t->log_n + 1) * 32);
+    for (int s = 0; s < 2; s++)
+        for (uint32_t q = 0; q < nq; q++) {
+            ltree_path(t, idx[q] ^ (uint64_t)s, path);
+            wr(w, t->log_n);
+            wrs(w, path, 8 * (size_t)t->log_n);
+        }
+    free(path);
+}
+
+int vxo_prove_lean(uint32_t a, uint32_t b, uint32_t log_n, uint32_t B, uint32_t nq, uint8_t **out, size_t *out_len) {
+    if (log_n < 4 || log_n + B > 31 || a >= P || b >= P || !out || !out_len) return 1;
+    uint32_t le = log_n + B;
+    uint64_t N = 1ull << le;
+    uint32_t *eval = (uint32_t *)calloc(N, 4);
+    if (!eval) return 2;
+    vxo_fibonacci_trace(a, b, log_n, eval);
+    vxo_coset tdom = vxo_coset_half_coset(log_n);
+    vxo_interpolate_on(eval, &tdom);
+    vxo_coset edom = eval_domain(le);
+    vxo_evaluate_on(eval, &edom);
+    lsrc ts = {LSRC_TRACE, eval, N, {0, 0, 0, 0}, {NULL, NULL, NULL, NULL}};
+    ltree ttree;
+    ltree_build(&ttree, &ts, le);
+    uint32_t troot[8]; memcpy(troot, ttree.levels[le], 32);
+    vxo_channel ch; vxo_channel_init(&ch);
+    vxo_channel_mix_digest(&ch, troot);
+    lsrc qs = {LSRC_QUOT, eval, N, {0, 0, 0, 0}, {NULL, NULL, NULL, NULL}};
+    vxo_channel_draw_felt(&ch, qs.alpha);
+    ltree qtree;
+    ltree_build(&qtree, &qs, le);
+    uint32_t qroot[8]; memcpy(qroot, qtree.levels[le], 32);
+    vxo_channel_mix_digest(&ch, qroot);
+    uint32_t nfri = le - 3;
+    uint32_t **lay = (uint32_t **)calloc((size_t)nfri * 4, sizeof(uint32_t *));
+    ltree *ftree = (ltree *)calloc(nfri, sizeof(ltree));
+    uint32_t *froots = (uint32_t *)malloc((size_t)nfri * 32);
+    uint32_t fa[4]; vxo_channel_draw_felt(&ch, fa);
+    uint32_t fa2[4]; vxo_qm31_mul(fa, fa, fa2);
+    uint32_t *tw = (uint32_t *)malloc((N / 2) * 4);
+    vxo_fold_twiddles(&edom, 1, tw);
+    for (int c = 0; c < 4; c++) lay[c] = (uint32_t *)malloc((N / 2) * 4);
+    {   /* circle fold of the recomputed quotient into a zero accumulator (fri.rs:163-191) */
+        qm al, al2; memcpy(al.v, fa, 16); memcpy(al2.v, fa2, 16);
+        #pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < (int64_t)(N / 2); i++) {
+            qm f0 = {{0, 0, 0, 0}}, f1 = {{0, 0, 0, 0}}, prev = {{0, 0, 0, 0}};
+            lsrc_words(&qs, 2 * (uint64_t)i, f0.v);
+            lsrc_words(&qs, 2 * (uint64_t)i + 1, f1.v);
+            qm fp = q_add(q_add(f0, f1), q_mul(al, q_mulm(q_sub(f0, f1), tw[i])));
+            qm r = q_add(q_mul(prev, al2), fp);
+            for (int c = 0; c < 4; c++) lay[c][i] = r.v[c];
+        }
+    }
+    uint32_t cur = le - 1;
+    lsrc fs = {LSRC_COLS4, NULL, 1ull << cur, {0, 0, 0, 0}, {lay[0], lay[1], lay[2], lay[3]}};
+    ltree_build(&ftree[0], &fs, cur);
+    memcpy(froots, ftree[0].levels[cur], 32);
+    vxo_channel_mix_digest(&ch, froots);
+    for (uint32_t k = 1; k < nfri; k++) {
+        uint32_t al[4]; vxo_channel_draw_felt(&ch, al);
+        vxo_coset dom = vxo_coset_half_odds(cur);
+        uint64_t half = 1ull << (cur - 1);
+        vxo_fold_twiddles(&dom, 0, tw);
+        for (int c = 0; c < 4; c++) lay[4 * k + c] = (uint32_t *)malloc(half * 4);
+        vxo_fold_line((const uint32_t *const *)(lay + 4 * (k - 1)), tw, al, lay + 4 * k, half);
+        cur--;
+        lsrc ks = {LSRC_COLS4, NULL, 1ull << cur, {0, 0, 0, 0},
+                   {lay[4 * k], lay[4 * k + 1], lay[4 * k + 2], lay[4 * k + 3]}};
+        ltree_build(&ftree[k], &ks, cur);
+        memcpy(froots + 8 * k, ftree[k].levels[cur], 32);
+        vxo_channel_mix_digest(&ch, froots + 8 * k);
+    }
+    free(tw);
+    uint32_t last[32];
+    for (int i = 0; i < 8; i++) for (int c = 0; c < 4; c++) last[4 * i + c] = lay[4 * (nfri - 1) + c][i];
+    vxo_channel_mix_felts(&ch, last, 8);
+    uint64_t *qi = (uint64_t *)malloc(sizeof(uint64_t) * (nq ? nq : 1));
+    for (uint32_t j = 0; j < nq; j++) qi[j] = vxo_channel_draw_number(&ch, N);
+    wbuf w = {NULL, 0, 0};
+    w.cap = vxo_proof_size(log_n, B, nq); w.p = (uint8_t *)malloc(w.cap);
+    wr(&w, 0x4B52414Bu); wr(&w, 1); wr(&w, log_n); wr(&w, a); wr(&w, b);
+    wrs(&w, troot, 8); wrs(&w, qroot, 8);
+    wr(&w, nfri); wrs(&w, froots, 8 * (size_t)nfri);
+    wr(&w, 8); wrs(&w, last, 32);
+    wr(&w, nq); for (uint32_t j = 0; j < nq; j++) wr(&w, (uint32_t)qi[j]);
+    write_ldecom(&w, &ttree, qi, nq);
+    write_ldecom(&w, &qtree, qi, nq);
+    wr(&w, nfri);
+    uint64_t *fi = (uint64_t *)malloc(sizeof(uint64_t) * (nq ? nq : 1));
+    for (uint32_t j = 0; j < nq; j++) fi[j] = qi[j] >> 1;
+    for (uint32_t k = 0; k < nfri; k++) {
+        write_ldecom(&w, &ftree[k], fi, nq);
+        for (uint32_t j = 0; j < nq; j++) fi[j] >>= 1;
+    }
+    free(fi); free(qi);
+    *out = w.p; *out_len = w.n;
+    for (uint32_t k = 0; k < nfri; k++) { ltree_free(&ftree[k]); for (int c = 0; c < 4; c++) free(lay[4 * k + c]); }
+    free(ftree); free(lay); free(froots);
+    ltree_free(&qtree); ltree_free(&ttree); free(eval);
+    return 0;
+}
 int vxo_prove_roots(uint32_t a, uint32_t b, uint32_t log_n, uint32_t B,
                     uint32_t *tr, uint32_t *qr, uint32_t *fr) {
     uint32_t le = log_n + B;

@@ -124,6 +124,12 @@ void vxo_channel_draw_query_indices(vxo_channel *ch, uint32_t log_domain, uint32
  * frees *out with vxo_free.  Returns 0 on success. */
 int vxo_prove(uint32_t a, uint32_t b, uint32_t log_n, uint32_t blowup_bits, uint32_t n_queries,
               uint8_t **out, size_t *out_len);
+/* The same proof bytes as vxo_prove in bounded host memory: the quotient is
+ * recomputed where it is read, trees keep levels from height 8 up and
+ * re-hash a 256-leaf subtree per authentication path.  For the 2^30- and
+ * 2^31-point proofs (log_n = 28 / blowup 2, log_n = 30 / blowup 1). */
+int vxo_prove_lean(uint32_t a, uint32_t b, uint32_t log_n, uint32_t blowup_bits, uint32_t n_queries,
+                   uint8_t **out, size_t *out_len);
 /* Proof size in bytes for (log_n, blowup_bits, n_queries). */
 size_t vxo_proof_size(uint32_t log_n, uint32_t blowup_bits, uint32_t n_queries);
 /* verifier.rs:39-310 on the byte layout; returns 0 if accepted, else a

@@ -109,6 +109,28 @@ def test_oracle_verifier_accepts(oracle, log_n):
         assert oracle.verify(blob) == (0, "")
 
 
+@pytest.mark.parametrize("log_n,blowup", [(4, 1), (5, 3), (7, 2), (8, 1), (10, 2), (13, 3), (16, 2)])
+def test_lean_prove_equals_full_prove(oracle, log_n, blowup):
+    """The memory-lean prove (recomputed quotient, trees stored from height
+    8 up) that generates the largest proofs' fixtures gives the same bytes as
+    the full prove, below and above the stored height."""
+    for a, b in [(1, 1), (123456789, 987654321)]:
+        assert oracle.prove_lean(a, b, log_n, blowup) == oracle.prove(a, b, log_n, blowup)
+
+
+def test_large_proof_fixtures(oracle):
+    """tests/golden/large_proofs.json holds the oracle's 2^30- and 2^31-point
+    proofs (log_n = 28 / blowup 2 and log_n = 30 / blowup 1) for the inputs
+    the GPU test proves."""
+    from vortexstark_b200.workload import fib_inputs
+
+    data = json.load(open(os.path.join(GOLDEN, "large_proofs.json")))
+    for log_n, blowup in [(28, 2), (30, 1)]:
+        e = data[f"{log_n}_{blowup}"]
+        assert (e["a"], e["b"]) == fib_inputs(9000 + log_n, 1)[0]
+        assert e["len"] == oracle.proof_size(log_n, blowup) and len(e["sha256"]) == 64
+
+
 def test_oracle_verifier_rejects_tampering(oracle):
     """verifier.rs:324-367 (trace / quotient / FRI values, commitments) plus
     random words of the decommitments.  Words 3 and 4 (the public inputs) are
