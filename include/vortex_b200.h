@@ -397,6 +397,19 @@ typedef struct {
 } vx_completion;
 int vx_server_create(size_t budget_bytes, uint32_t max_inflight, uint32_t blowup_bits, uint32_t n_queries,
                      int use_graphs, vx_server **out);
+/* Scheduling policy, before the first prewarm or submit (a slot's stream
+ * priority is fixed when the slot is created; VX_ERR_ARG afterwards).
+ * Proofs with at least 2^large_log_eval evaluation points are "large"; at
+ * most max_large of them are in flight at once (per size when
+ * large_per_size != 0).  priority: 0 puts small proofs on the
+ * highest-priority streams, 1 gives every slot the same priority, 2 puts
+ * large proofs on the highest-priority streams, 3 grades by size
+ * (2^(large_log_eval-2) .. 2^(large_log_eval-1) points in between, smaller
+ * ones highest, large ones lowest).  small_cap bounds the small proofs in
+ * flight while a large one is (0: no bound).  Defaults: 24, 1, 0, 0, 0.
+ * Proof bytes never depend on the policy. */
+int vx_server_set_policy(vx_server *s, uint32_t large_log_eval, uint32_t max_large, int priority,
+                         uint32_t small_cap, int large_per_size);
 /* Queue one request (non-blocking). */
 int vx_server_submit(vx_server *s, uint64_t tag, uint32_t log_n, uint32_t a, uint32_t b);
 /* Create up to `count` slots of this size ahead of time (counts against the budget). */
@@ -493,25 +506,28 @@ int vx_tune_set(uint32_t kind, uint32_t layers, uint32_t a, uint32_t b);
 /* Read the knob that launches on the current device use (b = 0 for kinds 1, 2). */
 int vx_tune_get(uint32_t kind, uint32_t layers, uint32_t *a, uint32_t *b);
 /* Host-only: the pass plan of a `total`-layer transform (4..31) for a bottom
- * pass of at most bottom_max (9..12) layers and upper passes of at most
- * upper_max (3..9); transforms of at most 12 layers are one pass.  Pass i applies layers [starts[i], starts[i] + layers[i])
- * on tiles of 2^tile_cols_log[i] contiguous columns (0 for the bottom pass). */
+ * pass of at most bottom_max (9..14) layers and upper passes of at most
+ * upper_max (3..12); transforms of at most max(12, bottom_max) layers are one
+ * pass.  Pass i applies layers [starts[i], starts[i] + layers[i]) on tiles of
+ * 2^tile_cols_log[i] contiguous columns (0 for the bottom pass). */
 int vx_ntt_plan(uint32_t total, uint32_t bottom_max, uint32_t upper_max, uint32_t starts[32], uint32_t layers[32],
                 uint32_t tile_cols_log[32], uint32_t *n_passes);
 
 /* Whole proof without any device allocation — no counterpart in the
- * reference.  For callers that may not allocate device memory: code inside a
- * stream capture or CUDA-graph construction, hosts whose device memory is
- * owned by another allocator (a Rust arena, a framework's caching pool), or
- * sandboxes that forbid cudaMalloc after start-up.  Same result as
+ * reference.  For callers that cannot call cudaMalloc: hosts whose device
+ * memory is owned by another allocator (a Rust arena, a framework's caching
+ * pool) and sandboxes that forbid cudaMalloc after start-up.  Same result as
  * vx_prove_fib, with every byte of device scratch in one fixed 8 MiB static
  * device array of this library (held on every GPU that loads it until the
  * process exits), so the size is limited to log_n + blowup_bits <= 14 and
  * n_queries <= 80; larger sizes are rejected with VX_ERR_ARG.  The first call
  * on a device looks up the array's device address and uploads constant
- * tables, so make it before any stream capture.  Runs on the legacy default
- * stream and returns when the proof is in `out`.  All calls share the array:
- * calls that overlap on the GPU (other host threads, other streams) race. */
+ * tables.  Every call is synchronous: it copies with cudaMemcpy, launches on
+ * the legacy default stream and returns when the proof is in `out`, so it
+ * must not be called while any stream capture is active in the process.
+ * All calls share the array and it keeps the last call's contents; calls
+ * that overlapped on the GPU would race on it, so a process-wide lock
+ * serialises them (each call blocks the others until its proof is back). */
 int vx_prove_fib_noalloc(uint32_t a, uint32_t b, uint32_t log_n, uint32_t blowup_bits, uint32_t n_queries,
                          uint8_t *out, size_t cap, size_t *out_len);
 
@@ -528,8 +544,10 @@ int vx_prove_fib_batch(const uint32_t *a, const uint32_t *b, uint32_t count, uin
                        uint32_t n_queries, uint8_t *out, size_t cap, size_t *proof_size);
 
 /* Free the slots cached by vx_prove_fib and vx_prove_fib_batch on every
- * device; a size's shared tables are freed with the last slot (of any
- * owner) that uses them. */
+ * device (a size's shared tables are freed with the last slot, of any
+ * owner, that uses them) and the column-pointer arrays the forge batch
+ * launchers keep per device.  After a cudaDeviceReset call this before the
+ * next call into the library. */
 void vx_release_all(void);
 
 #ifdef __cplusplus

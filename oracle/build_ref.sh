@@ -2,7 +2,8 @@
 # Recipe for oracle/_ref/libvxref.so — TEST INFRASTRUCTURE ONLY.
 #
 # Compiles the reference's own hot-path CUDA sources, read in place from
-# /root/reference/cuda (nothing is copied into this repository), for sm_100a
+# $VX_REFERENCE_ROOT/cuda (default /root/reference; nothing is copied into
+# this repository), for sm_100a
 # with the reference's default cargo features (forge-ntt, forge-ntt-batch,
 # forge-fri, forge-permute: build.rs:214-244), and links them with
 # ref_driver.cu (the prove_lean_inner orchestration restated over those

@@ -452,3 +452,48 @@ def test_forge_forms_match_plain(oracle, L):
     dz, oz = to_dev(z), empty(1000)
     L.cuda_batch_inverse_m31_forge(dz.data_ptr(), oz.data_ptr(), 1000)
     assert np.array_equal(to_host(oz, 1000), oracle.batch_inverse(z))
+
+
+@pytest.mark.parametrize("n_line", [0, 3, 8])
+def test_batched_ntt_partial_layer_count(oracle, L, n_line):
+    """A layer count below the full transform (circle_ntt.cu:314-404,
+    circle_ntt_batch_forge.cu:95-185): exactly n_line line layers and the
+    circle layer, then for the inverse the 2^-log_n scale, in both batched
+    forms (device pointer array and the forge host array)."""
+    from vortexstark_b200 import ntt
+    from vortexstark_b200.circle import Coset
+    k, ncol = 10, 3
+    n = 1 << k
+    cache = ntt.TwiddleCache(Coset.half_coset(k))
+    oline, ocirc, ooffs = oracle.twiddles(oracle.coset("half_coset", k), False)
+    iline, icirc, _ = oracle.twiddles(oracle.coset("half_coset", k), True)
+    cols = [m31_array(900 + c, n) for c in range(ncol)]
+    want_e = []
+    for x in cols:
+        for l in range(n_line - 1, -1, -1):
+            x = oracle.ntt_layer(x, oline[ooffs[l]:], l + 1, True)
+        want_e.append(oracle.ntt_layer(x, ocirc, 0, True))
+    want_i = []
+    for x in want_e:
+        x = oracle.ntt_layer(x, icirc, 0, False)
+        for l in range(n_line):
+            x = oracle.ntt_layer(x, iline[ooffs[l]:], l + 1, False)
+        e = (30 * k) % 31
+        want_i.append(np.array([(int(v) << e) % P for v in x], np.uint32))
+    off = (C.c_uint32 * len(cache.layer_offsets))(*cache.layer_offsets)
+    sz = (C.c_uint32 * len(cache.layer_sizes))(*cache.layer_sizes)
+    d1, d2 = [to_dev(c) for c in cols], [to_dev(c) for c in cols]
+    ptrs = ntt._ptr_array(d1)
+    hp = (C.c_void_p * ncol)(*[d.data_ptr() for d in d2])
+    L.cuda_circle_ntt_evaluate_batch(ptrs.data_ptr(), cache.d_twiddles.data_ptr(), cache.d_circle_twids.data_ptr(),
+                                     off, sz, n_line, n, ncol)
+    L.cuda_circle_ntt_evaluate_batch_forge(hp, cache.d_twiddles.data_ptr(), cache.d_circle_twids.data_ptr(), off, sz,
+                                           n_line, n, ncol)
+    for a, b, w in zip(d1, d2, want_e):
+        assert np.array_equal(to_host(a, n), w) and np.array_equal(to_host(b, n), w)
+    L.cuda_circle_ntt_interpolate_batch(ptrs.data_ptr(), cache.d_itwiddles.data_ptr(),
+                                        cache.d_circle_itwids.data_ptr(), off, sz, n_line, n, ncol)
+    L.cuda_circle_ntt_interpolate_batch_forge(hp, cache.d_itwiddles.data_ptr(), cache.d_circle_itwids.data_ptr(), off,
+                                              sz, n_line, n, ncol)
+    for a, b, w in zip(d1, d2, want_i):
+        assert np.array_equal(to_host(a, n), w) and np.array_equal(to_host(b, n), w)

@@ -63,3 +63,45 @@ def test_ntt_faster_than_reference_kernels(ref, log_n):
     print(f"\nNTT 2^{log_n}: evaluate {my_e:.3f} ms (reference kernels {ref_e:.3f} ms), "
           f"interpolate {my_i:.3f} ms (reference kernels {ref_i:.3f} ms)")
     assert my_e < ref_e and my_i < ref_i
+
+
+def _ref_ntt(ref, name):
+    from vortexstark_b200 import _lib
+
+    fn = getattr(ref.ref_lib(), name)
+    fn.argtypes = _lib._SIGS[name]
+    return fn
+
+
+@pytest.mark.parametrize("log_n", [20, 28])
+def test_ntt_words_equal_reference_kernels(ref, log_n):
+    """Every word of evaluate and interpolate on 2^log_n uniform M31 values
+    over half_coset(log_n) equals the reference's own launchers
+    (circle_ntt.cu:248-312, Forge layer kernels) run on the same twiddle
+    tables; the round trip returns the input."""
+    import torch
+    from vortexstark_b200 import ntt
+    from vortexstark_b200.circle import Coset
+    from vortexstark_b200.ntt import _host_u32
+    from vortexstark_b200.workload import m31_array
+    from gpu_util import to_dev
+
+    n = 1 << log_n
+    cache = ntt.TwiddleCache(Coset.half_coset(log_n))
+    x = to_dev(m31_array(7000 + log_n, n))
+    mine, theirs = x.clone(), x.clone()
+    offs, sizes = _host_u32(cache.layer_offsets), _host_u32(cache.layer_sizes)
+    ntt.evaluate(mine, cache)
+    _ref_ntt(ref, "cuda_circle_ntt_evaluate")(theirs.data_ptr(), cache.d_twiddles.data_ptr(),
+                                              cache.d_circle_twids.data_ptr(), offs, sizes, log_n - 1, n)
+    torch.cuda.synchronize()
+    assert torch.equal(mine, theirs)
+    assert not torch.equal(mine, x)
+    ntt.interpolate(mine, cache)
+    _ref_ntt(ref, "cuda_circle_ntt_interpolate")(theirs.data_ptr(), cache.d_itwiddles.data_ptr(),
+                                                 cache.d_circle_itwids.data_ptr(), offs, sizes, log_n - 1, n)
+    torch.cuda.synchronize()
+    assert torch.equal(mine, theirs)
+    assert torch.equal(mine, x)
+    del x, mine, theirs, cache
+    torch.cuda.empty_cache()

@@ -33,6 +33,34 @@ def test_mixed_stream_equals_alone(oracle):
             assert alone == oracle.prove(a, b, log_n)
 
 
+def test_measured_mix_equals_alone(oracle):
+    """The benchmark's own stream (log_n 16..24 at weights .4/.25/.2/.1/.05),
+    with three requests of each large size added, through the engine as the
+    benchmark configures it and at an arrival rate above the plain path's
+    capacity, so large and small proofs overlap on the device.  Every proof
+    equals the same request proved alone; the log_n = 16 ones equal the
+    oracle's."""
+    from vortexstark_b200.workload import served_stream
+
+    reqs = served_stream(2024, 40)
+    g = SplitMix64(99)
+    reqs += [(ln, g.m31(), g.m31()) for ln in (20, 22, 24) for _ in range(3)]
+    g2 = SplitMix64(5)
+    order = sorted(range(len(reqs)), key=lambda i: g2.next())
+    reqs = [reqs[i] for i in order]
+    with ProofServer(budget_bytes=48 << 30, max_inflight=24) as srv:
+        for ln, c in {16: 6, 18: 4, 20: 3, 22: 2, 24: 2}.items():
+            srv.prewarm(ln, c)
+        summary, results = run_stream(srv, reqs, poisson_arrivals(len(reqs), 600.0, 3), keep_results=True)
+    assert summary["n"] == len(reqs)
+    assert {ln for ln, _, _ in reqs} >= {16, 18, 20, 22, 24}
+    for i, (log_n, a, b) in enumerate(reqs):
+        alone = prover.prove_bytes(a, b, log_n)
+        assert results[i] == alone, (i, log_n)
+        if log_n == 16:
+            assert alone == oracle.prove(a, b, log_n)
+
+
 def test_tight_budget_queues_and_stays_exact():
     reqs = _stream(11, 16, [10, 12])
     # room for one slot of each size (slot buffers + device input words +

@@ -11,7 +11,8 @@ from vortexstark_b200.workload import m31_array
 pytestmark = pytest.mark.gpu
 P = 0x7FFFFFFF
 
-NTT_PLANS = [(9, 3), (9, 5), (10, 4), (10, 6), (11, 7), (12, 8), (12, 9)]
+NTT_PLANS = [(9, 3), (9, 5), (10, 4), (10, 6), (11, 7), (12, 8), (12, 9), (12, 10), (11, 11), (12, 12),
+             (13, 12), (14, 12), (14, 10), (13, 11), (13, 10), (11, 8)]
 
 
 @pytest.fixture(autouse=True)
@@ -21,7 +22,7 @@ def _defaults():
     tune.reset()
 
 
-@pytest.mark.parametrize("k", [11, 13, 14, 17, 20])
+@pytest.mark.parametrize("k", [11, 13, 14, 17, 20, 23, 24, 26])
 def test_ntt_plans_match_oracle(oracle, k):
     from vortexstark_b200 import ntt
     from vortexstark_b200.circle import Coset
@@ -38,7 +39,7 @@ def test_ntt_plans_match_oracle(oracle, k):
         assert np.array_equal(to_host(d), x), (bottom, upper)
 
 
-@pytest.mark.parametrize("L", [13, 16])
+@pytest.mark.parametrize("L", [13, 16, 22])
 def test_stwo_ntt_plans_match_oracle(oracle, L):
     from vortexstark_b200 import ntt
     cache = ntt.StwoNttCache(L)
@@ -104,7 +105,7 @@ def test_autotune_report_and_results(oracle):
         assert 1 <= k <= 4 and ms > 0
         assert tune.get(tune.FOLD_LEAF_K, d)[0] == k
     for t, (b, u, ms) in rep["ntt"].items():
-        assert 10 <= b <= 12 and 6 <= u <= 9 and ms > 0
+        assert 10 <= b <= 14 and 6 <= u <= 12 and ms > 0
         assert tune.get(tune.NTT_PLAN, t) == (b, u)
     for d, (k, ms) in rep["leaf_k"].items():
         assert 1 <= k <= 4 and ms > 0
@@ -115,7 +116,8 @@ def test_autotune_report_and_results(oracle):
 
 def test_tune_set_rejects_bad_knobs():
     from vortexstark_b200 import _lib
-    for args in ((0, 20, 8, 9), (0, 20, 12, 10), (1, 20, 5, 0), (2, 20, 5, 0), (3, 20, 1, 0), (0, 40, 12, 9)):
+    for args in ((0, 20, 8, 9), (0, 20, 12, 13), (0, 20, 15, 9), (0, 20, 12, 2), (1, 20, 5, 0), (2, 20, 5, 0),
+                 (3, 20, 1, 0), (0, 40, 12, 9)):
         with pytest.raises(_lib.VortexError):
             _lib.check(_lib.lib().vx_tune_set(*args))
 

@@ -9,13 +9,15 @@ from vortexstark_b200 import _lib
 import ctypes as C
 
 # (layers, log2 tile columns) pairs the pass kernels are instantiated for:
-# bottom passes on contiguous tiles, upper passes on 4096-element tiles
-BOTTOM_SHAPES = {(r, 0) for r in range(4, 13)}
-UPPER_SHAPES = {(r, 12 - r) for r in range(3, 10)}
+# bottom passes on contiguous tiles of up to 2^14 elements, upper passes of
+# 3..9 layers on 4096-element tiles, of 10 and 11 layers on 8192-element
+# tiles and of 12 layers on 16384-element tiles
+BOTTOM_SHAPES = {(r, 0) for r in range(4, 15)}
+UPPER_SHAPES = {(r, 12 - r) for r in range(3, 10)} | {(10, 3), (11, 2), (12, 2)}
 
 
-@pytest.mark.parametrize("bottom", range(9, 13))
-@pytest.mark.parametrize("upper", range(3, 10))
+@pytest.mark.parametrize("bottom", range(9, 15))
+@pytest.mark.parametrize("upper", range(3, 13))
 def test_every_ntt_plan_is_launchable(bottom, upper):
     for total in range(4, 32):
         plan = tune.ntt_plan(total, bottom, upper)
@@ -30,12 +32,20 @@ def test_every_ntt_plan_is_launchable(bottom, upper):
                 assert r <= bottom or r == total <= 12  # up to 12 layers: one pass
             else:
                 assert r <= max(upper, 5)
+                assert w >= 2  # rows of at least 16 bytes (one 16-byte access)
             start += r
         assert start == total
 
 
 def test_default_ntt_plan_matches_the_built_in_rule():
-    # the defaults (12, 9) give the plans the transforms were validated with
+    assert tune.ntt_plan(24, 12, 12) == [(0, 12, 0), (12, 12, 2)]
+    assert tune.ntt_plan(24, 11, 8) == [(0, 11, 0), (11, 7, 5), (18, 6, 6)]
+    assert tune.ntt_plan(26, 14, 12) == [(0, 14, 0), (14, 12, 2)]
+    assert tune.ntt_plan(24, 13, 11) == [(0, 13, 0), (13, 11, 2)]
+    assert tune.ntt_plan(23, 13, 10) == [(0, 13, 0), (13, 10, 3)]
+    assert tune.ntt_plan(26, 12, 12) == [(0, 12, 0), (12, 7, 5), (19, 7, 5)]
+    assert tune.ntt_plan(28, 12, 10) == [(0, 12, 0), (12, 8, 4), (20, 8, 4)]
+    assert tune.ntt_plan(13, 14, 12) == [(0, 13, 0)]
     assert tune.ntt_plan(24, 12, 9) == [(0, 12, 0), (12, 6, 6), (18, 6, 6)]
     assert tune.ntt_plan(14, 12, 9) == [(0, 11, 0), (11, 3, 9)]
     assert tune.ntt_plan(21, 12, 9) == [(0, 12, 0), (12, 9, 3)]
@@ -46,7 +56,7 @@ def test_default_ntt_plan_matches_the_built_in_rule():
 
 
 def test_ntt_plan_rejects_unbuilt_shapes():
-    for args in ((24, 8, 9), (24, 12, 10), (3, 12, 9), (32, 12, 9)):
+    for args in ((24, 8, 9), (24, 12, 13), (24, 15, 9), (3, 12, 9), (32, 12, 9)):
         with pytest.raises(_lib.VortexError):
             tune.ntt_plan(*args)
 

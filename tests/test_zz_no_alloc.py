@@ -1,9 +1,10 @@
 """vx_prove_fib_noalloc: the whole proof with no device allocation.
 
-Some callers cannot allocate device memory — code running inside a stream
-capture, hosts whose device memory belongs to another allocator, sandboxes
-that forbid cudaMalloc after start-up.  This entry point keeps all its device
-scratch in one static array of the library.  Its proofs must equal those of
+Some callers cannot call cudaMalloc — hosts whose device memory belongs to
+another allocator, sandboxes that forbid allocation after start-up.  This
+entry point keeps all its device scratch in one static array of the library
+(and, being synchronous on the legacy stream, is never called under a stream
+capture).  Its proofs must equal those of
 the allocating entry point (vx_prove_fib) byte for byte, on consecutive calls
 that reuse the shared array.  This file is collected last on purpose.
 """

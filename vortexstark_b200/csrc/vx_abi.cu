@@ -530,9 +530,35 @@ void ref_layers(uint32_t *d, const uint32_t *line, const uint32_t *circle, const
     }
 }
 
-__global__ void scale_kernel(uint32_t *d, uint32_t s, uint64_t n) {
+__global__ void scale_kernel(uint32_t *d, uint32_t *const *cols, uint32_t s, uint64_t n) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (cols) d = cols[blockIdx.y];
     if (i < n) d[i] = mmul(d[i], s);
+}
+
+// The batched reference order with a partial layer count (n_line line
+// layers and the circle layer, then the 2^-log_n scale for the inverse), as
+// the reference's batched launchers do for any n_line (circle_ntt.cu:314-404,
+// circle_ntt_batch_forge.cu:95-185): per-layer launches over all columns.
+cudaError_t ref_layers_cols(uint32_t *const *cols, uint32_t n_cols, const uint32_t *line, const uint32_t *circle,
+                            const uint32_t *h_off, uint32_t n_line, uint32_t log_n, bool forward) {
+    cudaError_t e = cudaSuccess;
+    if (forward) {
+        for (int l = (int)n_line - 1; l >= 0 && e == cudaSuccess; l--)
+            e = ntt_single_layer_cols(cols, n_cols, line + h_off[l], (uint32_t)l + 1, log_n, true, 0);
+        if (e == cudaSuccess) e = ntt_single_layer_cols(cols, n_cols, circle, 0, log_n, true, 0);
+    } else {
+        e = ntt_single_layer_cols(cols, n_cols, circle, 0, log_n, false, 0);
+        for (uint32_t l = 0; l < n_line && e == cudaSuccess; l++)
+            e = ntt_single_layer_cols(cols, n_cols, line + h_off[l], l + 1, log_n, false, 0);
+        if (e == cudaSuccess) {
+            const uint32_t e2 = (30u * log_n) % 31u;
+            const uint64_t n = 1ull << log_n;
+            scale_kernel<<<dim3(blocks_for(n, 256), n_cols), 256>>>(nullptr, cols, e2 == 0 ? 1u : (1u << e2), n);
+            e = cudaGetLastError();
+        }
+    }
+    return e;
 }
 
 }  // namespace
@@ -571,7 +597,7 @@ void cuda_circle_ntt_interpolate(uint32_t *d, const uint32_t *itw, const uint32_
     } else {
         ref_layers(d, itw, ictw, h_off, n_line, log_n, false);
         uint32_t e2 = (30u * log_n) % 31u;
-        scale_kernel<<<blocks_for(n, 256), 256>>>(d, e2 == 0 ? 1u : (1u << e2), n);
+        scale_kernel<<<blocks_for(n, 256), 256>>>(d, nullptr, e2 == 0 ? 1u : (1u << e2), n);
         VX_LAUNCH_CHECK();
     }
     cudaDeviceSynchronize();
@@ -582,7 +608,10 @@ void cuda_circle_ntt_evaluate_batch(uint32_t **cols, const uint32_t *tw, const u
     (void)h_sizes;
     uint32_t log_n = log2_exact(n);
     if (n_cols) {
-        cudaError_t e = ntt_transform(nullptr, cols, 0, n_cols, log_n, ref_tables(tw, ctw, h_off, n_line), true, nullptr, 0, 0);
+        cudaError_t e = n_line + 1 == log_n
+                            ? ntt_transform(nullptr, cols, 0, n_cols, log_n, ref_tables(tw, ctw, h_off, n_line), true,
+                                            nullptr, 0, 0)
+                            : ref_layers_cols(cols, n_cols, tw, ctw, h_off, n_line, log_n, true);
         if (e != cudaSuccess) set_last_error(VX_ERR_CUDA, "cuda_circle_ntt_evaluate_batch: %s", cudaGetErrorString(e));
     }
     cudaDeviceSynchronize();
@@ -594,7 +623,10 @@ void cuda_circle_ntt_interpolate_batch(uint32_t **cols, const uint32_t *itw, con
     (void)h_sizes;
     uint32_t log_n = log2_exact(n);
     if (n_cols) {
-        cudaError_t e = ntt_transform(nullptr, cols, 0, n_cols, log_n, ref_tables(itw, ictw, h_off, n_line), false, nullptr, 0, 0);
+        cudaError_t e = n_line + 1 == log_n
+                            ? ntt_transform(nullptr, cols, 0, n_cols, log_n, ref_tables(itw, ictw, h_off, n_line),
+                                            false, nullptr, 0, 0)
+                            : ref_layers_cols(cols, n_cols, itw, ictw, h_off, n_line, log_n, false);
         if (e != cudaSuccess) set_last_error(VX_ERR_CUDA, "cuda_circle_ntt_interpolate_batch: %s", cudaGetErrorString(e));
     }
     cudaDeviceSynchronize();
@@ -648,6 +680,26 @@ int forge_batch(bool fwd, uint32_t *const *col_ptrs, const uint32_t *tw, const u
     return VX_OK;
 }
 }  // namespace
+
+}  // extern "C"
+namespace vx {
+// Frees every device's column-pointer array of the forge forms (called by
+// vx_release_all; the next forge call allocates a fresh one).
+void forge_cols_release() {
+    std::lock_guard<std::mutex> lk(g_forge_cols_mu);
+    for (int d = 0; d < 64; d++) {
+        if (!g_forge_cols[d]) continue;
+        int cur = 0;
+        cudaGetDevice(&cur);
+        if (cudaSetDevice(d) == cudaSuccess) cudaFree(g_forge_cols[d]);
+        cudaSetDevice(cur);
+        cudaGetLastError();
+        g_forge_cols[d] = nullptr;
+        g_forge_cols_cap[d] = 0;
+    }
+}
+}  // namespace vx
+extern "C" {
 
 void cuda_circle_ntt_evaluate_batch_forge(uint32_t *const *col_ptrs, const uint32_t *tw, const uint32_t *ctw,
                                           const uint32_t *h_off, const uint32_t *h_sizes, uint32_t n_line, uint32_t n,

@@ -39,6 +39,32 @@ void set_last_error(int code, const char *fmt, ...);
                                  cudaGetErrorString(_e));                                   \
     } while (0)
 
+// Programmatic dependent launch.  A kernel launched with launch_pdl may have
+// its blocks scheduled while the previous kernel on the stream drains, so the
+// launch latency between dependent kernels is hidden; it calls pdl_wait()
+// before it touches memory that earlier work on the stream wrote.  pdl_wait()
+// returns at once when the kernel was launched without the attribute.
+__device__ __forceinline__ void pdl_wait() {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 900
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+#endif
+}
+template <class... KArgs, class... Args>
+inline cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 inline unsigned blocks_for(uint64_t n, unsigned threads) {
     return (unsigned)((n + threads - 1) / threads);
 }

@@ -95,6 +95,16 @@ __device__ __forceinline__ qm31 qmul_mat(const qmat &m, qm31 z) {
              dot4(m.a2, z0, m.na3, z1, m.a0, z2, m.na1, z3), dot4(m.a3, z0, m.a2, z1, m.a1, z2, m.a0, z3)}};
 }
 
+// Product with a doubled twiddle t2 = 2 t (t canonical, so t2 <= 2P - 2 <
+// 2^32): p = a t2 < 2^63 for canonical a, a t = p / 2 = hi 2^31 + lo / 2,
+// and 2^31 = 1 (mod P), so a t = hi + lo / 2 (mod P) with hi <= 2^31 - 2 and
+// lo / 2 <= 2^31 - 1: one conditional subtract makes it canonical.
+__device__ __forceinline__ uint32_t mmul_t2(uint32_t a, uint32_t t2) {
+    const uint64_t p = (uint64_t)a * t2;
+    const uint32_t r = (uint32_t)(p >> 32) + ((uint32_t)p >> 1);
+    return umin32(r, r - VX_P);
+}
+
 // Circle group point (x, y) with x^2 + y^2 = 1; group law of src/circle.rs:33-39.
 struct cpoint { uint32_t x, y; };
 __device__ __forceinline__ cpoint pmul(cpoint a, cpoint b) {

@@ -328,17 +328,19 @@ int lift_stage(vx_lifted *h, uint32_t stage, cudaStream_t st, uint32_t *launches
     uint32_t *proof = h->proof;
     const uint32_t B = L.B, S = L.S;
     switch (stage) {
-    case 0:  // LDE of every column, one launch per pass per size
+    case 0: {  // LDE of every column: each pass of all size groups in one launch
         VX_CUDA_TRY(cudaMemsetAsync(h->chan, 0, sizeof(DevChannel), st));
+        NttGroup gi[kMaxLiftCols], ge[kMaxLiftCols];
         for (uint32_t g = 0; g < h->n_groups; g++) {
             const uint32_t lg = h->glog[g];
-            VX_CUDA_TRY(ntt_transform(h->co[g], nullptr, 1ull << lg, h->gcnt[g], lg, stwo_tables(h->itw[g], lg), false,
-                                      h->in[g], lg, st));
-            VX_CUDA_TRY(ntt_transform(h->lde[g], nullptr, 1ull << (lg + B), h->gcnt[g], lg + B,
-                                      stwo_tables(h->tw[g], lg + B), true, h->co[g], lg, st));
-            *launches += ntt_pass_count(lg) + ntt_pass_count(lg);
+            gi[g] = NttGroup{h->co[g], 1ull << lg, h->gcnt[g], lg, stwo_tables(h->itw[g], lg), h->in[g], lg};
+            ge[g] = NttGroup{h->lde[g], 1ull << (lg + B), h->gcnt[g], lg + B, stwo_tables(h->tw[g], lg + B), h->co[g],
+                             lg};
         }
+        VX_CUDA_TRY(ntt_transform_groups(gi, h->n_groups, false, st, launches));
+        VX_CUDA_TRY(ntt_transform_groups(ge, h->n_groups, true, st, launches));
         break;
+    }
     case 1:  // lifted tree over the LDE rows, mix its root, draw alpha
         VX_CUDA_TRY(tree_build(h->cols, h->lv0, ChanStep{h->chan, proof + L.r0, h->alpha}, st));
         *launches += tree_launches(h->lv0);

@@ -8,6 +8,7 @@ namespace vx {
 
 __global__ void __launch_bounds__(256) node_subtree_kernel(const uint32_t *in, uint32_t *out, uint64_t n_threads,
                                                            uint32_t k, uint32_t one) {
+    pdl_wait();
     uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n_threads) return;
     uint32_t h[8];

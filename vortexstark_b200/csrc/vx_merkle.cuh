@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include "vx_blake2s.cuh"
+#include "vx_common.cuh"
 #include "vx_field.cuh"
 
 namespace vx {
@@ -230,6 +231,7 @@ __device__ __forceinline__ void store_hash(uint32_t *dst, const uint32_t h[8]) {
 template <class Src>
 __global__ void __launch_bounds__(256) leaf_subtree_kernel(Src src, uint32_t *out, uint64_t n_threads, uint32_t kl,
                                                            uint32_t one) {
+    pdl_wait();
     uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n_threads) return;
     if constexpr (plain_adds<Src>::value) one = 1u;
@@ -361,6 +363,7 @@ template <class Src>
 __global__ void __launch_bounds__(kReduceThreads) tree_reduce_kernel(Src src, TreeLevels lv, ChanStep cs, uint32_t one) {
     __shared__ __align__(16) uint32_t sh[8u << kStageLog];
     __shared__ uint32_t is_last;
+    pdl_wait();
     if constexpr (plain_adds<Src>::value) one = 1u;
     const uint32_t depth = lv.height[lv.n - 1];
     uint32_t h = lv.height[lv.top];
@@ -424,25 +427,31 @@ __global__ void __launch_bounds__(kReduceThreads) tree_reduce_kernel(Src src, Tr
     }
 }
 
-// Build all stored levels and the transcript step (no host sync).
+// Build all stored levels and the transcript step (no host sync).  Every
+// kernel is a programmatic dependent launch: the chain of a commitment (and
+// of consecutive commitments, FRI layer after FRI layer) is strictly ordered
+// by pdl_wait() at each kernel's start, and only the launch gaps overlap.
 template <class Src>
 cudaError_t tree_build(const Src &src, const TreeLevels &lv, const ChanStep &cs, cudaStream_t stream) {
     const uint32_t depth = lv.height[lv.n - 1];
+    cudaError_t e = cudaSuccess;
     if (lv.top > 0) {
         uint32_t kl = lv.height[1];
         uint64_t n1 = 1ull << (depth - kl);
-        leaf_subtree_kernel<Src><<<(unsigned)((n1 + 255) / 256), 256, 0, stream>>>(src, lv.hashes[1], n1, kl, 1u);
-        for (uint32_t i = 2; i <= lv.top; i++) {
+        e = launch_pdl(leaf_subtree_kernel<Src>, dim3((unsigned)((n1 + 255) / 256)), dim3(256), 0, stream, src,
+                       lv.hashes[1], n1, kl, 1u);
+        for (uint32_t i = 2; i <= lv.top && e == cudaSuccess; i++) {
             uint32_t k = lv.height[i] - lv.height[i - 1];
             uint64_t nt = 1ull << (depth - lv.height[i]);
-            node_subtree_kernel<<<(unsigned)((nt + 255) / 256), 256, 0, stream>>>(lv.hashes[i - 1], lv.hashes[i], nt,
-                                                                                  k, 1u);
+            e = launch_pdl(node_subtree_kernel, dim3((unsigned)((nt + 255) / 256)), dim3(256), 0, stream,
+                           (const uint32_t *)lv.hashes[i - 1], lv.hashes[i], nt, k, 1u);
         }
     }
+    if (e != cudaSuccess) return e;
     const uint32_t u = depth - lv.height[lv.top];
     const uint32_t c0 = u < kStageLog ? u : kStageLog;
-    tree_reduce_kernel<Src><<<(unsigned)(1ull << (u - c0)), kReduceThreads, 0, stream>>>(src, lv, cs, 1u);
-    return cudaGetLastError();
+    return launch_pdl(tree_reduce_kernel<Src>, dim3((unsigned)(1ull << (u - c0))), dim3(kReduceThreads), 0, stream,
+                      src, lv, cs, 1u);
 }
 
 // Kernels launched by tree_build for this plan.

@@ -75,9 +75,13 @@ __global__ void __launch_bounds__(512) ntt_pass_kernel(
     }
 }
 
-__global__ void ntt_layer_kernel(uint32_t *d, const uint32_t *__restrict__ tw, uint32_t L, uint64_t half_n, int fwd) {
+// One layer over a whole array; with `cols` non-null, over column
+// cols[blockIdx.y] instead of d.
+__global__ void ntt_layer_kernel(uint32_t *d, uint32_t *const *cols, const uint32_t *__restrict__ tw, uint32_t L,
+                                 uint64_t half_n, int fwd) {
     uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= half_n) return;
+    if (cols) d = cols[blockIdx.y];
     uint64_t stride = 1ull << L;
     uint64_t h = tid >> L;
     uint64_t i0 = (h << (L + 1)) + (tid & (stride - 1ull)), i1 = i0 + stride;
@@ -94,14 +98,16 @@ __global__ void ntt_layer_kernel(uint32_t *d, const uint32_t *__restrict__ tw, u
 
 // ---------------------------------------------------------------------
 // Register-radix pass: a tile of 2^(R+WL) elements (2^R rows of 2^WL
-// columns), 16 elements per thread.  The pass's R layers run in stages of up
-// to 4 layers; in a stage each thread holds the 16 elements that differ in
-// one contiguous block of 4 tile bits [A, A+4) covering the stage's layer
-// bits, and does all the stage's butterflies in registers.  Between stages
-// the tile goes through shared memory (padded by one word per 32 to spread
-// the strided accesses over the banks).  The tile's twiddles (2^R - 1 words,
-// one contiguous run of the reference table per layer) are staged in shared
-// memory once per tile.
+// columns) held in shared memory by NT threads, DPT = 2^(R+WL) / NT = 16 or
+// 32 elements per thread.  The pass's R layers run in stages of up to 4
+// layers; in a stage each thread takes groups of the 16 elements that
+// differ in one contiguous block of 4 tile bits [A, A+4) covering the
+// stage's layer bits, and does all the stage's butterflies on them in
+// registers.  Between stages the tile goes through shared memory (padded by
+// one word per 32 to spread the strided accesses over the banks).  The
+// tile's twiddles (2^R - 1 words, one contiguous run of the reference table
+// per layer) are staged in shared memory once per tile, doubled when the
+// butterflies multiply with mmul_t2 (kTwiddleX2).  All values stay canonical.
 // ---------------------------------------------------------------------
 struct Pass2Args {
     uint32_t *data;
@@ -113,50 +119,92 @@ struct Pass2Args {
     uint32_t cmode;
     PassOff off;
     uint32_t s;       // lowest layer of the pass
-    uint32_t scale;   // 1 = none
+    uint32_t scale;   // output scale (1 = none)
     uint32_t vec;     // 1: columns and source 16-byte aligned, 4 consecutive elements per access
 };
 
+// Butterfly products: with a doubled twiddle (mmul_t2: one multiply, one
+// shift-add, one conditional subtract) or the plain one (mmul: a fold of the
+// 64-bit product); both exact, the choice is the faster on the device.
+constexpr bool kTwiddleX2 = true;
+__device__ __forceinline__ uint32_t tw_stage(uint32_t t) { return kTwiddleX2 ? 2u * t : t; }
+__device__ __forceinline__ uint32_t tw_mul(uint32_t v, uint32_t t) { return kTwiddleX2 ? mmul_t2(v, t) : mmul(v, t); }
+
 __device__ __forceinline__ uint32_t pad32(uint32_t e) { return e + (e >> 5); }
+// Word offset of the staged twiddles after a padded tile of ts words, rounded
+// up to 16 bytes for the vector reads.
+constexpr uint32_t tw_base(uint32_t ts) { return (ts + ts / 32 + 3u) & ~3u; }
 // pad32(a | b) = pad32(a) + b + (b >> 5) when a and b have no bit in common
 // (a shift distributes over OR, and an OR of disjoint fields is a sum).  The
 // stage and tile accesses below are all of this form with b a compile-time
 // offset, so each thread computes one padded base and the accesses use
 // immediate offsets.
 
-template <bool FWD, int R, int WL, int LO, int HI, int A>
-__device__ __forceinline__ void ntt_stage(uint32_t *sm, const uint32_t *smtw, uint32_t tid) {
-    constexpr int TB = R + WL;
-    const uint32_t base = (tid & ((1u << A) - 1u)) | ((tid >> A) << (A + 4));  // bits [A, A+4) zero
-    const uint32_t pb = pad32(base);
-    uint32_t v[16];
+// One layer of a stage on the 16 register values of a group.  The layer's
+// 16 >> (rb + 1) twiddles are one aligned run: layer j sits at
+// smtw[2^(R-1-j) ..] and base >> S (S = A + rb + 1, base's bits [A, A+4)
+// zero) is a multiple of the run length, so the run is read with 16-, 8- or
+// 4-byte loads.
+template <bool FWD, int R, int WL, int A, int J>
+__device__ __forceinline__ void stage_layer(uint32_t v[16], uint32_t base, const uint32_t *smtw) {
+    constexpr int rb = J + WL - A;  // register bit of layer J
+    constexpr int S = J + 1 + WL;   // tile-index shift giving the twiddle index
+    constexpr int RL = 8 >> rb;
+    const uint32_t *tp = smtw + (1u << (R - 1 - J)) + (base >> S);
+    uint32_t tw[RL];
+    if constexpr (RL >= 4) {
 #pragma unroll
-    for (int i = 0; i < 16; i++) v[i] = sm[pb + ((uint32_t)i << A) + (((uint32_t)i << A) >> 5)];
-#pragma unroll
-    for (int jj = 0; jj < HI - LO; jj++) {
-        const int j = FWD ? (HI - 1 - jj) : (LO + jj);
-        const int rb = j + WL - A;            // register bit of layer j
-        const int S = j + 1 + WL;             // tile-index shift giving the twiddle index
-        const uint32_t *tw = smtw + ((1u << (R - 1 - j)) - 1u) + (base >> S);
-#pragma unroll
-        for (int i0 = 0; i0 < 16; i0++) {
-            if (i0 & (1 << rb)) continue;
-            const int i1 = i0 | (1 << rb);
-            const uint32_t t = tw[i0 >> (rb + 1)];
-            if (FWD) {
-                uint32_t x = mmul(v[i1], t);
-                v[i1] = msub(v[i0], x);
-                v[i0] = madd(v[i0], x);
-            } else {
-                uint32_t a = v[i0], b = v[i1];
-                v[i0] = madd(a, b);
-                v[i1] = mmul(msub(a, b), t);
-            }
+        for (int q = 0; q < RL / 4; q++) {
+            const uint4 x = ((const uint4 *)tp)[q];
+            tw[4 * q] = x.x; tw[4 * q + 1] = x.y; tw[4 * q + 2] = x.z; tw[4 * q + 3] = x.w;
         }
+    } else if constexpr (RL == 2) {
+        const uint2 x = *(const uint2 *)tp;
+        tw[0] = x.x; tw[1] = x.y;
+    } else {
+        tw[0] = tp[0];
     }
 #pragma unroll
-    for (int i = 0; i < 16; i++) sm[pb + ((uint32_t)i << A) + (((uint32_t)i << A) >> 5)] = v[i];
-    (void)TB;
+    for (int i0 = 0; i0 < 16; i0++) {
+        if (i0 & (1 << rb)) continue;
+        const int i1 = i0 | (1 << rb);
+        const uint32_t t = tw[i0 >> (rb + 1)];
+        if (FWD) {
+            const uint32_t x = tw_mul(v[i1], t);
+            v[i1] = msub(v[i0], x);
+            v[i0] = madd(v[i0], x);
+        } else {
+            const uint32_t a = v[i0], b = v[i1];
+            v[i0] = madd(a, b);
+            v[i1] = tw_mul(msub(a, b), t);
+        }
+    }
+}
+
+template <bool FWD, int R, int WL, int A, int LO, int HI, int JJ>
+__device__ __forceinline__ void stage_layers(uint32_t v[16], uint32_t base, const uint32_t *smtw) {
+    if constexpr (JJ < HI - LO) {
+        constexpr int J = FWD ? (HI - 1 - JJ) : (LO + JJ);
+        stage_layer<FWD, R, WL, A, J>(v, base, smtw);
+        stage_layers<FWD, R, WL, A, LO, HI, JJ + 1>(v, base, smtw);
+    }
+}
+
+template <bool FWD, int R, int WL, int NT, int LO, int HI, int A>
+__device__ __forceinline__ void ntt_stage(uint32_t *sm, const uint32_t *smtw, uint32_t tid) {
+    constexpr int G = (1 << (R + WL)) / 16 / NT;  // 16-element groups per thread
+#pragma unroll
+    for (int g = 0; g < G; g++) {
+        const uint32_t bi = tid + (uint32_t)g * NT;
+        const uint32_t base = (bi & ((1u << A) - 1u)) | ((bi >> A) << (A + 4));  // bits [A, A+4) zero
+        const uint32_t pb = pad32(base);
+        uint32_t v[16];
+#pragma unroll
+        for (int i = 0; i < 16; i++) v[i] = sm[pb + ((uint32_t)i << A) + (((uint32_t)i << A) >> 5)];
+        stage_layers<FWD, R, WL, A, LO, HI, 0>(v, base, smtw);
+#pragma unroll
+        for (int i = 0; i < 16; i++) sm[pb + ((uint32_t)i << A) + (((uint32_t)i << A) >> 5)] = v[i];
+    }
 }
 
 // Compile-time stage list: stage k covers pass layers [lo, hi), at most 4,
@@ -172,33 +220,36 @@ struct StageIdx {
     static constexpr int A = (HI + WL - A0) <= 4 ? A0 : (HI + WL - 4);
 };
 
-template <bool FWD, int R, int WL, int K>
+template <bool FWD, int R, int WL, int NT, int K>
 __device__ __forceinline__ void run_stages(uint32_t *sm, const uint32_t *smtw, uint32_t tid) {
     if constexpr (K < StageIdx<FWD, R, WL, K>::NST) {
         using St = StageIdx<FWD, R, WL, K>;
-        ntt_stage<FWD, R, WL, St::LO, St::HI, St::A>(sm, smtw, tid);
+        ntt_stage<FWD, R, WL, NT, St::LO, St::HI, St::A>(sm, smtw, tid);
         __syncthreads();
-        run_stages<FWD, R, WL, K + 1>(sm, smtw, tid);
+        run_stages<FWD, R, WL, NT, K + 1>(sm, smtw, tid);
     }
 }
 
-template <bool FWD, int R, int WL>
-__global__ void __launch_bounds__((1 << (R + WL)) / 16) ntt_pass2_kernel(Pass2Args p) {
-    constexpr int TB = R + WL, TS = 1 << TB, NT = TS / 16, W = 1 << WL;
-    extern __shared__ uint32_t dsm[];
+// Up to 1024 resident threads per SM: 64 registers a thread.
+constexpr int min_blocks_for(int nt) { return (1024 / nt) < 32 ? (1024 / nt) : 32; }
+
+// One tile of one column: tile index `tile` of column `ci`.
+template <bool FWD, int R, int WL, int NT>
+__device__ __forceinline__ void tile_pass(const Pass2Args &p, uint64_t tile, uint32_t ci, uint32_t *dsm) {
+    constexpr int TB = R + WL, TS = 1 << TB, W = 1 << WL;
+    constexpr int DPT = TS / NT;                // 16 or 32 data elements per thread
+    static_assert(DPT == 16 || DPT == 32, "16 or 32 elements per thread");
     uint32_t *sm = dsm;                          // TS + TS/32 words
-    uint32_t *smtw = dsm + TS + TS / 32;         // 2^R - 1 twiddles
+    uint32_t *smtw = dsm + tw_base(TS);          // 2^R words: layer j's twiddles at [2^(R-1-j), 2^(R-j))
     const uint32_t tid = threadIdx.x;
     const uint32_t s = p.s;
     const uint32_t cshift = s - WL;
-    const uint64_t tile = blockIdx.x;
     const uint64_t cb = tile & ((1ull << cshift) - 1ull);
     const uint64_t hb = tile >> cshift;
-    uint32_t *col = p.dev_cols ? p.dev_cols[blockIdx.y] : p.data + (uint64_t)blockIdx.y * p.col_stride;
-    const uint32_t *in = p.src ? p.src + (uint64_t)blockIdx.y * p.src_stride : col;
+    uint32_t *col = p.dev_cols ? p.dev_cols[ci] : p.data + (uint64_t)ci * p.col_stride;
+    const uint32_t *in = p.src ? p.src + (uint64_t)ci * p.src_stride : col;
     const uint64_t gbase = (hb << (s + R)) | (cb << WL);
 
-    constexpr int DPT = TS / NT;                // 16 data elements per thread
     // Data loads first (their latency overlaps the twiddle loads).  The
     // vector form moves 4 consecutive tile elements per access: a row of the
     // tile is 2^WL >= 4 contiguous words (or the whole tile is contiguous,
@@ -221,29 +272,32 @@ __global__ void __launch_bounds__((1 << (R + WL)) / 16) ntt_pass2_kernel(Pass2Ar
         }
     }
     // Twiddles of pass layer j are table words h in [hb 2^(R-1-j), (hb+1) 2^(R-1-j)),
-    // staged at smtw[2^(R-1-j) - 1 ..]; a flat index f decodes to (layer, offset).
-    // All loads are issued before the shared-memory stores.  (Per-layer loops
-    // over the contiguous runs measured slower: most of their predicated loads idle.)
+    // staged at smtw[2^(R-1-j) ..]; a flat index f decodes to (layer, offset).
+    // Loads are issued in batches of up to 8 per thread before their stores.
     {
         constexpr int TWN = (1 << R) - 1;
         constexpr int TWPT = (TWN + NT - 1) / NT;
-        uint32_t tv[TWPT];
+        constexpr int BATCH = TWPT < 8 ? TWPT : 8;
 #pragma unroll
-        for (int k = 0; k < TWPT; k++) {
-            uint32_t f = tid + (uint32_t)k * NT;
-            if (f < (uint32_t)TWN) {
-                uint32_t lg = 31u - __clz(f + 1u);
-                uint32_t j = R - 1 - lg;
-                uint32_t t = f + 1u - (1u << lg);
-                uint32_t L = s + j;
-                uint64_t h = (hb << lg) | t;
-                tv[k] = L ? __ldg(p.line + p.off.v[L - 1] + h) : circle_tw(p.circle, p.cmode, h);
+        for (int k0 = 0; k0 < TWPT; k0 += BATCH) {
+            uint32_t tv[BATCH];
+#pragma unroll
+            for (int kk = 0; kk < BATCH; kk++) {
+                const uint32_t f = tid + (uint32_t)(k0 + kk) * NT;
+                if (k0 + kk < TWPT && f < (uint32_t)TWN) {
+                    const uint32_t lg = 31u - __clz(f + 1u);
+                    const uint32_t j = R - 1 - lg;
+                    const uint32_t t = f + 1u - (1u << lg);
+                    const uint32_t L = s + j;
+                    const uint64_t h = (hb << lg) | t;
+                    tv[kk] = L ? __ldg(p.line + p.off.v[L - 1] + h) : circle_tw(p.circle, p.cmode, h);
+                }
             }
-        }
 #pragma unroll
-        for (int k = 0; k < TWPT; k++) {
-            uint32_t f = tid + (uint32_t)k * NT;
-            if (f < (uint32_t)TWN) smtw[f] = tv[k];
+            for (int kk = 0; kk < BATCH; kk++) {
+                const uint32_t f = tid + (uint32_t)(k0 + kk) * NT;
+                if (k0 + kk < TWPT && f < (uint32_t)TWN) smtw[f + 1u] = tw_stage(tv[kk]);
+            }
         }
     }
     // tid < NT and k NT (resp. 4 tid + q and 4 k NT) have disjoint bits
@@ -263,7 +317,7 @@ __global__ void __launch_bounds__((1 << (R + WL)) / 16) ntt_pass2_kernel(Pass2Ar
         }
     }
     __syncthreads();
-    run_stages<FWD, R, WL, 0>(sm, smtw, tid);
+    run_stages<FWD, R, WL, NT, 0>(sm, smtw, tid);
     if (p.vec) {
 #pragma unroll
         for (int k = 0; k < DPT / 4; k++) {
@@ -284,20 +338,85 @@ __global__ void __launch_bounds__((1 << (R + WL)) / 16) ntt_pass2_kernel(Pass2Ar
             const uint32_t e = tid + (uint32_t)k * NT;
             const uint64_t g = gbase | ((uint64_t)(e >> WL) << s) | (e & (W - 1u));
             const uint32_t o = (uint32_t)k * NT;
-            const uint32_t v = sm[ps1 + o + (o >> 5)];
-            col[g] = p.scale != 1u ? mmul(v, p.scale) : v;
+            const uint32_t w = sm[ps1 + o + (o >> 5)];
+            col[g] = p.scale != 1u ? mmul(w, p.scale) : w;
         }
     }
 }
 
+template <bool FWD, int R, int WL, int NT>
+__global__ void __launch_bounds__(NT, min_blocks_for(NT)) ntt_tile_kernel(Pass2Args p) {
+    extern __shared__ uint32_t dsm[];
+    tile_pass<FWD, R, WL, NT>(p, blockIdx.x, blockIdx.y, dsm);
+}
+
+// Several transforms of different lengths in one launch: group g's columns
+// and tiles are blocks [first[g], first[g+1]) of a 1-D grid, each group with
+// its own pass shape, all on 4096-element tiles of 256 threads (bottom
+// passes of 12 layers, upper passes of 3..9).  Used for columns of uneven
+// sizes, so a small size group does not run as a launch of its own that
+// leaves most SMs idle.
+constexpr uint32_t kMaxNttGroups = 4;
+struct MultiPassArgs {
+    Pass2Args g[kMaxNttGroups];
+    uint32_t R[kMaxNttGroups];
+    uint32_t first[kMaxNttGroups + 1];
+    uint32_t tiles[kMaxNttGroups];  // tiles per column
+    uint32_t n_groups;
+};
+
+template <bool FWD>
+__global__ void __launch_bounds__(256, 4) ntt_multi_kernel(MultiPassArgs a) {
+    extern __shared__ uint32_t dsm[];
+    const uint32_t b = blockIdx.x;
+    uint32_t gi = 0;
+    while (gi + 1 < a.n_groups && b >= a.first[gi + 1]) gi++;
+    const uint32_t local = b - a.first[gi];
+    const uint32_t ci = local / a.tiles[gi];
+    const uint64_t tile = local - ci * a.tiles[gi];
+    const Pass2Args &p = a.g[gi];
+    switch (a.R[gi]) {
+    case 12: tile_pass<FWD, 12, 0, 256>(p, tile, ci, dsm); break;
+    case 9: tile_pass<FWD, 9, 3, 256>(p, tile, ci, dsm); break;
+    case 8: tile_pass<FWD, 8, 4, 256>(p, tile, ci, dsm); break;
+    case 7: tile_pass<FWD, 7, 5, 256>(p, tile, ci, dsm); break;
+    case 6: tile_pass<FWD, 6, 6, 256>(p, tile, ci, dsm); break;
+    case 5: tile_pass<FWD, 5, 7, 256>(p, tile, ci, dsm); break;
+    case 4: tile_pass<FWD, 4, 8, 256>(p, tile, ci, dsm); break;
+    case 3: tile_pass<FWD, 3, 9, 256>(p, tile, ci, dsm); break;
+    default: break;
+    }
+}
+
+// Threads per tile: 16 elements per thread up to 2^12-element tiles (at most
+// 256 threads), 32 for 2^13 (256 threads) and 2^14 (512 threads).
+constexpr int threads_for(int tb) { return tb <= 12 ? (1 << tb) / 16 : (1 << tb) / 32; }
+
 template <bool FWD, int R, int WL>
 cudaError_t launch_pass2(const Pass2Args &a, uint64_t tiles, uint32_t n_cols, cudaStream_t st) {
-    constexpr int TS = 1 << (R + WL);
-    size_t smem = (TS + TS / 32 + (1 << R)) * 4;
-    ntt_pass2_kernel<FWD, R, WL><<<dim3((unsigned)tiles, n_cols), TS / 16, smem, st>>>(a);
+    constexpr int TB = R + WL, TS = 1 << TB, NT = threads_for(TB);
+    const size_t smem = (tw_base(TS) + (1u << R)) * 4;
+    if (smem > 48 * 1024) {  // large tiles need the opt-in shared-memory size, once per device
+        static bool attr_done[64] = {false};
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        if (dev < 0 || dev >= 64 || !attr_done[dev]) {
+            e = cudaFuncSetAttribute(ntt_tile_kernel<FWD, R, WL, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem);
+            if (e != cudaSuccess) return e;
+            if (dev >= 0 && dev < 64) attr_done[dev] = true;
+        }
+    }
+    ntt_tile_kernel<FWD, R, WL, NT><<<dim3((unsigned)tiles, n_cols), NT, smem, st>>>(a);
     return cudaGetLastError();
 }
 
+// Pass shapes the kernels are built for (ntt_plan only emits these):
+// bottom passes (WL = 0) of 4..14 layers; upper passes of 3..9 layers on
+// 2^12-element tiles (WL = 12 - R), of 10 and 11 layers on 2^13-element
+// tiles (WL = 13 - R) and of 12 layers on 2^14-element tiles (WL = 2): rows
+// of at least 16 bytes.
 template <bool FWD>
 cudaError_t dispatch_pass2(uint32_t r, uint32_t wl, const Pass2Args &a, uint64_t tiles, uint32_t n_cols,
                            cudaStream_t st) {
@@ -312,6 +431,8 @@ cudaError_t dispatch_pass2(uint32_t r, uint32_t wl, const Pass2Args &a, uint64_t
         case 10: return launch_pass2<FWD, 10, 0>(a, tiles, n_cols, st);
         case 11: return launch_pass2<FWD, 11, 0>(a, tiles, n_cols, st);
         case 12: return launch_pass2<FWD, 12, 0>(a, tiles, n_cols, st);
+        case 13: return launch_pass2<FWD, 13, 0>(a, tiles, n_cols, st);
+        case 14: return launch_pass2<FWD, 14, 0>(a, tiles, n_cols, st);
         }
     } else if (wl + r == 12) {
         switch (r) {
@@ -323,6 +444,13 @@ cudaError_t dispatch_pass2(uint32_t r, uint32_t wl, const Pass2Args &a, uint64_t
         case 8: return launch_pass2<FWD, 8, 4>(a, tiles, n_cols, st);
         case 9: return launch_pass2<FWD, 9, 3>(a, tiles, n_cols, st);
         }
+    } else if (wl + r == 13) {
+        switch (r) {
+        case 10: return launch_pass2<FWD, 10, 3>(a, tiles, n_cols, st);
+        case 11: return launch_pass2<FWD, 11, 2>(a, tiles, n_cols, st);
+        }
+    } else if (wl + r == 14 && r == 12) {
+        return launch_pass2<FWD, 12, 2>(a, tiles, n_cols, st);
     }
     return cudaErrorInvalidValue;
 }
@@ -360,8 +488,11 @@ void ntt_table_offsets(uint32_t log_n, uint32_t off[32]) {
 namespace {
 
 // Pass-plan knobs per device and transform length (in layers): the bottom
-// pass's maximum layers (10..12) and the upper passes' maximum (6..9).  The
-// autotuner writes them; every choice computes the same values.
+// pass's maximum layers (9..14) and the upper passes' maximum (3..12).  The
+// autotuner writes them; every choice computes the same values.  Larger
+// tiles (2 passes for 24 layers) measured slower than 4096-element tiles
+// with 3 passes: 32 elements per thread lose more to load latency and
+// barriers than the third pass costs in HBM traffic.
 struct PlanKnobs { uint8_t bottom, upper; };
 PlanKnobs g_knobs[64][32];
 bool g_knobs_init[64] = {false};
@@ -369,7 +500,7 @@ bool g_knobs_init[64] = {false};
 PlanKnobs knobs_for(uint32_t total) {
     int dev = 0;
     cudaGetDevice(&dev);
-    PlanKnobs k{12, 9};
+    PlanKnobs k{11, 8};  // the fastest plans measured on a B200 without tuning (3 passes for 24..27 layers)
     if (dev >= 0 && dev < 64 && g_knobs_init[dev] && total < 32 && g_knobs[dev][total].bottom) k = g_knobs[dev][total];
     return k;
 }
@@ -378,18 +509,24 @@ PlanKnobs knobs_for(uint32_t total) {
 
 // Pass plan for `total` layers (0 .. total-1): a bottom pass of up to
 // `bottom` layers on contiguous tiles (WL = 0), then passes of 3..`upper`
-// layers, sizes balanced, on tiles of 2^(12-R) contiguous columns (every tile
-// 4096 elements; rows of at least 8 words = one 32-byte sector).  An upper
-// pass starting at layer s reads rows 2^s apart, so its 2^(12-R) columns
-// must fit in one row gap: 12 - R <= s.  Transforms of at most 12 layers are
-// therefore one bottom pass, and a longer one keeps a bottom pass of at
-// least 9 layers (bottom_max >= 9; at least 10 after the 3-layer rule).
-// Transforms of fewer than 4 layers use the one-tile shared-memory kernel.
+// layers, sizes balanced.  An upper pass of R <= 9 layers runs on tiles of
+// 2^12 elements, 2^(12-R) contiguous columns (rows of at least 8 words, one
+// 32-byte sector); one of 10 or 11 layers on tiles of 2^13 elements, 2^(13-R)
+// columns; one of 12 layers on tiles of 2^14 elements, 4 columns (rows of 16
+// bytes).  An upper pass starting at layer s reads
+// rows 2^s apart, so its columns must fit in one row gap: WL <= s.  A
+// transform of at most max(12, bottom) layers is therefore one bottom pass,
+// and a longer one keeps a bottom pass of at least 9 layers (bottom_max >=
+// 9), so every WL (at most 9) fits.  Transforms of fewer than 4 layers use
+// the one-tile shared-memory kernel.
 uint32_t ntt_plan(uint32_t total, uint32_t bottom_max, uint32_t upper_max, uint32_t ps[32], uint32_t pr[32],
                   uint32_t pw[32]) {
     uint32_t np = 0;
     if (bottom_max < 9u) bottom_max = 9u;
-    uint32_t bottom = (total <= 12u || total < bottom_max) ? total : bottom_max;
+    if (bottom_max > 14u) bottom_max = 14u;
+    if (upper_max < 3u) upper_max = 3u;
+    if (upper_max > 12u) upper_max = 12u;
+    uint32_t bottom = (total <= 12u || total <= bottom_max) ? total : bottom_max;
     if (total > bottom && total - bottom < 3u) bottom = total - 3u;  // leave at least 3 layers above
     ps[np] = 0; pr[np] = bottom; pw[np] = 0; np++;
     uint32_t rest = total - bottom;
@@ -399,7 +536,7 @@ uint32_t ntt_plan(uint32_t total, uint32_t bottom_max, uint32_t upper_max, uint3
         uint32_t lo = bottom;
         for (uint32_t i = 0; i < nu; i++) {
             uint32_t r = rest / nu + (i < rest % nu ? 1u : 0u);
-            ps[np] = lo; pr[np] = r; pw[np] = 12u - r; np++;
+            ps[np] = lo; pr[np] = r; pw[np] = (r <= 9u ? 12u : r <= 11u ? 13u : 14u) - r; np++;
             lo += r;
         }
     }
@@ -494,11 +631,96 @@ cudaError_t ntt_transform_planned(uint32_t *data, uint32_t *const *dev_cols, uin
     return cudaSuccess;
 }
 
+cudaError_t ntt_transform_groups(const NttGroup *grp, uint32_t n_groups, bool forward, cudaStream_t stream,
+                                 uint32_t *launches) {
+    // groups whose transform is exactly a 12-layer bottom pass plus one upper
+    // pass of 3..9 layers (15..21 layers) share the launches; the others run
+    // as transforms of their own
+    if (n_groups > 64) return cudaErrorInvalidValue;
+    bool merge[64] = {false};
+    uint32_t n_merge = 0;
+    for (uint32_t g = 0; g < n_groups; g++) {
+        const uint32_t total = (grp[g].src && forward) ? grp[g].src_log : grp[g].log_n;
+        merge[g] = n_merge < kMaxNttGroups && grp[g].n_cols > 0 && total >= 15 && total <= 21 &&
+                   !(grp[g].src && !forward && grp[g].src_log != grp[g].log_n);
+        n_merge += merge[g];
+    }
+    for (uint32_t g = 0; g < n_groups; g++) {
+        if (merge[g] && n_merge >= 2) continue;
+        const NttGroup &G = grp[g];
+        cudaError_t e = ntt_transform(G.data, nullptr, G.col_stride, G.n_cols, G.log_n, G.tw, forward, G.src,
+                                      G.src_log, stream);
+        if (e != cudaSuccess) return e;
+        if (launches) *launches += ntt_pass_count((G.src && forward) ? G.src_log : G.log_n);
+    }
+    if (n_merge < 2) return cudaSuccess;
+    static bool attr_done[64] = {false};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const size_t smem = (tw_base(4096) + 4096) * 4;
+    if (dev < 0 || dev >= 64 || !attr_done[dev]) {
+        e = cudaFuncSetAttribute(forward ? ntt_multi_kernel<true> : ntt_multi_kernel<false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(forward ? ntt_multi_kernel<false> : ntt_multi_kernel<true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 64) attr_done[dev] = true;
+    }
+    for (uint32_t q = 0; q < 2; q++) {
+        const uint32_t pi = forward ? 1u - q : q;  // forward: the upper pass first
+        MultiPassArgs a;
+        memset(&a, 0, sizeof(a));
+        uint32_t blocks = 0;
+        for (uint32_t g = 0; g < n_groups; g++) {
+            if (!merge[g]) continue;
+            const NttGroup &G = grp[g];
+            const uint32_t total = (G.src && forward) ? G.src_log : G.log_n;
+            const uint32_t r = pi == 0 ? 12u : total - 12u, wl = pi == 0 ? 0u : 12u - r;
+            const uint32_t e2 = (30u * G.log_n) % 31u;
+            Pass2Args &p = a.g[a.n_groups];
+            p.data = G.data; p.dev_cols = nullptr; p.col_stride = G.col_stride;
+            p.src = (q == 0 && G.src) ? G.src : nullptr;
+            p.src_mask = G.src ? ((1ull << G.src_log) - 1ull) : ~0ull;
+            p.src_stride = G.src ? (1ull << G.src_log) : 0ull;
+            p.line = G.tw.line; p.circle = G.tw.circle; p.cmode = G.tw.circle_mode;
+            for (int i = 0; i < 32; i++) p.off.v[i] = G.tw.off[i];
+            p.s = pi == 0 ? 0u : 12u;
+            p.scale = (!forward && q == 1u) ? (e2 == 0 ? 1u : (1u << e2)) : 1u;
+            p.vec = ((((uintptr_t)G.data & 15u) == 0) && (G.n_cols == 1 || G.col_stride % 4u == 0) &&
+                     (!G.src || ((((uintptr_t)G.src & 15u) == 0) && G.src_log >= 2))) ? 1u : 0u;
+            a.R[a.n_groups] = r;
+            a.tiles[a.n_groups] = (uint32_t)((1ull << G.log_n) >> 12);
+            a.first[a.n_groups] = blocks;
+            blocks += a.tiles[a.n_groups] * G.n_cols;
+            a.n_groups++;
+            (void)wl;
+        }
+        a.first[a.n_groups] = blocks;
+        if (forward) ntt_multi_kernel<true><<<blocks, 256, smem, stream>>>(a);
+        else ntt_multi_kernel<false><<<blocks, 256, smem, stream>>>(a);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        if (launches) *launches += 1;
+    }
+    return cudaSuccess;
+}
+
 cudaError_t ntt_single_layer(uint32_t *data, const uint32_t *tw, uint32_t layer_idx, uint32_t log_n, bool forward,
                              cudaStream_t stream) {
     uint64_t half = (1ull << log_n) / 2;
     if (!half) return cudaSuccess;
-    ntt_layer_kernel<<<blocks_for(half, 256), 256, 0, stream>>>(data, tw, layer_idx, half, forward ? 1 : 0);
+    ntt_layer_kernel<<<blocks_for(half, 256), 256, 0, stream>>>(data, nullptr, tw, layer_idx, half, forward ? 1 : 0);
+    return cudaGetLastError();
+}
+
+cudaError_t ntt_single_layer_cols(uint32_t *const *dev_cols, uint32_t n_cols, const uint32_t *tw, uint32_t layer_idx,
+                                  uint32_t log_n, bool forward, cudaStream_t stream) {
+    uint64_t half = (1ull << log_n) / 2;
+    if (!half || !n_cols) return cudaSuccess;
+    ntt_layer_kernel<<<dim3(blocks_for(half, 256), n_cols), 256, 0, stream>>>(nullptr, dev_cols, tw, layer_idx, half,
+                                                                            forward ? 1 : 0);
     return cudaGetLastError();
 }
 

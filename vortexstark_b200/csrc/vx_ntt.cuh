@@ -43,6 +43,23 @@ cudaError_t ntt_transform_planned(uint32_t *data, uint32_t *const *dev_cols, uin
                                   uint32_t log_n, const NttTables &tw, bool forward, const uint32_t *src,
                                   uint32_t src_log, uint32_t bottom_max, uint32_t upper_max, cudaStream_t stream);
 
+// Transforms of several column groups of different lengths, for the same
+// direction: group g is n_cols columns of 2^log_n words at data + c *
+// col_stride, with its own tables and optional source (as ntt_transform).
+// Groups of 15..21 applied layers share one launch per pass (a 12-layer
+// bottom pass and one upper pass); the others run as their own transforms.
+// `launches` (if non-null) is increased by the kernels enqueued.
+struct NttGroup {
+    uint32_t *data;
+    uint64_t col_stride;
+    uint32_t n_cols, log_n;
+    NttTables tw;
+    const uint32_t *src;
+    uint32_t src_log;
+};
+cudaError_t ntt_transform_groups(const NttGroup *groups, uint32_t n_groups, bool forward, cudaStream_t stream,
+                                 uint32_t *launches);
+
 // Kernel launches of a transform that applies `layers` layers.
 uint32_t ntt_pass_count(uint32_t layers);
 
@@ -60,6 +77,9 @@ void ntt_knobs_get(uint32_t total, uint32_t *bottom_max, uint32_t *upper_max);
 // One butterfly layer over the whole array (reference cuda_circle_ntt_layer).
 cudaError_t ntt_single_layer(uint32_t *data, const uint32_t *tw, uint32_t layer_idx, uint32_t log_n, bool forward,
                              cudaStream_t stream);
+// The same layer over n_cols columns given as a device array of pointers.
+cudaError_t ntt_single_layer_cols(uint32_t *const *dev_cols, uint32_t n_cols, const uint32_t *tw, uint32_t layer_idx,
+                                  uint32_t log_n, bool forward, cudaStream_t stream);
 
 // Reference table layout for a coset of 2^log_n points: line twiddles
 // (2^log_n - 1 words) and circle twiddles (2^(log_n-1) words); offsets of

@@ -60,8 +60,10 @@ void proof_layout(uint32_t log_n, uint32_t blowup, uint32_t nq, ProofLayout *L) 
 
 // Constant words of the layout (everything except a, b, roots, last layer,
 // query indices, values and path hashes).
-static void proof_template(const ProofLayout &L, std::vector<uint32_t> &t) {
-    t.assign(L.words, 0u);
+// `t` holds L.words words; both the allocating path and the no-allocation
+// entry point fill their staging buffer here.
+static void proof_template(const ProofLayout &L, uint32_t *t) {
+    memset(t, 0, (size_t)L.words * 4);
     t[L.magic] = 0x4B52414Bu; t[L.magic + 1] = 1u; t[L.magic + 2] = L.log_n;
     t[L.nfri_w] = L.nfri;
     t[L.nlast] = 8u;
@@ -510,8 +512,8 @@ extern "C" int vx_prover_create(uint32_t log_n, uint32_t blowup_bits, uint32_t n
     S.alpha_f = b + o_af;
     S.qidx = b + o_qi;
     S.proof = b + o_proof;
-    std::vector<uint32_t> tmpl;
-    proof_template(L, tmpl);
+    std::vector<uint32_t> tmpl(L.words);
+    proof_template(L, tmpl.data());
     cudaError_t e = cudaMemcpy(S.proof, tmpl.data(), L.words * 4, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(S.chan, 0, sizeof(DevChannel));
     if (e == cudaSuccess) e = tree_reset(S.trace_lv, nullptr);
@@ -864,6 +866,8 @@ extern "C" int vx_prove_fib_batch(const uint32_t *a, const uint32_t *b, uint32_t
 }
 
 extern "C" void vx_release_all(void) {
+    // the forge batch launchers' column-pointer arrays
+    forge_cols_release();
     // the cached slots of vx_prove_fib and vx_prove_fib_batch; each size's
     // tables go with their last slot
     std::lock_guard<std::mutex> lk(g_slot_mu);
@@ -876,14 +880,16 @@ extern "C" void vx_release_all(void) {
 // ---------------------------------------------------------------------
 // vx_prove_fib_noalloc: the whole proof without any device allocation.
 //
-// For callers that may not allocate device memory: code running inside a
-// stream capture or a CUDA graph being built, hosts whose device memory is
+// For callers that cannot call cudaMalloc: hosts whose device memory is
 // owned by another allocator (a Rust arena, a framework's caching pool) and
 // sandboxes that forbid cudaMalloc after start-up.  Every byte of device
 // scratch — generator tables, twiddle tables, the LDE, FRI layers, stored
 // tree levels, transcript state and the proof — lives in one file-scope
 // static __device__ array of kNoAllocWords words (8 MiB), which every GPU
-// that loads this library keeps until the process exits.
+// that loads this library keeps until the process exits.  Each call copies
+// synchronously and runs on the legacy default stream, so it must not be
+// called while a stream capture is active.  g_na_mu serialises the calls:
+// they share the array, which keeps the last call's contents.
 // ---------------------------------------------------------------------
 namespace {
 constexpr uint64_t kNoAllocWords = 1ull << 21;   // 8 MiB of device scratch
@@ -996,23 +1002,7 @@ extern "C" int vx_prove_fib_noalloc(uint32_t a, uint32_t b, uint32_t log_n, uint
         D.tab_blowup = blowup_bits;
     }
     // the proof's constant words; everything else is overwritten by the stages
-    memset(g_na_proof_tmpl, 0, L.words * 4);
-    {
-        g_na_proof_tmpl[L.magic] = 0x4B52414Bu; g_na_proof_tmpl[L.magic + 1] = 1u; g_na_proof_tmpl[L.magic + 2] = log_n;
-        g_na_proof_tmpl[L.nfri_w] = L.nfri;
-        g_na_proof_tmpl[L.nlast] = 8u;
-        g_na_proof_tmpl[L.nq_w] = L.nq;
-        auto dec = [&](const DecomLayout &d) {
-            g_na_proof_tmpl[d.n] = L.nq;
-            for (uint32_t q = 0; q < L.nq; q++) {
-                g_na_proof_tmpl[d.paths + (uint64_t)q * (1 + 8ull * d.depth)] = d.depth;
-                g_na_proof_tmpl[d.spaths + (uint64_t)q * (1 + 8ull * d.depth)] = d.depth;
-            }
-        };
-        dec(L.trace); dec(L.quot);
-        g_na_proof_tmpl[L.nfd] = L.nfri;
-        for (uint32_t k = 0; k < L.nfri; k++) dec(L.fri[k]);
-    }
+    proof_template(L, g_na_proof_tmpl);
     VX_CUDA_TRY(cudaMemcpy(S.proof, g_na_proof_tmpl, L.words * 4, cudaMemcpyHostToDevice));
     uint32_t launches = 0;
     for (uint32_t stage = 0; stage < VX_N_STAGES; stage++) {

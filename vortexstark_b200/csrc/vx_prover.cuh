@@ -68,4 +68,6 @@ uint32_t prover_log_n(const vx_prover *p);
 void prover_footprint(uint32_t log_n, uint32_t blowup, uint32_t nq, size_t *slot_b, size_t *tab_b);
 size_t prover_proof_bytes(const vx_prover *p);
 const uint32_t *prover_chan_err(const vx_prover *p);
+// Frees the forge batch launchers' per-device column-pointer arrays.
+void forge_cols_release();
 }  // namespace vx

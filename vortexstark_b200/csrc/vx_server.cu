@@ -13,13 +13,18 @@
 // proof's own kernels stay in order; every proof is computed by the same
 // kernels on its own buffers, so its bytes do not depend on what else runs.
 //
-// Scheduling policy.  A proof with an evaluation domain of 2^24 points or
-// more fills every SM by itself for most of its kernels, so two of them in
-// flight only split the GPU and both finish later: at most one such "large"
-// proof is admitted at a time (others wait in the queue, oldest first).
-// Smaller proofs are chains of short kernels that leave most SMs idle; their
-// streams get the device's highest priority so their blocks are dispatched
-// ahead of a large proof's waiting blocks and fill the gaps it leaves.
+// Scheduling policy (vx_server_set_policy).  A proof whose evaluation
+// domain has at least 2^large_log_eval points (default 2^24) fills every SM
+// by itself for most of its kernels, so two of them in flight only split the
+// GPU and both finish later: at most `max_large` such proofs (default 1) are
+// admitted at a time, others wait in the queue, oldest first.  Smaller
+// proofs are chains of short kernels that leave most SMs idle.  Stream
+// priorities decide whose blocks the hardware dispatches first when both
+// wait: by default small proofs run on the highest-priority streams, so
+// their blocks are dispatched ahead of a large proof's waiting blocks and
+// fill the gaps it leaves; the reverse order keeps a large proof close to
+// its solo time.  `small_cap` optionally bounds the small proofs in flight
+// while a large one is.
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -46,9 +51,12 @@ struct Request {
     uint64_t submit_ns;
 };
 
-// Evaluation domains of at least 2^kLargeLogEval points fill the GPU alone.
+// Default policy: evaluation domains of at least 2^24 points fill the GPU
+// alone; one such proof in flight; small proofs on the highest-priority
+// streams; no cap on small proofs.
 constexpr uint32_t kLargeLogEval = 24;
 constexpr uint32_t kMaxLargeInflight = 1;
+constexpr int kPrioDefault = 0;
 
 struct Slot {
     vx_prover *p = nullptr;
@@ -80,7 +88,12 @@ struct vx_server {
     std::thread worker;
     bool stop = false;
     size_t budget = 0, used = 0;
-    uint32_t max_inflight = 1, inflight = 0, large_inflight = 0, blowup = 2, nq = 80;
+    uint32_t max_inflight = 1, inflight = 0, large_inflight = 0, small_inflight = 0, blowup = 2, nq = 80;
+    // policy (vx_server_set_policy)
+    uint32_t large_log_eval = kLargeLogEval, max_large = kMaxLargeInflight, small_cap = 0;
+    bool large_per_size = false;               // max_large counts per size instead of overall
+    std::map<uint32_t, uint32_t> large_by_size;  // large proofs in flight per log_n
+    int prio_mode = kPrioDefault;  // 0: small proofs highest, 1: all equal, 2: large proofs highest, 3: graded
     int device = 0;
     bool use_graphs = true;
     int fatal = VX_OK;
@@ -110,11 +123,18 @@ int slot_create(vx_server *s, uint32_t log_n, Slot **out) {
         return VX_ERR_CUDA;
     };
     cudaError_t e;
-    sl->large = log_n + s->blowup >= kLargeLogEval;
+    sl->large = log_n + s->blowup >= s->large_log_eval;
     int prio_least = 0, prio_greatest = 0;
     if ((e = cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest)) != cudaSuccess) return fail("priorities", e);
-    if ((e = cudaStreamCreateWithPriority(&sl->st, cudaStreamNonBlocking, sl->large ? prio_least : prio_greatest)) !=
-        cudaSuccess)
+    int prio = prio_least;
+    if (s->prio_mode == 0) prio = sl->large ? prio_least : prio_greatest;
+    if (s->prio_mode == 2) prio = sl->large ? prio_greatest : prio_least;
+    if (s->prio_mode == 3) {  // graded: the two sizes below the large threshold in between
+        const uint32_t le = log_n + s->blowup;
+        prio = le >= s->large_log_eval ? prio_least
+               : le + 2 >= s->large_log_eval ? (prio_least + prio_greatest) / 2 : prio_greatest;
+    }
+    if ((e = cudaStreamCreateWithPriority(&sl->st, cudaStreamNonBlocking, prio)) != cudaSuccess)
         return fail("stream", e);
     if ((e = cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming)) != cudaSuccess) return fail("event", e);
     // proof bytes, then the transcript status word
@@ -156,7 +176,8 @@ int launch(vx_server *s, Slot *sl, const Request &r) {
     sl->req = r;
     sl->start_ns = now_ns();
     s->inflight++;
-    if (sl->large) s->large_inflight++;
+    if (sl->large) { s->large_inflight++; s->large_by_size[sl->log_n]++; }
+    else s->small_inflight++;
     if (sl->exec) {
         sl->pinned_ab[0] = r.a;
         sl->pinned_ab[1] = r.b;
@@ -206,7 +227,8 @@ void worker_loop(vx_server *s) {
             s->completed.push_back(c);
             sl->busy = false;
             s->inflight--;
-            if (sl->large) s->large_inflight--;
+            if (sl->large) { s->large_inflight--; s->large_by_size[sl->log_n]--; }
+            else s->small_inflight--;
             progress = true;
         }
         // admit queued requests, oldest first, skipping ones that cannot start
@@ -216,8 +238,13 @@ void worker_loop(vx_server *s) {
         // so an index keeps naming the same request.
         for (size_t qi = 0; qi < s->pending.size() && s->inflight < s->max_inflight;) {
             const uint32_t log_n = s->pending[qi].log_n;
-            if (log_n + s->blowup >= kLargeLogEval && s->large_inflight >= kMaxLargeInflight) {
+            const bool large = log_n + s->blowup >= s->large_log_eval;
+            if (large && (s->large_per_size ? s->large_by_size[log_n] : s->large_inflight) >= s->max_large) {
                 ++qi;  // a large proof is running: this one waits, smaller ones behind it may start
+                continue;
+            }
+            if (!large && s->small_cap && s->large_inflight && s->small_inflight >= s->small_cap) {
+                ++qi;  // small proofs at their cap beside a large one
                 continue;
             }
             Slot *free_slot = nullptr;
@@ -287,6 +314,24 @@ extern "C" int vx_server_create(size_t budget_bytes, uint32_t max_inflight, uint
     s->use_graphs = use_graphs != 0;
     s->worker = std::thread(worker_loop, s);
     *out = s;
+    return VX_OK;
+}
+
+extern "C" int vx_server_set_policy(vx_server *s, uint32_t large_log_eval, uint32_t max_large, int priority,
+                                    uint32_t small_cap, int large_per_size) {
+    VX_CHECK_ARG(s != nullptr, "vx_server_set_policy: null server");
+    VX_CHECK_ARG(large_log_eval >= 1 && large_log_eval <= 32, "vx_server_set_policy: bad large_log_eval %u",
+                 large_log_eval);
+    VX_CHECK_ARG(max_large >= 1, "vx_server_set_policy: max_large must be at least 1");
+    VX_CHECK_ARG(priority >= 0 && priority <= 3, "vx_server_set_policy: priority must be 0, 1, 2 or 3");
+    std::lock_guard<std::mutex> lk(s->mu);
+    VX_CHECK_ARG(s->slots.empty() && s->pending.empty(),
+                 "vx_server_set_policy: call before the first prewarm or submit (slot streams keep their priority)");
+    s->large_log_eval = large_log_eval;
+    s->max_large = max_large;
+    s->large_per_size = large_per_size != 0;
+    s->prio_mode = priority;
+    s->small_cap = small_cap;
     return VX_OK;
 }
 

@@ -56,8 +56,8 @@ extern "C" int vx_tune_set(uint32_t kind, uint32_t layers, uint32_t a, uint32_t 
     if (kind == 0) {
         // a = 0 restores the default; a bottom pass of at least 9 layers lets
         // every upper pass's columns fit between its rows
-        VX_CHECK_ARG(a == 0 || (a >= 9 && a <= 12 && b >= 3 && b <= 9),
-                     "vx_tune_set: NTT plan needs bottom 9..12 and upper 3..9 (or 0 for the default)");
+        VX_CHECK_ARG(a == 0 || (a >= 9 && a <= 14 && b >= 3 && b <= 12),
+                     "vx_tune_set: NTT plan needs bottom 9..14 and upper 3..12 (or 0 for the default)");
         ntt_knobs_set(dev, layers, a, b);
     } else if (kind == 1 || kind == 2) {
         VX_CHECK_ARG(a <= 4, "vx_tune_set: leaf subtree log must be 0 (default) .. 4");
@@ -85,8 +85,8 @@ extern "C" int vx_tune_get(uint32_t kind, uint32_t layers, uint32_t *a, uint32_t
 extern "C" int vx_ntt_plan(uint32_t total, uint32_t bottom_max, uint32_t upper_max, uint32_t starts[32],
                            uint32_t layers[32], uint32_t tile_cols_log[32], uint32_t *n_passes) {
     VX_CHECK_ARG(total >= 4 && total <= 31, "vx_ntt_plan: total %u outside 4..31", total);
-    VX_CHECK_ARG(bottom_max >= 9 && bottom_max <= 12 && upper_max >= 3 && upper_max <= 9,
-                 "vx_ntt_plan: bottom 9..12 and upper 3..9");
+    VX_CHECK_ARG(bottom_max >= 9 && bottom_max <= 14 && upper_max >= 3 && upper_max <= 12,
+                 "vx_ntt_plan: bottom 9..14 and upper 3..12");
     VX_CHECK_ARG(starts && layers && tile_cols_log && n_passes, "vx_ntt_plan: null output");
     *n_passes = ntt_plan(total, bottom_max, upper_max, starts, layers, tile_cols_log);
     return VX_OK;
@@ -121,10 +121,10 @@ extern "C" int vx_autotune(uint32_t max_log, char *report, size_t cap) {
         NttTables tw{tab, tab + n, {}, 0u};
         ntt_table_offsets(total, tw.off);
         float best = 1e30f;
-        uint32_t bb = 12, bu = 9;
+        uint32_t bb = 12, bu = 12;
         std::vector<std::vector<uint32_t>> seen;
-        for (uint32_t bottom = 10; bottom <= 12; bottom++)
-            for (uint32_t upper = 6; upper <= 9; upper++) {
+        for (uint32_t bottom = 10; bottom <= 14; bottom++)
+            for (uint32_t upper = 6; upper <= 12; upper++) {
                 uint32_t ps[32], pr[32], pw[32];
                 uint32_t np = ntt_plan(total, bottom, upper, ps, pr, pw);
                 std::vector<uint32_t> key(pr, pr + np);

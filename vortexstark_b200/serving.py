@@ -33,6 +33,16 @@ class ProofServer:
         _lib.check(_lib.lib().vx_server_create(int(budget_bytes), max_inflight, blowup_bits, n_queries,
                                                1 if use_graphs else 0, C.byref(self._s)))
 
+    def set_policy(self, large_log_eval: int = 24, max_large: int = 1, priority: int = 0,
+                   small_cap: int = 0, large_per_size: bool = False) -> None:
+        """Scheduling policy (before the first prewarm or submit): proofs of at
+        least 2^large_log_eval evaluation points are large, at most max_large
+        of them in flight (per size if large_per_size); priority 0 = small
+        proofs first, 1 = equal, 2 = large proofs first, 3 = graded by size;
+        small_cap bounds small proofs in flight beside a large one (0 = none)."""
+        _lib.check(_lib.lib().vx_server_set_policy(self._s, large_log_eval, max_large, priority, small_cap,
+                                                   1 if large_per_size else 0))
+
     def prewarm(self, log_n: int, count: int) -> None:
         _lib.check(_lib.lib().vx_server_prewarm(self._s, log_n, count))
 
@@ -100,11 +110,21 @@ def poisson_arrivals(n: int, rate: float, seed: int):
     return out
 
 
-def _summary(lat_ms, makespan_s, n):
+def _pct(sorted_vals, q):
+    return sorted_vals[min(len(sorted_vals) - 1, int(round(q * (len(sorted_vals) - 1))))]
+
+
+def _summary(lat_ms, makespan_s, n, sizes=None):
     lat = sorted(lat_ms)
-    p99 = lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))]
-    return {"proofs_per_s": n / makespan_s, "p50_ms": statistics.median(lat), "p99_ms": p99,
-            "mean_ms": statistics.fmean(lat), "makespan_s": makespan_s, "n": n}
+    out = {"proofs_per_s": n / makespan_s, "p50_ms": statistics.median(lat), "p99_ms": _pct(lat, 0.99),
+           "mean_ms": statistics.fmean(lat), "makespan_s": makespan_s, "n": n, "lat_ms": list(lat_ms)}
+    if sizes is not None:
+        by = {}
+        for ln in sorted(set(sizes)):
+            v = sorted(x for x, s in zip(lat_ms, sizes) if s == ln)
+            by[str(ln)] = {"n": len(v), "p50_ms": statistics.median(v), "p99_ms": _pct(v, 0.99)}
+        out["by_log_n"] = by
+    return out
 
 
 def run_stream(server: ProofServer, requests, arrivals, keep_results: bool = False):
@@ -146,7 +166,7 @@ def run_stream(server: ProofServer, requests, arrivals, keep_results: bool = Fal
             got += 1
     th.join()
     done.set()
-    s = _summary(lat, (last_done - t0) / 1e9, n)
+    s = _summary(lat, (last_done - t0) / 1e9, n, [r[0] for r in requests])
     return s, results
 
 
@@ -177,4 +197,4 @@ def run_sequential(requests, arrivals, blowup_bits: int = 2, n_queries: int = 80
         start_wait = t0 + at
         prover.prove_cached_bytes(a, b, caches[log_n])
         lat.append((time.perf_counter() - start_wait) * 1e3)
-    return _summary(lat, time.perf_counter() - t0, n)
+    return _summary(lat, time.perf_counter() - t0, n, [r[0] for r in requests])

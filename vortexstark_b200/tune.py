@@ -32,7 +32,7 @@ def autotune(max_log: int = 24) -> dict:
 
 def set_ntt_plan(layers: int, bottom: int = 0, upper: int = 0) -> None:
     """Plan of ``layers``-layer transforms: bottom pass of at most ``bottom``
-    layers (9..12), upper passes of at most ``upper`` (3..9); 0 = default."""
+    layers (9..14), upper passes of at most ``upper`` (3..12); 0 = default."""
     _lib.check(_lib.lib().vx_tune_set(NTT_PLAN, layers, bottom, upper))
 
 
