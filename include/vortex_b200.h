@@ -480,7 +480,7 @@ int vx_fri_chain_fetch(vx_fri_chain *h, uint32_t *roots, uint32_t *alphas, uint3
 /* Autotuner — no counterpart in the reference, whose kernels have fixed
  * shapes (circle_ntt.cu: one launch per layer; blake2s.cu: one leaf per
  * thread).  On the current device, times every distinct NTT pass plan
- * (bottom pass of 10..12 layers, upper passes of at most 6..9) of each
+ * (bottom pass of 10..14 layers, upper passes of at most 6..12) of each
  * transform length 13..max_log (shorter ones are a single pass), and the
  * Merkle leaf kernel's subtree size (2^1..2^4 leaves per thread) of each tree
  * depth 17..max_log, separately for narrow leaves (M31 columns) and for wide
@@ -496,9 +496,11 @@ int vx_fri_chain_fetch(vx_fri_chain *h, uint32_t *roots, uint32_t *alphas, uint3
  * (cap bytes, NUL-terminated, truncated).  12 <= max_log <= 28.  Not safe
  * to run while other host threads launch on the same device. */
 int vx_autotune(uint32_t max_log, char *report, size_t cap);
-/* Set one knob on the current device.  kind 0: NTT plan of `layers`-layer
- * transforms, a = bottom pass maximum (9..12), b = upper pass maximum
- * (3..9), a = 0 restores the default (12, 9).  kind 1: leaf kernel subtree
+/* Set one knob on the current device.  kind 0: NTT plan of transforms over
+ * 2^`layers` elements (applied to the layers such a transform runs; an LDE
+ * of 2^26 points from 2^24 coefficients runs 24 layers under the 2^26
+ * plan), a = bottom pass maximum (9..14), b = upper pass maximum (3..12),
+ * a = 0 restores the default (11, 8).  kind 1: leaf kernel subtree
  * log for narrow-leaf trees of depth `layers`, a in 1..4, 0 restores the
  * default; kind 2: the same for wide-leaf trees (FRI layers, lifted rows,
  * their combinations). */

@@ -97,3 +97,18 @@ def test_plain_launches_without_graphs():
         summary, results = run_stream(srv, reqs, [0.0] * len(reqs), keep_results=True)
     for i, (log_n, a, b) in enumerate(reqs):
         assert results[i] == prover.prove_bytes(a, b, log_n)
+
+
+def test_multi_engine_router_equals_alone(oracle):
+    """The multi-GPU request loop's router over two engines (here both on
+    GPU 0; a node gives each its own GPU): every proof equals the same
+    request proved alone, whichever engine ran it."""
+    from vortexstark_b200.serving import MultiGpuServer
+
+    reqs = _stream(23, 24, [10, 12, 14, 16])
+    with MultiGpuServer([0, 0], budget_bytes=4 << 30, max_inflight=8) as srv:
+        summary, results = run_stream(srv, reqs, poisson_arrivals(len(reqs), 3000.0, 2), keep_results=True)
+    assert summary["n"] == len(reqs)
+    for i, (log_n, a, b) in enumerate(reqs):
+        assert results[i] == prover.prove_bytes(a, b, log_n), (i, log_n)
+    assert results[0] == oracle.prove(reqs[0][1], reqs[0][2], reqs[0][0])

@@ -121,6 +121,7 @@ struct Pass2Args {
     uint32_t s;       // lowest layer of the pass
     uint32_t scale;   // output scale (1 = none)
     uint32_t vec;     // 1: columns and source 16-byte aligned, 4 consecutive elements per access
+    uint32_t hb_log;  // > 0: the 2^hb_log tiles that read the same source tile are consecutive blocks
 };
 
 // Butterfly products: with a doubled twiddle (mmul_t2: one multiply, one
@@ -230,8 +231,14 @@ __device__ __forceinline__ void run_stages(uint32_t *sm, const uint32_t *smtw, u
     }
 }
 
-// Up to 1024 resident threads per SM: 64 registers a thread.
-constexpr int min_blocks_for(int nt) { return (1024 / nt) < 32 ? (1024 / nt) : 32; }
+// Resident threads per SM the pass kernels are compiled for (registers per
+// thread = 65536 / this).
+#ifndef VX_NTT_THREADS_PER_SM
+#define VX_NTT_THREADS_PER_SM 1024
+#endif
+constexpr int min_blocks_for(int nt) {
+    return (VX_NTT_THREADS_PER_SM / nt) < 32 ? (VX_NTT_THREADS_PER_SM / nt) : 32;
+}
 
 // One tile of one column: tile index `tile` of column `ci`.
 template <bool FWD, int R, int WL, int NT>
@@ -243,9 +250,15 @@ __device__ __forceinline__ void tile_pass(const Pass2Args &p, uint64_t tile, uin
     uint32_t *smtw = dsm + tw_base(TS);          // 2^R words: layer j's twiddles at [2^(R-1-j), 2^(R-j))
     const uint32_t tid = threadIdx.x;
     const uint32_t s = p.s;
+    // tile = (hb, cb): the high index bits above the pass and the column
+    // block.  Column blocks are consecutive by default (neighbouring blocks
+    // share DRAM pages); the first pass of an LDE, whose hb values above the
+    // source's length are replicas reading the same source tile, puts those
+    // replicas in consecutive blocks so the source comes from L2 after its
+    // first read.
     const uint32_t cshift = s - WL;
-    const uint64_t cb = tile & ((1ull << cshift) - 1ull);
-    const uint64_t hb = tile >> cshift;
+    const uint64_t cb = p.hb_log ? tile >> p.hb_log : tile & ((1ull << cshift) - 1ull);
+    const uint64_t hb = p.hb_log ? tile & ((1ull << p.hb_log) - 1ull) : tile >> cshift;
     uint32_t *col = p.dev_cols ? p.dev_cols[ci] : p.data + (uint64_t)ci * p.col_stride;
     const uint32_t *in = p.src ? p.src + (uint64_t)ci * p.src_stride : col;
     const uint64_t gbase = (hb << (s + R)) | (cb << WL);
@@ -487,7 +500,7 @@ void ntt_table_offsets(uint32_t log_n, uint32_t off[32]) {
 
 namespace {
 
-// Pass-plan knobs per device and transform length (in layers): the bottom
+// Pass-plan knobs per device and transform length (log2 of the elements): the bottom
 // pass's maximum layers (9..14) and the upper passes' maximum (3..12).  The
 // autotuner writes them; every choice computes the same values.  Larger
 // tiles (2 passes for 24 layers) measured slower than 4096-element tiles
@@ -559,17 +572,21 @@ void ntt_knobs_get(uint32_t total, uint32_t *bottom, uint32_t *upper) {
 }
 
 namespace {
-uint32_t plan_passes(uint32_t total, uint32_t ps[32], uint32_t pr[32], uint32_t pw[32]) {
-    PlanKnobs k = knobs_for(total);
+// The knobs are looked up by the transform's length in elements (2^log_n),
+// which sets its memory regime (an LDE applies 24 layers to 2^26 elements
+// in HBM, an interpolation of 2^24 elements stays in L2), and applied to
+// the `total` layers it runs.
+uint32_t plan_passes(uint32_t total, uint32_t log_n, uint32_t ps[32], uint32_t pr[32], uint32_t pw[32]) {
+    PlanKnobs k = knobs_for(log_n);
     return ntt_plan(total, k.bottom, k.upper, ps, pr, pw);
 }
 }  // namespace
 
-uint32_t ntt_pass_count(uint32_t layers) {
+uint32_t ntt_pass_count(uint32_t layers, uint32_t log_n) {
     if (layers == 0) return 0;
     if (layers < 4) return 1;
     uint32_t ps[32], pr[32], pw[32];
-    return plan_passes(layers, ps, pr, pw);
+    return plan_passes(layers, log_n ? log_n : layers, ps, pr, pw);
 }
 
 cudaError_t ntt_transform(uint32_t *data, uint32_t *const *dev_cols, uint64_t col_stride, uint32_t n_cols,
@@ -607,7 +624,8 @@ cudaError_t ntt_transform_planned(uint32_t *data, uint32_t *const *dev_cols, uin
         return cudaGetLastError();
     }
     uint32_t ps[32], pr[32], pw[32];
-    const uint32_t np = bottom_max ? ntt_plan(total, bottom_max, upper_max, ps, pr, pw) : plan_passes(total, ps, pr, pw);
+    const uint32_t np =
+        bottom_max ? ntt_plan(total, bottom_max, upper_max, ps, pr, pw) : plan_passes(total, log_n, ps, pr, pw);
     // 16-byte accesses of 4 consecutive elements: contiguous columns with
     // 16-byte aligned bases (a device pointer array is not inspected on the
     // host, so it keeps the scalar form), a source of at least 4 words
@@ -623,6 +641,8 @@ cudaError_t ntt_transform_planned(uint32_t *data, uint32_t *const *dev_cols, uin
         a.s = ps[i];
         a.scale = (!forward && q == np - 1u) ? inv_n : 1u;
         a.vec = (vec && (pw[i] >= 2u || ps[i] == 0u)) ? 1u : 0u;
+        // the first forward pass of an LDE reads each source tile for 2^(log_n - src_log) replicas
+        a.hb_log = (q == 0 && src && forward && log_n > src_log && ps[i] + pr[i] == src_log) ? log_n - src_log : 0u;
         uint64_t tiles = (1ull << log_n) >> (pr[i] + pw[i]);
         e = forward ? dispatch_pass2<true>(pr[i], pw[i], a, tiles, n_cols, stream)
                     : dispatch_pass2<false>(pr[i], pw[i], a, tiles, n_cols, stream);
@@ -651,7 +671,7 @@ cudaError_t ntt_transform_groups(const NttGroup *grp, uint32_t n_groups, bool fo
         cudaError_t e = ntt_transform(G.data, nullptr, G.col_stride, G.n_cols, G.log_n, G.tw, forward, G.src,
                                       G.src_log, stream);
         if (e != cudaSuccess) return e;
-        if (launches) *launches += ntt_pass_count((G.src && forward) ? G.src_log : G.log_n);
+        if (launches) *launches += ntt_pass_count((G.src && forward) ? G.src_log : G.log_n, G.log_n);
     }
     if (n_merge < 2) return cudaSuccess;
     static bool attr_done[64] = {false};
@@ -690,6 +710,8 @@ cudaError_t ntt_transform_groups(const NttGroup *grp, uint32_t n_groups, bool fo
             p.scale = (!forward && q == 1u) ? (e2 == 0 ? 1u : (1u << e2)) : 1u;
             p.vec = ((((uintptr_t)G.data & 15u) == 0) && (G.n_cols == 1 || G.col_stride % 4u == 0) &&
                      (!G.src || ((((uintptr_t)G.src & 15u) == 0) && G.src_log >= 2))) ? 1u : 0u;
+            p.hb_log = (q == 0 && G.src && forward && G.log_n > G.src_log && p.s + r == G.src_log)
+                           ? G.log_n - G.src_log : 0u;
             a.R[a.n_groups] = r;
             a.tiles[a.n_groups] = (uint32_t)((1ull << G.log_n) >> 12);
             a.first[a.n_groups] = blocks;

@@ -60,8 +60,9 @@ struct NttGroup {
 cudaError_t ntt_transform_groups(const NttGroup *groups, uint32_t n_groups, bool forward, cudaStream_t stream,
                                  uint32_t *launches);
 
-// Kernel launches of a transform that applies `layers` layers.
-uint32_t ntt_pass_count(uint32_t layers);
+// Kernel launches of a transform that applies `layers` layers to 2^log_n
+// elements (log_n = 0: as many elements as layers).
+uint32_t ntt_pass_count(uint32_t layers, uint32_t log_n = 0);
 
 // Pass plan of a `total`-layer transform for a bottom pass of at most
 // bottom_max (9..12) layers and upper passes of at most upper_max (3..9):
@@ -69,10 +70,11 @@ uint32_t ntt_pass_count(uint32_t layers);
 // Transforms of at most 12 layers are one pass.
 uint32_t ntt_plan(uint32_t total, uint32_t bottom_max, uint32_t upper_max, uint32_t ps[32], uint32_t pr[32],
                   uint32_t pw[32]);
-// Per-device plan choice for `total`-layer transforms (default 12 / 9);
-// every choice computes the same values.
-void ntt_knobs_set(int dev, uint32_t total, uint32_t bottom_max, uint32_t upper_max);
-void ntt_knobs_get(uint32_t total, uint32_t *bottom_max, uint32_t *upper_max);
+// Per-device plan choice for transforms over 2^log_n elements (default 11 /
+// 8), applied to the layers such a transform runs; every choice computes
+// the same values.
+void ntt_knobs_set(int dev, uint32_t log_n, uint32_t bottom_max, uint32_t upper_max);
+void ntt_knobs_get(uint32_t log_n, uint32_t *bottom_max, uint32_t *upper_max);
 
 // One butterfly layer over the whole array (reference cuda_circle_ntt_layer).
 cudaError_t ntt_single_layer(uint32_t *data, const uint32_t *tw, uint32_t layer_idx, uint32_t log_n, bool forward,

@@ -555,7 +555,7 @@ static int enqueue_stage(vx_prover *p, uint32_t stage, uint32_t a, uint32_t b, c
     const uint64_t n = 1ull << log_n, N = 1ull << le;
     uint32_t *proof = S.proof;
     LeafQuotient lq{S.eval, N - 1, S.alpha_q, {0, 0, 0, 0}};
-    auto ntt_launches = [](uint32_t layers) { return ntt_pass_count(layers); };
+    auto ntt_launches = [](uint32_t layers, uint32_t elems_log) { return ntt_pass_count(layers, elems_log); };
     switch (stage) {
     case 0:
         VX_CUDA_TRY(cudaMemsetAsync(S.chan, 0, sizeof(DevChannel), st));
@@ -567,14 +567,14 @@ static int enqueue_stage(vx_prover *p, uint32_t stage, uint32_t a, uint32_t b, c
         NttTables it{T.itw_line, T.itw_circle, {}};
         memcpy(it.off, T.itw_off, sizeof(it.off));
         VX_CUDA_TRY(ntt_transform(S.coeffs, nullptr, 0, 1, log_n, it, false, nullptr, 0, st));
-        *launches += ntt_launches(log_n);
+        *launches += ntt_launches(log_n, log_n);
         break;
     }
     case 2: {
         NttTables ft{T.ftw_line, T.ftw_circle, {}};
         memcpy(ft.off, T.ftw_off, sizeof(ft.off));
         VX_CUDA_TRY(ntt_transform(S.eval, nullptr, 0, 1, le, ft, true, S.coeffs, log_n, st));
-        *launches += ntt_launches(log_n);
+        *launches += ntt_launches(log_n, le);
         break;
     }
     case 3:

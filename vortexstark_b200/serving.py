@@ -198,3 +198,104 @@ def run_sequential(requests, arrivals, blowup_bits: int = 2, n_queries: int = 80
         prover.prove_cached_bytes(a, b, caches[log_n])
         lat.append((time.perf_counter() - start_wait) * 1e3)
     return _summary(lat, time.perf_counter() - t0, n, [r[0] for r in requests])
+
+
+class MultiGpuServer:
+    """One serving engine per GPU behind a host router: the request loop of a
+    node with several GPUs (no traffic between GPUs; every proof runs on one
+    device).  A request goes to the device with the least outstanding work,
+    counted as the evaluation points (2^(log_n + blowup_bits)) of its
+    admitted, unfinished requests, so a GPU busy with a large proof takes the
+    next small ones elsewhere.  Tags are global; completions and proof bytes
+    come back from whichever device ran the request.
+
+    ``server_factory(device, **kw)`` builds one engine; the default builds a
+    ProofServer with that device current (its dispatcher thread keeps it)."""
+
+    def __init__(self, devices, budget_bytes: int, max_inflight: int = 24, blowup_bits: int = 2,
+                 n_queries: int = 80, use_graphs: bool = True, server_factory=None):
+        if not devices:
+            raise ValueError("MultiGpuServer needs at least one device")
+        self._blowup_bits = blowup_bits
+        factory = server_factory or _device_server
+        self._servers = [factory(d, budget_bytes=budget_bytes, max_inflight=max_inflight, blowup_bits=blowup_bits,
+                                 n_queries=n_queries, use_graphs=use_graphs) for d in devices]
+        self._devices = list(devices)
+        self._load = [0] * len(self._servers)
+        self._where = {}    # tag -> server index, until its result is taken
+        self._weight = {}   # tag -> points counted in _load, until it completes
+        self._lock = threading.Lock()
+
+    def pick(self, log_n: int) -> int:
+        """Index of the device that takes the next request (least outstanding points; lowest index on ties)."""
+        with self._lock:
+            return min(range(len(self._load)), key=lambda i: (self._load[i], i))
+
+    def submit(self, tag: int, log_n: int, a: int, b: int) -> int:
+        w = 1 << (log_n + self._blowup_bits)
+        with self._lock:
+            if tag in self._where:
+                raise ValueError(f"tag {tag} is already in use")
+            i = min(range(len(self._load)), key=lambda k: (self._load[k], k))
+            self._load[i] += w
+            self._where[tag], self._weight[tag] = i, w
+        try:
+            self._servers[i].submit(tag, log_n, a, b)
+        except Exception:
+            with self._lock:
+                self._load[i] -= w
+                self._where.pop(tag, None)
+                self._weight.pop(tag, None)
+            raise
+        return i
+
+    def poll(self, max_items: int = 256, wait_ms: int = 0):
+        """Completions from every device; waits up to wait_ms (split across
+        the devices) only when none is ready."""
+        out = []
+        for s in self._servers:
+            if len(out) < max_items:
+                out += s.poll(max_items - len(out), 0)
+        if not out and wait_ms > 0:
+            per = max(1, wait_ms // len(self._servers))
+            for s in self._servers:
+                out += s.poll(max_items - len(out), per)
+                if out:
+                    break
+        with self._lock:
+            for c in out:
+                tag = int(c.tag)
+                i = self._where.get(tag)
+                if i is not None:
+                    self._load[i] -= self._weight.pop(tag, 0)
+        return out
+
+    def result(self, tag: int, keep: bool = True):
+        with self._lock:
+            i = self._where.pop(tag)
+        return self._servers[i].result(tag, keep)
+
+    def device_of(self, tag: int) -> int:
+        with self._lock:
+            return self._devices[self._where[tag]]
+
+    def outstanding(self) -> list:
+        with self._lock:
+            return list(self._load)
+
+    def close(self) -> None:
+        for s in self._servers:
+            s.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def _device_server(device: int, **kw) -> ProofServer:
+    import torch
+
+    with torch.cuda.device(device):
+        return ProofServer(**kw)

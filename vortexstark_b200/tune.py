@@ -31,8 +31,9 @@ def autotune(max_log: int = 24) -> dict:
 
 
 def set_ntt_plan(layers: int, bottom: int = 0, upper: int = 0) -> None:
-    """Plan of ``layers``-layer transforms: bottom pass of at most ``bottom``
-    layers (9..14), upper passes of at most ``upper`` (3..12); 0 = default."""
+    """Plan of transforms over 2^``layers`` elements (applied to the layers
+    such a transform runs): bottom pass of at most ``bottom`` layers (9..14),
+    upper passes of at most ``upper`` (3..12); 0 = default."""
     _lib.check(_lib.lib().vx_tune_set(NTT_PLAN, layers, bottom, upper))
 
 
