@@ -276,8 +276,11 @@ def served_benchmark(seed: int, n_requests: int = 512, policy=None):
 # DRAM bytes of one LDE (iNTT 2^24 + evaluate 2^26) at log_n = 24 from an ncu
 # capture of the current kernels (dram__bytes_read.sum + dram__bytes_write.sum
 # of the LDE's pass launches); None until measured.
-LDE_TRAFFIC_LOG24 = None
-LDE_TRAFFIC_SOURCE = "not yet captured for the current pass kernels"
+LDE_TRAFFIC_LOG24 = 1141.03e6 + 673.23e6
+LDE_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the LDE's six pass launches (plans "
+                      "11 + 7 + 6 each way), one proof slot at log_n = 24, one-pass metrics: "
+                      "profiles/ntt_tile_lde_log24.md. The bottom evaluate pass reads its twiddles, as large as "
+                      "the data")
 
 LIFT_LOGS = [16] * 8 + [18] * 16 + [20] * 10  # 34 columns, blowup 4: LDEs of 2^18 / 2^20 / 2^22
 
@@ -411,6 +414,39 @@ def _ntt_words_equal_reference(O, cache, k: int) -> dict:
            "round_trip": bool(torch.equal(mine, x)), "words": n}
     del x, mine, theirs
     return out
+
+
+def lde_only(log_n: int, steps: int, warmup: int) -> dict:
+    """The LDE of one Fibonacci proof slot: trace, then interpolate and
+    evaluate (the timed part) per step, inside an NVTX range 'lde' after
+    the warm-up steps.  One slot keeps the device footprint small."""
+    import torch
+
+    from vortexstark_b200 import _lib, prover
+
+    L = _lib.lib()
+    cache = prover.ProverCache(log_n)
+    ms = []
+    for r in range(warmup + steps):
+        if r == warmup:
+            torch.cuda.nvtx.range_push("lde")
+        _lib.check(L.vx_prover_stage_async(cache._p, 0, 3, 5, None))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _lib.check(L.vx_prover_stage_async(cache._p, 1, 3, 5, None))
+        _lib.check(L.vx_prover_stage_async(cache._p, 2, 3, 5, None))
+        e1.record()
+        e1.synchronize()
+        if r >= warmup:
+            ms.append(e0.elapsed_time(e1))
+    torch.cuda.nvtx.range_pop()
+    torch.cuda.synchronize()
+    cache.close()
+    n, N = 1 << log_n, 1 << (log_n + 2)
+    t = statistics.median(ms)
+    peak, _ = _peaks()
+    return {"log_n": log_n, "steps": steps, "ms": t, "gbs": (8 * n + 4 * n + 4 * N) / (t / 1e3) / 1e9,
+            "frac": (8 * n + 4 * n + 4 * N) / (t / 1e3) / 1e9 / peak}
 
 
 def ntt_microbench(peak_gbs: float, sizes=(20, 24, 28), reps: int = 5):
@@ -1005,6 +1041,9 @@ def main():
     ap.add_argument("--kernel-log", type=int, default=26, help="log2 size of the standalone kernel microbench")
     ap.add_argument("--batched-only", action="store_true",
                     help="run only the batched lifted commitment and print its object")
+    ap.add_argument("--lde-only", action="store_true",
+                    help="run only the LDE (trace, interpolate, evaluate) of one proof slot, --steps times inside "
+                         "an NVTX range 'lde', and print its time (the small case for profiling the NTT passes)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -1046,6 +1085,12 @@ def main():
         res = kernel_microbench(peak, probe, log_n=args.kernel_log, cpu=not args.no_cpu_baseline)
         if rank == 0:
             print(json.dumps({"kernel_microbench": res}), flush=True)
+        return
+
+    if args.lde_only:
+        res = lde_only(args.log_n, args.steps, args.warmup)
+        if rank == 0:
+            print(json.dumps({"lde_only": res}), flush=True)
         return
 
     if args.batched_only:

@@ -480,7 +480,8 @@ int vx_fri_chain_fetch(vx_fri_chain *h, uint32_t *roots, uint32_t *alphas, uint3
 /* Autotuner — no counterpart in the reference, whose kernels have fixed
  * shapes (circle_ntt.cu: one launch per layer; blake2s.cu: one leaf per
  * thread).  On the current device, times every distinct NTT pass plan
- * (bottom pass of 10..14 layers, upper passes of at most 6..12) of each
+ * on 4096-element tiles (bottom pass of 10..12 layers, upper passes of at
+ * most 6..9; the larger tiles are set with vx_tune_set) of each
  * transform length 13..max_log (shorter ones are a single pass), and the
  * Merkle leaf kernel's subtree size (2^1..2^4 leaves per thread) of each tree
  * depth 17..max_log, separately for narrow leaves (M31 columns) and for wide

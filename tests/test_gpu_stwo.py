@@ -189,6 +189,11 @@ def _cols(seed, logs):
     ([2], 2, 8), ([3, 3], 1, 5), ([4, 4, 6], 2, 16), ([2, 5, 7], 3, 33), ([6] * 8, 2, 80),
     ([8] * 8 + [10] * 16 + [12] * 10, 2, 80),
     ([5] * 17 + [9] * 20, 2, 40),
+    # size groups of 15..21 layers share one NTT launch per pass (up to four groups per launch); the others
+    # run on their own: all merged, mixed, and more mergeable groups than one launch takes
+    ([15] * 2 + [17] * 3 + [19] * 2, 2, 40),
+    ([12] * 3 + [15] * 2 + [21], 1, 40),
+    ([14] + [16] * 2 + [18] * 2 + [20] * 2 + [21] * 2, 1, 30),
 ])
 def test_commit_lifted_matches_oracle(oracle, logs, B, nq):
     cols = _cols(sum(logs) + B, logs)

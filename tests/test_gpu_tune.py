@@ -105,7 +105,7 @@ def test_autotune_report_and_results(oracle):
         assert 1 <= k <= 4 and ms > 0
         assert tune.get(tune.FOLD_LEAF_K, d)[0] == k
     for t, (b, u, ms) in rep["ntt"].items():
-        assert 10 <= b <= 14 and 6 <= u <= 12 and ms > 0
+        assert 10 <= b <= 12 and 6 <= u <= 9 and ms > 0
         assert tune.get(tune.NTT_PLAN, t) == (b, u)
     for d, (k, ms) in rep["leaf_k"].items():
         assert 1 <= k <= 4 and ms > 0

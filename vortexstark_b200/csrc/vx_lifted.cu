@@ -323,6 +323,35 @@ struct vx_lifted {
 
 namespace {
 
+// The lifted tree with the leaf specialised for the last block's word count.
+template <uint32_t W>
+cudaError_t lifted_tree_w(const LeafLifted &c, const TreeLevels &lv, const ChanStep &cs, cudaStream_t st) {
+    LeafLiftedW<W> leaf;
+    static_cast<LeafLifted &>(leaf) = c;
+    return tree_build(leaf, lv, cs, st);
+}
+cudaError_t lifted_tree_build(const LeafLifted &c, const TreeLevels &lv, const ChanStep &cs, cudaStream_t st) {
+    switch (c.n_cols ? c.n_cols - 16u * ((c.n_cols - 1u) / 16u) : 0u) {
+    case 1: return lifted_tree_w<1>(c, lv, cs, st);
+    case 2: return lifted_tree_w<2>(c, lv, cs, st);
+    case 3: return lifted_tree_w<3>(c, lv, cs, st);
+    case 4: return lifted_tree_w<4>(c, lv, cs, st);
+    case 5: return lifted_tree_w<5>(c, lv, cs, st);
+    case 6: return lifted_tree_w<6>(c, lv, cs, st);
+    case 7: return lifted_tree_w<7>(c, lv, cs, st);
+    case 8: return lifted_tree_w<8>(c, lv, cs, st);
+    case 9: return lifted_tree_w<9>(c, lv, cs, st);
+    case 10: return lifted_tree_w<10>(c, lv, cs, st);
+    case 11: return lifted_tree_w<11>(c, lv, cs, st);
+    case 12: return lifted_tree_w<12>(c, lv, cs, st);
+    case 13: return lifted_tree_w<13>(c, lv, cs, st);
+    case 14: return lifted_tree_w<14>(c, lv, cs, st);
+    case 15: return lifted_tree_w<15>(c, lv, cs, st);
+    case 16: return lifted_tree_w<16>(c, lv, cs, st);
+    default: return tree_build(c, lv, cs, st);
+    }
+}
+
 int lift_stage(vx_lifted *h, uint32_t stage, cudaStream_t st, uint32_t *launches) {
     const LiftLayout &L = h->L;
     uint32_t *proof = h->proof;
@@ -342,7 +371,7 @@ int lift_stage(vx_lifted *h, uint32_t stage, cudaStream_t st, uint32_t *launches
         break;
     }
     case 1:  // lifted tree over the LDE rows, mix its root, draw alpha
-        VX_CUDA_TRY(tree_build(h->cols, h->lv0, ChanStep{h->chan, proof + L.r0, h->alpha}, st));
+        VX_CUDA_TRY(lifted_tree_build(h->cols, h->lv0, ChanStep{h->chan, proof + L.r0, h->alpha}, st));
         *launches += tree_launches(h->lv0);
         break;
     case 2: {  // C = sum alpha^c lift(col_c), committed; draw the first fold challenge

@@ -169,6 +169,28 @@ struct LeafLifted {
     }
 };
 
+// The same leaf with the number of words in the last message block fixed at
+// compile time (WL = n_cols - 16 (blocks - 1), 1..16): full blocks load their
+// 16 words without per-word bounds, and the zero words past WL fold out of
+// the last compression.  Same digests as LeafLifted.
+template <uint32_t WL>
+struct LeafLiftedW : LeafLifted {
+    __device__ __forceinline__ void digest(uint64_t idx, uint32_t h[8], uint32_t one = 1u) const {
+        blake2s_init(h);
+        const uint32_t nfull = (n_cols - WL) / 16u;
+        for (uint32_t b = 0; b < nfull; b++) {
+            uint32_t m[16];
+#pragma unroll
+            for (uint32_t w = 0; w < 16; w++) m[w] = word(16u * b + w, idx);
+            blake2s_compress(h, m, 64u * (b + 1), false, one);
+        }
+        uint32_t m[16];
+#pragma unroll
+        for (uint32_t w = 0; w < 16; w++) m[w] = w < WL ? word(16u * nfull + w, idx) : 0u;
+        blake2s_compress(h, m, 4u * n_cols, true, one);
+    }
+};
+
 // Fold a subtree of 2^kl leaves (kl <= KMAX) starting at `base` into its root.
 template <class Src, uint32_t KMAX = 5>
 __device__ __forceinline__ void subtree_root(const Src &src, uint64_t base, uint32_t kl, uint32_t root[8],

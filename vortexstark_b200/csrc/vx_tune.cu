@@ -121,10 +121,14 @@ extern "C" int vx_autotune(uint32_t max_log, char *report, size_t cap) {
         NttTables tw{tab, tab + n, {}, 0u};
         ntt_table_offsets(total, tw.off);
         float best = 1e30f;
-        uint32_t bb = 12, bu = 12;
+        uint32_t bb = 11, bu = 8;
         std::vector<std::vector<uint32_t>> seen;
-        for (uint32_t bottom = 10; bottom <= 14; bottom++)
-            for (uint32_t upper = 6; upper <= 12; upper++) {
+        // 4096-element tiles only: the larger tiles (bottom passes of 13-14
+        // layers, upper passes of 10-12) can win this timing of an L2-resident
+        // transform and then lose inside proofs, where the LDE's data is in
+        // HBM; they stay available through vx_tune_set
+        for (uint32_t bottom = 10; bottom <= 12; bottom++)
+            for (uint32_t upper = 6; upper <= 9; upper++) {
                 uint32_t ps[32], pr[32], pw[32];
                 uint32_t np = ntt_plan(total, bottom, upper, ps, pr, pw);
                 std::vector<uint32_t> key(pr, pr + np);
@@ -134,7 +138,7 @@ extern "C" int vx_autotune(uint32_t max_log, char *report, size_t cap) {
                     [&] {
                         return ntt_transform_planned(data, nullptr, 0, 1, total, tw, true, nullptr, 0, bottom, upper, st);
                     },
-                    st, 3, &err);
+                    st, 5, &err);
                 if (ms < best) { best = ms; bb = bottom; bu = upper; }
             }
         ntt_knobs_set(dev, total, bb, bu);
