@@ -357,9 +357,13 @@ __device__ __forceinline__ void tile_pass(const Pass2Args &p, uint64_t tile, uin
     }
 }
 
+// Passes are programmatic dependent launches (launch_pdl): a pass's blocks may
+// be scheduled while the previous kernel on the stream drains, and wait here
+// before reading what it wrote.
 template <bool FWD, int R, int WL, int NT>
 __global__ void __launch_bounds__(NT, min_blocks_for(NT)) ntt_tile_kernel(Pass2Args p) {
     extern __shared__ uint32_t dsm[];
+    pdl_wait();
     tile_pass<FWD, R, WL, NT>(p, blockIdx.x, blockIdx.y, dsm);
 }
 
@@ -381,6 +385,7 @@ struct MultiPassArgs {
 template <bool FWD>
 __global__ void __launch_bounds__(256, 4) ntt_multi_kernel(MultiPassArgs a) {
     extern __shared__ uint32_t dsm[];
+    pdl_wait();
     const uint32_t b = blockIdx.x;
     uint32_t gi = 0;
     while (gi + 1 < a.n_groups && b >= a.first[gi + 1]) gi++;
@@ -421,8 +426,7 @@ cudaError_t launch_pass2(const Pass2Args &a, uint64_t tiles, uint32_t n_cols, cu
             if (dev >= 0 && dev < 64) attr_done[dev] = true;
         }
     }
-    ntt_tile_kernel<FWD, R, WL, NT><<<dim3((unsigned)tiles, n_cols), NT, smem, st>>>(a);
-    return cudaGetLastError();
+    return launch_pdl(ntt_tile_kernel<FWD, R, WL, NT>, dim3((unsigned)tiles, n_cols), dim3(NT), smem, st, a);
 }
 
 // Pass shapes the kernels are built for (ntt_plan only emits these):
@@ -720,9 +724,8 @@ cudaError_t ntt_transform_groups(const NttGroup *grp, uint32_t n_groups, bool fo
             (void)wl;
         }
         a.first[a.n_groups] = blocks;
-        if (forward) ntt_multi_kernel<true><<<blocks, 256, smem, stream>>>(a);
-        else ntt_multi_kernel<false><<<blocks, 256, smem, stream>>>(a);
-        e = cudaGetLastError();
+        e = launch_pdl(forward ? ntt_multi_kernel<true> : ntt_multi_kernel<false>, dim3(blocks), dim3(256), smem,
+                       stream, a);
         if (e != cudaSuccess) return e;
         if (launches) *launches += 1;
     }
