@@ -5,13 +5,18 @@ circle LDE): trace, LDE, trace / quotient / FRI commitments, transcript,
 queries and decommitment, on the device.
 
   value    proofs/s with the proof state resident in HBM (device path:
-           vx_prover_prove_async back to back on one stream), all ranks.
-  e2e      the same metric through the C ABI with a host buffer
-           (vx_prove_fib: launch, run, copy the proof bytes to the host).
-  p50/p99  per-proof latency of the e2e loop, ms.
-  roofline LDE (interpolate + zero-pad + evaluate) against the measured HBM
-           copy bandwidth; roofline_alu: the trace commitment (Blake2s)
-           against a register-only Blake2s probe on the same GPU.
+           vx_prover_prove_async, four proofs in flight on four streams),
+           all ranks.
+  e2e      the same metric through the C ABI with host buffers
+           (vx_prove_fib_batch: launch, run, copy the proof bytes to the host).
+  p50/p99  per-proof latency through vx_prove_fib, one proof at a time, ms.
+  roofline the dominant kernel, the trace commitment (Blake2s, integer ALU
+           pipe), against a register-only Blake2s probe on the same GPU and
+           against the ALU-pipe ceiling; lde_roofline: the LDE (interpolate
+           + zero-pad + evaluate) against the measured HBM copy bandwidth.
+  served   the metric's mixed log_n 16-24 stream: the serving engine and the
+           plain one-at-a-time path, swept over arrival rates, compared by
+           the rate each sustains at common p99 bounds.
 
 N > 1 (torchrun): independent replicas, one per GPU, no collective on the
 data path ("replicas only"); barrier + max-over-ranks timing.
