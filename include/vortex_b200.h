@@ -406,10 +406,14 @@ int vx_server_create(size_t budget_bytes, uint32_t max_inflight, uint32_t blowup
  * large proofs on the highest-priority streams, 3 grades by size
  * (2^(large_log_eval-2) .. 2^(large_log_eval-1) points in between, smaller
  * ones highest, large ones lowest).  small_cap bounds the small proofs in
- * flight while a large one is (0: no bound).  Defaults: 24, 1, 0, 0, 0.
+ * flight while a large one is (0: no bound).  split_large != 0 runs a large
+ * proof as two graphs: its head (LDE, trace, quotient and first FRI
+ * commitments) counts against max_large, its tail (line folds, queries,
+ * decommitment) runs on a highest-priority stream after it and does not, so
+ * the next large proof's head overlaps it.  Defaults: 24, 1, 0, 0, 0, 1.
  * Proof bytes never depend on the policy. */
 int vx_server_set_policy(vx_server *s, uint32_t large_log_eval, uint32_t max_large, int priority,
-                         uint32_t small_cap, int large_per_size);
+                         uint32_t small_cap, int large_per_size, int split_large);
 /* Queue one request (non-blocking). */
 int vx_server_submit(vx_server *s, uint64_t tag, uint32_t log_n, uint32_t a, uint32_t b);
 /* Create up to `count` slots of this size ahead of time (counts against the budget). */

@@ -1058,6 +1058,66 @@ int prover_capture_graph(vx_prover *p, cudaStream_t st, uint32_t *dev_ab, const 
     p->launches = launches;
     return VX_OK;
 }
+// The same proof as two graphs: `head` copies (a, b) in and runs stages
+// [0, split); `tail` runs stages [split, VX_N_STAGES) and copies the proof
+// bytes and the transcript status word out.  The caller launches tail after
+// head (on the same stream, or on another stream that waits for an event
+// recorded after head).
+int prover_capture_graph_split(vx_prover *p, cudaStream_t st, uint32_t *dev_ab, const uint32_t *pinned_ab,
+                               void *pinned_out, uint32_t split, cudaGraphExec_t *head, cudaGraphExec_t *tail) {
+    VX_CHECK_ARG(split >= 1 && split < VX_N_STAGES, "prover_capture_graph_split: split %u outside 1..%u", split,
+                 VX_N_STAGES - 1);
+    ProofSlot &S = p->s;
+    uint32_t launches = 0;
+    for (uint32_t stage = 0; stage < VX_N_STAGES; stage++) {
+        int rc = enqueue_stage(p, stage, 1u, 1u, st, &launches);
+        if (rc) return rc;
+    }
+    VX_CUDA_TRY(cudaStreamSynchronize(st));
+    S.inputs = dev_ab;
+    launches = 0;
+    cudaGraphExec_t ex[2] = {nullptr, nullptr};
+    int rc = VX_OK;
+    for (int part = 0; part < 2 && rc == VX_OK; part++) {
+        cudaGraph_t g = nullptr;
+        if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) { rc = VX_ERR_CUDA; break; }
+        if (part == 0) {
+            if (cudaMemcpyAsync(dev_ab, pinned_ab, 8, cudaMemcpyHostToDevice, st) != cudaSuccess) rc = VX_ERR_CUDA;
+            for (uint32_t stage = 0; stage < split && rc == VX_OK; stage++)
+                rc = enqueue_stage(p, stage, 0u, 0u, st, &launches);
+        } else {
+            for (uint32_t stage = split; stage < VX_N_STAGES && rc == VX_OK; stage++)
+                rc = enqueue_stage(p, stage, 0u, 0u, st, &launches);
+            if (rc == VX_OK &&
+                cudaMemcpyAsync(pinned_out, S.proof, S.L.words * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+                rc = VX_ERR_CUDA;
+            if (rc == VX_OK && cudaMemcpyAsync((uint8_t *)pinned_out + S.L.words * 4, &S.chan->err, 4,
+                                               cudaMemcpyDeviceToHost, st) != cudaSuccess)
+                rc = VX_ERR_CUDA;
+        }
+        cudaError_t e = cudaStreamEndCapture(st, &g);
+        if (rc == VX_OK && e != cudaSuccess) {
+            set_last_error(VX_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+            rc = VX_ERR_CUDA;
+        }
+        if (rc == VX_OK && (e = cudaGraphInstantiate(&ex[part], g, 0)) != cudaSuccess) {
+            set_last_error(VX_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+            rc = VX_ERR_CUDA;
+        }
+        if (g) cudaGraphDestroy(g);
+    }
+    S.inputs = nullptr;
+    if (rc != VX_OK) {
+        for (auto &x : ex)
+            if (x) cudaGraphExecDestroy(x);
+        return rc;
+    }
+    *head = ex[0];
+    *tail = ex[1];
+    p->launches = launches;
+    return VX_OK;
+}
+
 // Device bytes vx_prover_create takes for one slot of this size, and the
 // shared tables of the size (same arithmetic as the carving above).
 void prover_footprint(uint32_t log_n, uint32_t blowup, uint32_t nq, size_t *slot_b, size_t *tab_b) {

@@ -64,6 +64,10 @@ namespace vx {
 // (pinned_out holds prover_proof_bytes + 4 bytes).
 int prover_capture_graph(vx_prover *p, cudaStream_t st, uint32_t *dev_ab, const uint32_t *pinned_ab,
                          void *pinned_out, cudaGraphExec_t *exec);
+// The same proof split into two graphs at stage `split`: head (inputs in,
+// stages before split) and tail (the rest, proof bytes and status word out).
+int prover_capture_graph_split(vx_prover *p, cudaStream_t st, uint32_t *dev_ab, const uint32_t *pinned_ab,
+                               void *pinned_out, uint32_t split, cudaGraphExec_t *head, cudaGraphExec_t *tail);
 uint32_t prover_log_n(const vx_prover *p);
 void prover_footprint(uint32_t log_n, uint32_t blowup, uint32_t nq, size_t *slot_b, size_t *tab_b);
 size_t prover_proof_bytes(const vx_prover *p);

@@ -24,7 +24,11 @@
 // their blocks are dispatched ahead of a large proof's waiting blocks and
 // fill the gaps it leaves; the reverse order keeps a large proof close to
 // its solo time.  `small_cap` optionally bounds the small proofs in flight
-// while a large one is.
+// while a large one is.  With `split_large` (default) a large proof is two
+// graphs: its head (LDE and the trace, quotient and first FRI commitments)
+// counts against max_large; its tail (line folds, queries, decommitment)
+// runs on a highest-priority stream and no longer does, so the next large
+// proof's head overlaps it.
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -57,6 +61,7 @@ struct Request {
 constexpr uint32_t kLargeLogEval = 24;
 constexpr uint32_t kMaxLargeInflight = 1;
 constexpr int kPrioDefault = 0;
+constexpr uint32_t kTailStage = 6;  // a split large proof's tail: line folds, queries, decommitment
 
 struct Slot {
     vx_prover *p = nullptr;
@@ -65,6 +70,12 @@ struct Slot {
     cudaStream_t st = nullptr;
     cudaEvent_t done = nullptr;
     cudaGraphExec_t exec = nullptr;
+    // split large proofs: exec is the head (inputs, LDE, trace / quotient / first FRI commitments) on st,
+    // tail_exec the rest on tail_st (highest priority), after head_done
+    cudaGraphExec_t tail_exec = nullptr;
+    cudaStream_t tail_st = nullptr;
+    cudaEvent_t head_done = nullptr;
+    bool active = false;   // a large proof counted against max_large (in flight, or in its head if split)
     uint8_t *pinned_out = nullptr;
     uint32_t *pinned_ab = nullptr;
     uint32_t *dev_ab = nullptr;
@@ -88,11 +99,13 @@ struct vx_server {
     std::thread worker;
     bool stop = false;
     size_t budget = 0, used = 0;
+    // large_inflight: large proofs counted against max_large (see Slot::active)
     uint32_t max_inflight = 1, inflight = 0, large_inflight = 0, small_inflight = 0, blowup = 2, nq = 80;
     // policy (vx_server_set_policy)
     uint32_t large_log_eval = kLargeLogEval, max_large = kMaxLargeInflight, small_cap = 0;
     bool large_per_size = false;               // max_large counts per size instead of overall
-    std::map<uint32_t, uint32_t> large_by_size;  // large proofs in flight per log_n
+    bool split_large = true;                   // large proofs as head + tail graphs (see slot_create)
+    std::map<uint32_t, uint32_t> large_by_size;  // active large proofs per log_n
     int prio_mode = kPrioDefault;  // 0: small proofs highest, 1: all equal, 2: large proofs highest, 3: graded
     int device = 0;
     bool use_graphs = true;
@@ -141,15 +154,31 @@ int slot_create(vx_server *s, uint32_t log_n, Slot **out) {
     if ((e = cudaMallocHost(&sl->pinned_out, sl->bytes + 16)) != cudaSuccess) return fail("pinned output", e);
     if ((e = cudaMallocHost(&sl->pinned_ab, 8)) != cudaSuccess) return fail("pinned input", e);
     if ((e = cudaMalloc(&sl->dev_ab, 256)) != cudaSuccess) return fail("device input", e);
-    if (s->use_graphs) {
-        rc = prover_capture_graph(sl->p, sl->st, sl->dev_ab, sl->pinned_ab, sl->pinned_out, &sl->exec);
-        if (rc) {
-            cudaStreamDestroy(sl->st); cudaEventDestroy(sl->done);
-            cudaFreeHost(sl->pinned_out); cudaFreeHost(sl->pinned_ab); cudaFree(sl->dev_ab);
-            vx_prover_destroy(sl->p);
-            delete sl;
-            return rc;
+    if (s->use_graphs && sl->large && s->split_large) {
+        // A large proof's head fills the GPU; its tail (line folds, queries,
+        // decommitment) ends in latency-bound chains.  The tail runs on a
+        // highest-priority stream behind an event, and the next large proof
+        // may start as soon as this head is done, so its head overlaps this
+        // tail instead of the GPU idling through it.
+        if ((e = cudaStreamCreateWithPriority(&sl->tail_st, cudaStreamNonBlocking, prio_greatest)) != cudaSuccess)
+            return fail("tail stream", e);
+        if ((e = cudaEventCreateWithFlags(&sl->head_done, cudaEventDisableTiming)) != cudaSuccess) {
+            cudaStreamDestroy(sl->tail_st);
+            return fail("head event", e);
         }
+        rc = prover_capture_graph_split(sl->p, sl->st, sl->dev_ab, sl->pinned_ab, sl->pinned_out, kTailStage,
+                                        &sl->exec, &sl->tail_exec);
+    } else if (s->use_graphs) {
+        rc = prover_capture_graph(sl->p, sl->st, sl->dev_ab, sl->pinned_ab, sl->pinned_out, &sl->exec);
+    }
+    if (rc) {
+        if (sl->tail_st) cudaStreamDestroy(sl->tail_st);
+        if (sl->head_done) cudaEventDestroy(sl->head_done);
+        cudaStreamDestroy(sl->st); cudaEventDestroy(sl->done);
+        cudaFreeHost(sl->pinned_out); cudaFreeHost(sl->pinned_ab); cudaFree(sl->dev_ab);
+        vx_prover_destroy(sl->p);
+        delete sl;
+        return rc;
     }
     *out = sl;
     return VX_OK;
@@ -157,6 +186,9 @@ int slot_create(vx_server *s, uint32_t log_n, Slot **out) {
 
 void slot_destroy(Slot *sl) {
     if (sl->exec) cudaGraphExecDestroy(sl->exec);
+    if (sl->tail_exec) cudaGraphExecDestroy(sl->tail_exec);
+    if (sl->tail_st) cudaStreamDestroy(sl->tail_st);
+    if (sl->head_done) cudaEventDestroy(sl->head_done);
     cudaStreamDestroy(sl->st);
     cudaEventDestroy(sl->done);
     cudaFreeHost(sl->pinned_out);
@@ -176,8 +208,23 @@ int launch(vx_server *s, Slot *sl, const Request &r) {
     sl->req = r;
     sl->start_ns = now_ns();
     s->inflight++;
-    if (sl->large) { s->large_inflight++; s->large_by_size[sl->log_n]++; }
-    else s->small_inflight++;
+    if (sl->large) {
+        s->large_inflight++;
+        s->large_by_size[sl->log_n]++;
+        sl->active = true;
+    } else {
+        s->small_inflight++;
+    }
+    if (sl->tail_exec) {
+        sl->pinned_ab[0] = r.a;
+        sl->pinned_ab[1] = r.b;
+        VX_CUDA_TRY(cudaGraphLaunch(sl->exec, sl->st));
+        VX_CUDA_TRY(cudaEventRecord(sl->head_done, sl->st));
+        VX_CUDA_TRY(cudaStreamWaitEvent(sl->tail_st, sl->head_done, 0));
+        VX_CUDA_TRY(cudaGraphLaunch(sl->tail_exec, sl->tail_st));
+        VX_CUDA_TRY(cudaEventRecord(sl->done, sl->tail_st));
+        return VX_OK;
+    }
     if (sl->exec) {
         sl->pinned_ab[0] = r.a;
         sl->pinned_ab[1] = r.b;
@@ -200,11 +247,28 @@ void size_estimate(vx_server *s, uint32_t log_n, size_t *slot_b, size_t *tab_b) 
     *slot_b += 256;  // the slot's device input words
 }
 
+// A large proof stops counting against max_large when its head is done
+// (split) or when it completes.
+void deactivate(vx_server *s, Slot *sl) {
+    if (!sl->active) return;
+    sl->active = false;
+    s->large_inflight--;
+    s->large_by_size[sl->log_n]--;
+}
+
 void worker_loop(vx_server *s) {
     cudaSetDevice(s->device);
     std::unique_lock<std::mutex> lk(s->mu);
     while (!s->stop) {
         bool progress = false;
+        // split large proofs whose head is done free their large-proof place
+        for (Slot *sl : s->slots) {
+            if (!sl->busy || !sl->active || !sl->tail_exec) continue;
+            if (cudaEventQuery(sl->head_done) != cudaErrorNotReady) {
+                deactivate(s, sl);
+                progress = true;
+            }
+        }
         // complete finished proofs
         for (Slot *sl : s->slots) {
             if (!sl->busy) continue;
@@ -227,7 +291,7 @@ void worker_loop(vx_server *s) {
             s->completed.push_back(c);
             sl->busy = false;
             s->inflight--;
-            if (sl->large) { s->large_inflight--; s->large_by_size[sl->log_n]--; }
+            if (sl->large) deactivate(s, sl);
             else s->small_inflight--;
             progress = true;
         }
@@ -318,7 +382,7 @@ extern "C" int vx_server_create(size_t budget_bytes, uint32_t max_inflight, uint
 }
 
 extern "C" int vx_server_set_policy(vx_server *s, uint32_t large_log_eval, uint32_t max_large, int priority,
-                                    uint32_t small_cap, int large_per_size) {
+                                    uint32_t small_cap, int large_per_size, int split_large) {
     VX_CHECK_ARG(s != nullptr, "vx_server_set_policy: null server");
     VX_CHECK_ARG(large_log_eval >= 1 && large_log_eval <= 32, "vx_server_set_policy: bad large_log_eval %u",
                  large_log_eval);
@@ -330,6 +394,7 @@ extern "C" int vx_server_set_policy(vx_server *s, uint32_t large_log_eval, uint3
     s->large_log_eval = large_log_eval;
     s->max_large = max_large;
     s->large_per_size = large_per_size != 0;
+    s->split_large = split_large != 0;
     s->prio_mode = priority;
     s->small_cap = small_cap;
     return VX_OK;

@@ -34,14 +34,16 @@ class ProofServer:
                                                1 if use_graphs else 0, C.byref(self._s)))
 
     def set_policy(self, large_log_eval: int = 24, max_large: int = 1, priority: int = 0,
-                   small_cap: int = 0, large_per_size: bool = False) -> None:
+                   small_cap: int = 0, large_per_size: bool = False, split_large: bool = True) -> None:
         """Scheduling policy (before the first prewarm or submit): proofs of at
         least 2^large_log_eval evaluation points are large, at most max_large
         of them in flight (per size if large_per_size); priority 0 = small
         proofs first, 1 = equal, 2 = large proofs first, 3 = graded by size;
-        small_cap bounds small proofs in flight beside a large one (0 = none)."""
+        small_cap bounds small proofs in flight beside a large one (0 = none);
+        split_large runs a large proof's latency-bound tail on a high-priority
+        stream outside the max_large count, overlapping the next one's head."""
         _lib.check(_lib.lib().vx_server_set_policy(self._s, large_log_eval, max_large, priority, small_cap,
-                                                   1 if large_per_size else 0))
+                                                   1 if large_per_size else 0, 1 if split_large else 0))
 
     def prewarm(self, log_n: int, count: int) -> None:
         _lib.check(_lib.lib().vx_server_prewarm(self._s, log_n, count))
