@@ -407,10 +407,11 @@ int vx_server_create(size_t budget_bytes, uint32_t max_inflight, uint32_t blowup
  * (2^(large_log_eval-2) .. 2^(large_log_eval-1) points in between, smaller
  * ones highest, large ones lowest).  small_cap bounds the small proofs in
  * flight while a large one is (0: no bound).  split_large != 0 runs a large
- * proof as two graphs: its head (LDE, trace, quotient and first FRI
- * commitments) counts against max_large, its tail (line folds, queries,
- * decommitment) runs on a highest-priority stream after it and does not, so
- * the next large proof's head overlaps it.  Defaults: 24, 1, 0, 0, 0, 1.
+ * proof as two graphs: its head (LDE, trace and quotient commitments, the
+ * FRI layers whose trees are deeper than 16) counts against max_large, its
+ * tail (the smaller FRI layers, queries, decommitment) runs on a
+ * highest-priority stream after it and does not, so the next large proof's
+ * head overlaps it.  Defaults: 24, 1, 0, 0, 0, 1.
  * Proof bytes never depend on the policy. */
 int vx_server_set_policy(vx_server *s, uint32_t large_log_eval, uint32_t max_large, int priority,
                          uint32_t small_cap, int large_per_size, int split_large);

@@ -547,7 +547,10 @@ extern "C" size_t vx_prover_table_bytes(const vx_prover *p) { return p && p->s.t
 //   0 trace, 1 interpolate, 2 LDE evaluate, 3 trace commitment,
 //   4 quotient commitment, 5 circle fold + FRI layer 0, 6 line folds,
 //   7 last layer + queries, 8 decommitment.
-static int enqueue_stage(vx_prover *p, uint32_t stage, uint32_t a, uint32_t b, cudaStream_t st, uint32_t *launches) {
+// Stage 6 folds FRI layers k = 1 .. nfri-1; enqueue_stage(..., k_lo, k_hi)
+// enqueues only layers [k_lo, k_hi) of it (the other stages ignore them).
+static int enqueue_stage(vx_prover *p, uint32_t stage, uint32_t a, uint32_t b, cudaStream_t st, uint32_t *launches,
+                         uint32_t k_lo = 1, uint32_t k_hi = ~0u) {
     ProofSlot &S = p->s;
     const ProofLayout &L = S.L;
     const SizeTables &T = *S.tw;
@@ -593,7 +596,7 @@ static int enqueue_stage(vx_prover *p, uint32_t stage, uint32_t a, uint32_t b, c
         break;
     }
     case 6:
-        for (uint32_t k = 1; k < L.nfri; k++) {
+        for (uint32_t k = k_lo < 1 ? 1 : k_lo; k < L.nfri && k < k_hi; k++) {
             uint32_t lsrc = le - k;  // log size of the layer being folded
             LeafLineFold lf{S.fri[k - 1][0], S.fri[k - 1][1], S.fri[k - 1][2], S.fri[k - 1][3],
                             T.fold_line + T.fold_line_off[lsrc], S.alpha_f + 4 * k,
@@ -1068,6 +1071,12 @@ int prover_capture_graph_split(vx_prover *p, cudaStream_t st, uint32_t *dev_ab, 
     VX_CHECK_ARG(split >= 1 && split < VX_N_STAGES, "prover_capture_graph_split: split %u outside 1..%u", split,
                  VX_N_STAGES - 1);
     ProofSlot &S = p->s;
+    // Split at the line folds (stage 6): the FRI layers whose trees start with
+    // the leaf kernel (deeper than 16, GPU-filling) go to the head, the small
+    // layers, reduced by one latency-bound launch each, to the tail.
+    uint32_t k_split = 1;
+    if (split == 6)
+        while (k_split < S.L.nfri && S.L.le - 1 - k_split > 16u) k_split++;
     uint32_t launches = 0;
     for (uint32_t stage = 0; stage < VX_N_STAGES; stage++) {
         int rc = enqueue_stage(p, stage, 1u, 1u, st, &launches);
@@ -1085,9 +1094,10 @@ int prover_capture_graph_split(vx_prover *p, cudaStream_t st, uint32_t *dev_ab, 
             if (cudaMemcpyAsync(dev_ab, pinned_ab, 8, cudaMemcpyHostToDevice, st) != cudaSuccess) rc = VX_ERR_CUDA;
             for (uint32_t stage = 0; stage < split && rc == VX_OK; stage++)
                 rc = enqueue_stage(p, stage, 0u, 0u, st, &launches);
+            if (rc == VX_OK && split == 6 && k_split > 1) rc = enqueue_stage(p, 6, 0u, 0u, st, &launches, 1, k_split);
         } else {
             for (uint32_t stage = split; stage < VX_N_STAGES && rc == VX_OK; stage++)
-                rc = enqueue_stage(p, stage, 0u, 0u, st, &launches);
+                rc = enqueue_stage(p, stage, 0u, 0u, st, &launches, stage == 6 ? k_split : 1);
             if (rc == VX_OK &&
                 cudaMemcpyAsync(pinned_out, S.proof, S.L.words * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess)
                 rc = VX_ERR_CUDA;

@@ -66,6 +66,8 @@ int prover_capture_graph(vx_prover *p, cudaStream_t st, uint32_t *dev_ab, const 
                          void *pinned_out, cudaGraphExec_t *exec);
 // The same proof split into two graphs at stage `split`: head (inputs in,
 // stages before split) and tail (the rest, proof bytes and status word out).
+// At split 6 (the line folds) the head also takes the FRI layers whose trees
+// are deeper than 16; the tail starts with the first smaller layer.
 int prover_capture_graph_split(vx_prover *p, cudaStream_t st, uint32_t *dev_ab, const uint32_t *pinned_ab,
                                void *pinned_out, uint32_t split, cudaGraphExec_t *head, cudaGraphExec_t *tail);
 uint32_t prover_log_n(const vx_prover *p);

@@ -25,10 +25,10 @@
 // fill the gaps it leaves; the reverse order keeps a large proof close to
 // its solo time.  `small_cap` optionally bounds the small proofs in flight
 // while a large one is.  With `split_large` (default) a large proof is two
-// graphs: its head (LDE and the trace, quotient and first FRI commitments)
-// counts against max_large; its tail (line folds, queries, decommitment)
-// runs on a highest-priority stream and no longer does, so the next large
-// proof's head overlaps it.
+// graphs: its head (LDE, the trace, quotient and FRI commitments of layers
+// deeper than 16) counts against max_large; its tail (the small FRI layers,
+// queries, decommitment) runs on a highest-priority stream and no longer
+// does, so the next large proof's head overlaps it.
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -61,7 +61,9 @@ struct Request {
 constexpr uint32_t kLargeLogEval = 24;
 constexpr uint32_t kMaxLargeInflight = 1;
 constexpr int kPrioDefault = 0;
-constexpr uint32_t kTailStage = 6;  // a split large proof's tail: line folds, queries, decommitment
+// A split large proof's tail: the line folds of layers of at most 2^16 values
+// (one latency-bound reduce launch each), queries and decommitment.
+constexpr uint32_t kTailStage = 6;
 
 struct Slot {
     vx_prover *p = nullptr;
@@ -155,8 +157,8 @@ int slot_create(vx_server *s, uint32_t log_n, Slot **out) {
     if ((e = cudaMallocHost(&sl->pinned_ab, 8)) != cudaSuccess) return fail("pinned input", e);
     if ((e = cudaMalloc(&sl->dev_ab, 256)) != cudaSuccess) return fail("device input", e);
     if (s->use_graphs && sl->large && s->split_large) {
-        // A large proof's head fills the GPU; its tail (line folds, queries,
-        // decommitment) ends in latency-bound chains.  The tail runs on a
+        // A large proof's head fills the GPU; its tail (the small FRI layers,
+        // queries, decommitment) is a chain of latency-bound launches.  The tail runs on a
         // highest-priority stream behind an event, and the next large proof
         // may start as soon as this head is done, so its head overlaps this
         // tail instead of the GPU idling through it.
