@@ -114,16 +114,19 @@ def test_multi_engine_router_equals_alone(oracle):
     assert results[0] == oracle.prove(reqs[0][1], reqs[0][2], reqs[0][0])
 
 
-def test_policy_knobs_validated_and_bytes_unchanged():
+@pytest.mark.parametrize("split", [True, False])
+def test_policy_knobs_validated_and_bytes_unchanged(split):
     """vx_server_set_policy rejects bad values and calls after the first
-    slot exists; a non-default policy changes scheduling only."""
+    slot exists; a non-default policy changes scheduling only, with large
+    proofs (here log_n 12, 2^14 points) as head + tail graphs or whole."""
     from vortexstark_b200 import _lib
 
     with ProofServer(budget_bytes=1 << 30, max_inflight=4) as srv:
         for kw in (dict(priority=4), dict(max_large=0), dict(large_log_eval=0), dict(large_log_eval=40)):
             with pytest.raises(_lib.VortexError):
                 srv.set_policy(**kw)
-        srv.set_policy(large_log_eval=14, max_large=1, priority=3, small_cap=2, large_per_size=True)
+        srv.set_policy(large_log_eval=14, max_large=1, priority=3, small_cap=2, large_per_size=True,
+                       split_large=split)
         srv.prewarm(10, 1)
         with pytest.raises(_lib.VortexError):
             srv.set_policy()
