@@ -343,6 +343,33 @@ def batched_commit_benchmark(seed: int, steps: int, warmup: int, peak_gbs: float
         lat.append(a.elapsed_time(b))
     com.result_bytes()
     e2e_ms = statistics.median(lat)
+    # end to end with two commitments in flight: a second context on a second
+    # stream, so one commitment's column upload (copy engine) overlaps the
+    # other's device work; every commitment still uploads all its columns and
+    # reads its words back inside the timed region
+    com2 = LiftedCommitter(LIFT_LOGS, 2, 80)
+    st2 = torch.cuda.Stream()
+    ctx = [(com, st), (com2, st2)]
+    for c, t in ctx:
+        c.upload_async(ptrs, t.cuda_stream)
+        c.commit_async(t.cuda_stream, graph=True)
+        c.fetch_async(t.cuda_stream)
+    torch.cuda.synchronize()
+    p0, p1, j2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    p0.record(st)
+    st2.wait_event(p0)
+    for i in range(2 * steps):
+        c, t = ctx[i % 2]
+        c.upload_async(ptrs, t.cuda_stream)
+        c.commit_async(t.cuda_stream, graph=True)
+        c.fetch_async(t.cuda_stream)
+    j2.record(st2)
+    st.wait_event(j2)
+    p1.record(st)
+    p1.synchronize()
+    pipe_ms = p0.elapsed_time(p1) / (2 * steps)
+    pipe_equal = com.result_bytes() == com2.result_bytes()
+    com2.close()
     # per-stage device times
     names = ["lde", "lifted_tree", "combination_tree", "circle_fold", "line_folds", "queries", "openings"]
     reps = 3
@@ -367,8 +394,12 @@ def batched_commit_benchmark(seed: int, steps: int, warmup: int, peak_gbs: float
                     "one lifted Blake2s tree (2^22 leaves of 34 words), QM31 combination + FRI to 8 values, "
                     "80 queries; one CUDA graph per commitment",
         "value": 1e3 / dev_ms, "unit": "commitments/s", "ms_per_commit": dev_ms,
-        "e2e": {"value": 1e3 / e2e_ms, "unit": "commitments/s", "ms": e2e_ms, "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": com.size},
+        "e2e": {"value": 1e3 / pipe_ms, "unit": "commitments/s", "ms_per_commit": pipe_ms,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": com.size,
+                "how": "two contexts on two streams, CUDA events around the loop: each commitment uploads its 34 "
+                       "columns from pinned memory, commits and reads its words back",
+                "latency_ms": e2e_ms, "latency_how": "one commitment alone: upload, commit, read back (CUDA events)",
+                "contexts_bytes_equal": pipe_equal},
         "launches_per_commit": com.launches(), "device_bytes": com.device_bytes(),
         "stages_ms": stages,
         "roofline": {"bound": "hbm", "kernel": "stwo LDE of all 34 columns", "achieved": lde_gbs,

@@ -224,6 +224,29 @@ def test_commit_lifted_graph_and_uploads(oracle):
     com.close()
 
 
+def test_two_commitments_in_flight_on_two_streams(oracle):
+    """Two contexts of one shape, each on its own stream with different
+    columns, enqueued alternately without synchronising (the pipelined
+    end-to-end loop): each context's words equal the oracle's for its own
+    columns."""
+    import torch
+
+    logs = [10] * 3 + [12] * 4 + [14] * 2
+    coms = [LiftedCommitter(logs, 2, 40) for _ in range(2)]
+    streams = [torch.cuda.Stream() for _ in range(2)]
+    cols = [_cols(40 + i, logs) for i in range(2)]
+    pinned = [[torch.from_numpy(c.view(np.int32).copy()).pin_memory() for c in cs] for cs in cols]
+    for _ in range(3):
+        for com, st, pin in zip(coms, streams, pinned):
+            com.upload_async([t.data_ptr() for t in pin], st.cuda_stream)
+            com.commit_async(st.cuda_stream, graph=True)
+            com.fetch_async(st.cuda_stream)
+    torch.cuda.synchronize()
+    for com, cs in zip(coms, cols):
+        assert com.result_bytes() == oracle.commit_lifted(cs, 2, 40)
+        com.close()
+
+
 def _qm(rng, n):
     return rng.integers(0, P, (n, 4), dtype=np.uint32)
 
