@@ -203,15 +203,18 @@ def plain_sweep(reqs, cap, seed, caches, mults=PLAIN_RATE_MULTS):
     return out
 
 
-def engine_sweep(reqs, cap, seed, policy=None, mults=ENGINE_RATE_MULTS):
+def engine_sweep(reqs, cap, seed, policy=None, mults=ENGINE_RATE_MULTS, queue=None):
     """The serving engine over the same stream at each offered rate; returns
-    the sweep and the engine's slot statistics."""
+    the sweep and the engine's slot statistics.  `policy` and `queue` are
+    keyword arguments of ProofServer.set_policy / set_queue_order."""
     from vortexstark_b200.serving import ProofServer, poisson_arrivals, run_stream
 
     n, sizes = len(reqs), [r[0] for r in reqs]
     with ProofServer(budget_bytes=64 << 30, max_inflight=24) as srv:
         if policy:
             srv.set_policy(**policy)
+        if queue:
+            srv.set_queue_order(**queue)
         counts = {16: 12, 18: 8, 20: 6, 22: 3, 24: 2}
         for ln in sorted(set(sizes)):
             srv.prewarm(ln, counts.get(ln, 2))

@@ -415,6 +415,13 @@ int vx_server_create(size_t budget_bytes, uint32_t max_inflight, uint32_t blowup
  * Proof bytes never depend on the policy. */
 int vx_server_set_policy(vx_server *s, uint32_t large_log_eval, uint32_t max_large, int priority,
                          uint32_t small_cap, int large_per_size, int split_large);
+/* Order in which waiting large proofs take a free large place (any time;
+ * ignored when large_per_size is set).  smallest_first == 0: oldest first
+ * (the default).  smallest_first != 0: the smallest log_n first, oldest
+ * within a size, except that once the oldest waiting large proof has waited
+ * max_wait_us (0: never) it goes first.  Small proofs are not affected.
+ * Proof bytes never depend on the order. */
+int vx_server_set_queue_order(vx_server *s, int smallest_first, uint32_t max_wait_us);
 /* Queue one request (non-blocking). */
 int vx_server_submit(vx_server *s, uint64_t tag, uint32_t log_n, uint32_t a, uint32_t b);
 /* Create up to `count` slots of this size ahead of time (counts against the budget). */

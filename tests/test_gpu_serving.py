@@ -134,3 +134,34 @@ def test_policy_knobs_validated_and_bytes_unchanged(split):
         summary, results = run_stream(srv, reqs, [0.0] * len(reqs), keep_results=True)
     for i, (log_n, a, b) in enumerate(reqs):
         assert results[i] == prover.prove_bytes(a, b, log_n), (i, log_n)
+
+
+@pytest.mark.parametrize("smallest_first", [False, True])
+def test_large_queue_order(smallest_first):
+    """Waiting large proofs take the free large place oldest first, or
+    smallest first (vx_server_set_queue_order): a 2^24-point proof runs
+    while three smaller large proofs queue behind it; their start order
+    follows the rule, and every proof equals the same request proved alone."""
+    import time
+
+    reqs = [(22, 11, 12), (14, 13, 14), (12, 15, 16), (13, 17, 18)]
+    with ProofServer(budget_bytes=8 << 30, max_inflight=8) as srv:
+        srv.set_policy(large_log_eval=14)  # log_n >= 12 is large
+        srv.set_queue_order(smallest_first=smallest_first)
+        for s in (22, 14, 12, 13):
+            srv.prewarm(s, 1)
+        srv.submit(0, *reqs[0])
+        t0 = time.time()
+        while srv.stats()["inflight"] == 0 and time.time() - t0 < 5:
+            time.sleep(0.0001)
+        for i in (1, 2, 3):  # queued while the 2^24-point proof's head runs (about 4 ms)
+            srv.submit(i, *reqs[i])
+        done = {}
+        while len(done) < 4:
+            for c in srv.poll(8, wait_ms=100):
+                assert c.status == 0
+                done[int(c.tag)] = (c.start_ns, srv.result(int(c.tag)))
+    order = [t for t, _ in sorted(done.items(), key=lambda kv: kv[1][0])]
+    assert order == ([0, 2, 3, 1] if smallest_first else [0, 1, 2, 3])
+    for i, (log_n, a, b) in enumerate(reqs):
+        assert done[i][1] == prover.prove_bytes(a, b, log_n), i

@@ -120,6 +120,7 @@ _SIGS = {
     "vx_server_create": ([C.c_size_t, u32, u32, u32, C.c_int, C.POINTER(vp)], C.c_int),
     "vx_server_submit": ([vp, C.c_uint64, u32, u32, u32], C.c_int),
     "vx_server_set_policy": ([vp, u32, u32, C.c_int, u32, C.c_int, C.c_int], C.c_int),
+    "vx_server_set_queue_order": ([vp, C.c_int, u32], C.c_int),
     "vx_server_prewarm": ([vp, u32, u32], C.c_int),
     "vx_server_poll": ([vp, vp, u32, C.POINTER(u32), C.c_int], C.c_int),
     "vx_server_result": ([vp, C.c_uint64, vp, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),

@@ -109,6 +109,10 @@ struct vx_server {
     bool split_large = true;                   // large proofs as head + tail graphs (see slot_create)
     std::map<uint32_t, uint32_t> large_by_size;  // active large proofs per log_n
     int prio_mode = kPrioDefault;  // 0: small proofs highest, 1: all equal, 2: large proofs highest, 3: graded
+    // order of waiting large proofs (vx_server_set_queue_order): oldest first,
+    // or smallest first with the oldest going first once it has waited max_wait_ns
+    bool smallest_first = false;
+    uint64_t max_wait_ns = 0;
     int device = 0;
     bool use_graphs = true;
     int fatal = VX_OK;
@@ -258,6 +262,22 @@ void deactivate(vx_server *s, Slot *sl) {
     s->large_by_size[sl->log_n]--;
 }
 
+// Smallest-first order of the waiting large requests: the smallest log_n,
+// oldest within a size; but once the oldest waiting large request has waited
+// max_wait_ns it goes first.  `pending` is in arrival order.  False when no
+// large request waits.
+bool next_large(const vx_server *s, uint64_t now, uint64_t *tag) {
+    const Request *oldest = nullptr, *best = nullptr;
+    for (const Request &r : s->pending) {
+        if (r.log_n + s->blowup < s->large_log_eval) continue;
+        if (!oldest) oldest = &r;
+        if (!best || r.log_n < best->log_n) best = &r;
+    }
+    if (!oldest) return false;
+    *tag = (s->max_wait_ns && now - oldest->submit_ns >= s->max_wait_ns) ? oldest->tag : best->tag;
+    return true;
+}
+
 void worker_loop(vx_server *s) {
     cudaSetDevice(s->device);
     std::unique_lock<std::mutex> lk(s->mu);
@@ -297,6 +317,9 @@ void worker_loop(vx_server *s) {
             else s->small_inflight--;
             progress = true;
         }
+        // the large request a free large place goes to
+        uint64_t large_tag = 0;
+        bool large_pick = s->smallest_first && !s->large_per_size && next_large(s, now_ns(), &large_tag);
         // admit queued requests, oldest first, skipping ones that cannot start
         // yet.  Requests are addressed by index: submitters append to
         // `pending` while the lock is released for a slot creation (which
@@ -307,6 +330,10 @@ void worker_loop(vx_server *s) {
             const bool large = log_n + s->blowup >= s->large_log_eval;
             if (large && (s->large_per_size ? s->large_by_size[log_n] : s->large_inflight) >= s->max_large) {
                 ++qi;  // a large proof is running: this one waits, smaller ones behind it may start
+                continue;
+            }
+            if (large && large_pick && s->pending[qi].tag != large_tag) {
+                ++qi;  // another large request goes first
                 continue;
             }
             if (!large && s->small_cap && s->large_inflight && s->small_inflight >= s->small_cap) {
@@ -345,6 +372,7 @@ void worker_loop(vx_server *s) {
                     s->stop = true;
                     break;
                 }
+                if (large && large_pick) large_pick = next_large(s, now_ns(), &large_tag);
                 progress = true;
             } else {
                 ++qi;
@@ -399,6 +427,14 @@ extern "C" int vx_server_set_policy(vx_server *s, uint32_t large_log_eval, uint3
     s->split_large = split_large != 0;
     s->prio_mode = priority;
     s->small_cap = small_cap;
+    return VX_OK;
+}
+
+extern "C" int vx_server_set_queue_order(vx_server *s, int smallest_first, uint32_t max_wait_us) {
+    VX_CHECK_ARG(s != nullptr, "vx_server_set_queue_order: null server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->smallest_first = smallest_first != 0;
+    s->max_wait_ns = (uint64_t)max_wait_us * 1000ull;
     return VX_OK;
 }
 

@@ -45,6 +45,12 @@ class ProofServer:
         _lib.check(_lib.lib().vx_server_set_policy(self._s, large_log_eval, max_large, priority, small_cap,
                                                    1 if large_per_size else 0, 1 if split_large else 0))
 
+    def set_queue_order(self, smallest_first: bool = False, max_wait_ms: float = 0.0) -> None:
+        """Order of waiting large proofs: oldest first, or the smallest first
+        with the oldest going first once it has waited max_wait_ms (0 = never)."""
+        _lib.check(_lib.lib().vx_server_set_queue_order(self._s, 1 if smallest_first else 0,
+                                                        int(round(max_wait_ms * 1000))))
+
     def prewarm(self, log_n: int, count: int) -> None:
         _lib.check(_lib.lib().vx_server_prewarm(self._s, log_n, count))
 
