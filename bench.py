@@ -291,6 +291,14 @@ LDE_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the L
                       "profiles/ntt_tile_lde_log24.md. The bottom evaluate pass reads its twiddles, as large as "
                       "the data")
 
+# DRAM bytes of the trace commitment at log_n = 24 (2^26 leaves: leaf subtrees,
+# 16 -> 1 nodes, reduce) from an ncu capture of one proof slot.
+TRACE_COMMIT_TRAFFIC_LOG24 = (269.08e6 + 176.44e6) + (142.33e6 + 18.59e6) + (8.46e6 + 0.0)
+TRACE_COMMIT_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the trace commitment's three launches "
+                               "(leaf_subtree_kernel<LeafM31>, node_subtree_kernel, tree_reduce_kernel<LeafM31>), one "
+                               "proof slot at log_n = 24, one-pass metrics: profiles/merkle_trace_commit_log24.md. "
+                               "Reads: the 2^26 leaf words once, then the stored level of 2^22 hashes")
+
 LIFT_LOGS = [16] * 8 + [18] * 16 + [20] * 10  # 34 columns, blowup 4: LDEs of 2^18 / 2^20 / 2^22
 
 
@@ -487,6 +495,40 @@ def lde_only(log_n: int, steps: int, warmup: int) -> dict:
     peak, _ = _peaks()
     return {"log_n": log_n, "steps": steps, "ms": t, "gbs": (8 * n + 4 * n + 4 * N) / (t / 1e3) / 1e9,
             "frac": (8 * n + 4 * n + 4 * N) / (t / 1e3) / 1e9 / peak}
+
+
+def trace_commit_only(log_n: int, steps: int, warmup: int) -> dict:
+    """The trace commitment of one Fibonacci proof slot (the Blake2s tree of
+    the 2^(log_n+2)-point LDE: leaf-subtree, node and reduce kernels), --steps
+    times inside an NVTX range 'trace_commit' after the warm-up steps; the
+    trace and its LDE are computed once before.  One slot keeps the device
+    footprint small (2.3 GB at log_n = 24)."""
+    import torch
+
+    from vortexstark_b200 import _lib, prover
+
+    L = _lib.lib()
+    cache = prover.ProverCache(log_n)
+    for k in range(3):
+        _lib.check(L.vx_prover_stage_async(cache._p, k, 3, 5, None))
+    ms = []
+    for r in range(warmup + steps):
+        if r == warmup:
+            torch.cuda.nvtx.range_push("trace_commit")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _lib.check(L.vx_prover_stage_async(cache._p, 3, 3, 5, None))
+        e1.record()
+        e1.synchronize()
+        if r >= warmup:
+            ms.append(e0.elapsed_time(e1))
+    torch.cuda.nvtx.range_pop()
+    torch.cuda.synchronize()
+    cache.close()
+    N = 1 << (log_n + 2)
+    t = statistics.median(ms)
+    return {"log_n": log_n, "steps": steps, "ms": t, "compressions": 2 * N - 1,
+            "g_compressions_per_s": (2 * N - 1) / (t / 1e3) / 1e9, "leaf_bytes": 4 * N}
 
 
 def ntt_microbench(peak_gbs: float, sizes=(20, 24, 28), reps: int = 5):
@@ -1084,6 +1126,10 @@ def main():
     ap.add_argument("--lde-only", action="store_true",
                     help="run only the LDE (trace, interpolate, evaluate) of one proof slot, --steps times inside "
                          "an NVTX range 'lde', and print its time (the small case for profiling the NTT passes)")
+    ap.add_argument("--trace-commit-only", action="store_true",
+                    help="run only the trace commitment (Blake2s tree of the LDE) of one proof slot, --steps times "
+                         "inside an NVTX range 'trace_commit', and print its time (the small case for profiling the "
+                         "tree kernels)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -1125,6 +1171,12 @@ def main():
         res = kernel_microbench(peak, probe, log_n=args.kernel_log, cpu=not args.no_cpu_baseline)
         if rank == 0:
             print(json.dumps({"kernel_microbench": res}), flush=True)
+        return
+
+    if args.trace_commit_only:
+        res = trace_commit_only(args.log_n, args.steps, args.warmup)
+        if rank == 0:
+            print(json.dumps({"trace_commit_only": res}), flush=True)
         return
 
     if args.lde_only:
@@ -1335,9 +1387,11 @@ def main():
                          "nominal_source": f"ALU-pipe ceiling: 148 SMs x 64 lanes x {sm_mhz:.0f} MHz (median SM clock "
                                            "of the timed region) / 640 ALU-pipe ops per compression (10 rounds x 8 G x "
                                            "4 xor + 4 rotate; the additions run on the FMA pipe)",
-                         "traffic": None,
-                         "traffic_note": "DRAM reads of the leaf kernel equal the algorithmic bytes (4 B per leaf): "
-                                         "profiles/merkle_leaf_subtree_log20.md"},
+                         "traffic": TRACE_COMMIT_TRAFFIC_LOG24 if log_n == 24 else None,
+                         "traffic_source": TRACE_COMMIT_TRAFFIC_SOURCE,
+                         "algorithmic_bytes": 4 * (1 << (log_n + 2)),
+                         "algorithmic_note": "the leaves read once (4 B each); the stored tree levels written for the "
+                                             "decommitment (32 B per hash at heights 4, 8, ...) are outputs on top"},
             "lde_roofline": {"bound": "hbm",
                              "kernel": f"LDE (interpolate 2^{log_n} + zero-pad + evaluate 2^{log_n + 2})",
                              "achieved": lde_gbs, "peak": peak, "unit": "GB/s", "frac": lde_gbs / peak,
