@@ -17,6 +17,9 @@ P = 0x7FFFFFFF
 
 @pytest.fixture(scope="module")
 def L():
+    # test_no_launch_errors checks the launch errors of this module's tests
+    # only: clear what earlier modules left (some test rejected arguments)
+    _lib.lib().vx_clear_error()
     return _lib.lib()
 
 
