@@ -209,9 +209,10 @@ __global__ void __launch_bounds__(kEvalThreads) eval_chunk_kernel(const uint32_t
 //   value = sum_hi W(hi) sum_lo c[i] w(lo),
 // w(lo) the product of the factors of lo's set bits (bits 0..10) and W(hi)
 // that of hi's (bits 11..), W(hi) = T1[hi mod 2^m1] T2[hi >> m1].  One block
-// builds w, T1 and T2 by doubling; persistent blocks hold w in shared memory,
-// take 2048-coefficient chunks, multiply-accumulate in 64 bits and scale each
-// chunk sum by W(hi); a last launch adds the block sums.
+// builds w, T1 and T2 by doubling and a second launch multiplies them into
+// W(hi) for every chunk; persistent blocks hold w in shared memory, take
+// 2048-coefficient chunks, multiply-accumulate in 64 bits and scale each
+// thread's part of a chunk by W(hi); a last launch adds the block sums.
 constexpr uint32_t kEvTabLog = 11, kEvTabThreads = 1024, kEvAccThreads = 256;
 
 // Block 0 builds w (index bits 0..10), block 1 T1 (bits 11..11+m1-1),
@@ -236,22 +237,40 @@ __global__ void __launch_bounds__(kEvTabThreads) eval_tables_kernel(const uint32
         for (int c = 0; c < 4; c++) out[4 * x + c] = tab[x].v[c];
 }
 
+// W(hi) = T1[hi mod 2^m1] T2[hi >> m1] for every chunk.
+__global__ void eval_wtab_kernel(const uint32_t *__restrict__ t1, const uint32_t *__restrict__ t2, uint32_t m1,
+                                 uint64_t chunks, uint32_t *__restrict__ wtab) {
+    const uint64_t hi = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (hi >= chunks) return;
+    const uint64_t i1 = hi & ((1ull << m1) - 1ull), i2 = hi >> m1;
+    const qm31 r = qmul(qm31{{t1[4 * i1], t1[4 * i1 + 1], t1[4 * i1 + 2], t1[4 * i1 + 3]}},
+                        qm31{{t2[4 * i2], t2[4 * i2 + 1], t2[4 * i2 + 2], t2[4 * i2 + 3]}});
+#pragma unroll
+    for (int k = 0; k < 4; k++) wtab[4 * hi + k] = r.v[k];
+}
+
+// Persistent blocks hold w in shared memory and take 2048-coefficient
+// chunks; each thread multiply-accumulates its 8 coefficients of a chunk in
+// 64 bits, scales that partial sum by the chunk's W(hi) and keeps its own
+// running sum, so chunks need no block-wide step; the block adds its
+// threads' sums once at the end.
 __global__ void __launch_bounds__(kEvAccThreads) eval_accum_kernel(const uint32_t *__restrict__ coeffs,
                                                                    const uint32_t *__restrict__ wlo,
-                                                                   const uint32_t *__restrict__ t1,
-                                                                   const uint32_t *__restrict__ t2, uint32_t m1,
+                                                                   const uint32_t *__restrict__ wtab,
                                                                    uint64_t chunks, uint32_t *__restrict__ partial) {
     __shared__ uint4 w[1u << kEvTabLog];
     __shared__ qm31 red[kEvAccThreads / 32];
     const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
     for (uint32_t x = t; x < (1u << kEvTabLog); x += kEvAccThreads) w[x] = __ldg((const uint4 *)wlo + x);
     __syncthreads();
-    qm31 bacc{{0u, 0u, 0u, 0u}};
+    qm31 acc{{0u, 0u, 0u, 0u}};
     for (uint64_t hi = blockIdx.x; hi < chunks; hi += gridDim.x) {
         const uint32_t *cp = coeffs + (hi << kEvTabLog);
         uint32_t c[8];
 #pragma unroll
         for (int j = 0; j < 8; j++) c[j] = __ldg(cp + t + kEvAccThreads * j);
+        const qm31 W{{__ldg(wtab + 4 * hi), __ldg(wtab + 4 * hi + 1), __ldg(wtab + 4 * hi + 2),
+                      __ldg(wtab + 4 * hi + 3)}};
         // products < 2^62: four of them, or a reduced value and four, stay below 2^64
         uint64_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
 #pragma unroll
@@ -261,34 +280,26 @@ __global__ void __launch_bounds__(kEvAccThreads) eval_accum_kernel(const uint32_
             a0 += (uint64_t)c[j] * q.x; a1 += (uint64_t)c[j] * q.y;
             a2 += (uint64_t)c[j] * q.z; a3 += (uint64_t)c[j] * q.w;
         }
-        qm31 v{{reduce64(a0), reduce64(a1), reduce64(a2), reduce64(a3)}};
-#pragma unroll
-        for (int m = 16; m > 0; m >>= 1) {
-            qm31 o;
-#pragma unroll
-            for (int k = 0; k < 4; k++) o.v[k] = __shfl_xor_sync(0xFFFFFFFFu, v.v[k], m);
-            v = qadd(v, o);
-        }
-        if (lane == 0) red[warp] = v;
-        __syncthreads();
-        if (t == 0) {
-            qm31 sum = red[0];
-            for (uint32_t k = 1; k < kEvAccThreads / 32; k++) sum = qadd(sum, red[k]);
-            const uint64_t i1 = hi & ((1ull << m1) - 1ull), i2 = hi >> m1;
-            const qm31 W = qmul(qm31{{t1[4 * i1], t1[4 * i1 + 1], t1[4 * i1 + 2], t1[4 * i1 + 3]}},
-                                qm31{{t2[4 * i2], t2[4 * i2 + 1], t2[4 * i2 + 2], t2[4 * i2 + 3]}});
-            bacc = qadd(bacc, qmul(sum, W));
-        }
-        __syncthreads();
+        const qm31 v{{reduce64(a0), reduce64(a1), reduce64(a2), reduce64(a3)}};
+        acc = qadd(acc, qmul_mat(qmat_of(W), v));
     }
-    if (t == 0) {
 #pragma unroll
-        for (int k = 0; k < 4; k++) partial[4ull * blockIdx.x + k] = bacc.v[k];
+    for (int m = 16; m > 0; m >>= 1) {
+        qm31 o;
+#pragma unroll
+        for (int k = 0; k < 4; k++) o.v[k] = __shfl_xor_sync(0xFFFFFFFFu, acc.v[k], m);
+        acc = qadd(acc, o);
+    }
+    if (lane == 0) red[warp] = acc;
+    __syncthreads();
+    if (t == 0) {
+        qm31 sum = red[0];
+        for (uint32_t k = 1; k < kEvAccThreads / 32; k++) sum = qadd(sum, red[k]);
+#pragma unroll
+        for (int k = 0; k < 4; k++) partial[4ull * blockIdx.x + k] = sum.v[k];
     }
 }
 
-// Sum of `count` QM31 values (chunk values), or for n < 2^11 the direct sum
-// of c[i] w(i); one block, the total to out[0..4).
 __global__ void __launch_bounds__(kEvalThreads) eval_sum_kernel(const uint32_t *__restrict__ vals, uint64_t count,
                                                                 const uint32_t *__restrict__ coeffs,
                                                                 const uint32_t *__restrict__ factors, uint32_t log_n,
@@ -344,7 +355,18 @@ __global__ void __launch_bounds__(256) barycentric_kernel(const uint32_t *__rest
                                                           uint32_t *__restrict__ out) {
     __shared__ qm31 s[8];
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    qm31 acc{{0u, 0u, 0u, 0u}};
+    // 64-bit multiply-accumulate per coordinate, folded every 4 products:
+    // (x & P) + (x >> 31) < 2^34 plus four products of canonical words
+    // (< 2^62 each) stays below 2^64; reduced to canonical M31 once
+    uint64_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+    auto fold = [&]() {
+        a0 = (a0 & VX_P) + (a0 >> 31); a1 = (a1 & VX_P) + (a1 >> 31);
+        a2 = (a2 & VX_P) + (a2 >> 31); a3 = (a3 & VX_P) + (a3 >> 31);
+    };
+    auto mac = [&](const qm31 &w, uint32_t e) {
+        a0 += (uint64_t)w.v[0] * e; a1 += (uint64_t)w.v[1] * e;
+        a2 += (uint64_t)w.v[2] * e; a3 += (uint64_t)w.v[3] * e;
+    };
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     for (; i + (kBaryInFlight - 1) * stride < n; i += kBaryInFlight * stride) {
         uint32_t e[kBaryInFlight];
@@ -355,9 +377,17 @@ __global__ void __launch_bounds__(256) barycentric_kernel(const uint32_t *__rest
             w[k] = bary_weight<VEC>(weights, i + k * stride);
         }
 #pragma unroll
-        for (int k = 0; k < kBaryInFlight; k++) acc = qadd(acc, qmulm(w[k], e[k]));
+        for (int k = 0; k < kBaryInFlight; k++) {
+            mac(w[k], e[k]);
+            if ((k & 3) == 3) fold();
+        }
     }
-    for (; i < n; i += stride) acc = qadd(acc, qmulm(bary_weight<VEC>(weights, i), __ldg(evals + i)));
+    for (; i < n; i += stride) {
+        mac(bary_weight<VEC>(weights, i), __ldg(evals + i));
+        fold();
+    }
+    fold();
+    qm31 acc{{reduce64(a0), reduce64(a1), reduce64(a2), reduce64(a3)}};
 #pragma unroll
     for (int m = 16; m > 0; m >>= 1) {
         qm31 o;
@@ -514,8 +544,8 @@ void cuda_barycentric_eval(const uint32_t *evals, const uint32_t *weights, uint3
 
 // Scratch as poly_ops.rs allocates it (2n words each).  log_n >= 12 with a
 // 16-byte-aligned d_scratch1: the low-bit table (2^13 words) in d_scratch1,
-// the high-bit tables and block sums (at most 12 n / 2^11 + 4 words) in
-// d_scratch2.  Smaller or unaligned: the chunk fold, which uses at most
+// the high-bit tables, the chunk weights and the block sums (at most
+// 12 n / 2^11 + 8 words) in d_scratch2.  Smaller or unaligned: the chunk fold, which uses at most
 // 4 n / 2^11 + 4 words of d_scratch1.
 void cuda_eval_at_point(const uint32_t *d_coeffs, const uint32_t *d_folding_factors, uint32_t *h_result, uint32_t n,
                         uint32_t *d_scratch1, uint32_t *d_scratch2) {
@@ -534,8 +564,9 @@ void cuda_eval_at_point(const uint32_t *d_coeffs, const uint32_t *d_folding_fact
         eval_sum_kernel<<<1, kEvalThreads>>>(nullptr, 0, d_coeffs, d_folding_factors, log_n, d_scratch1);
     } else if (log_n > kEvTabLog && ((uintptr_t)d_scratch1 & 15u) == 0 && d_scratch2 != nullptr) {
         const uint32_t H = log_n - kEvTabLog, m1 = H < 10u ? H : 10u, m2 = H - m1;
-        uint32_t *wlo = d_scratch1, *t1 = d_scratch2, *t2 = t1 + (4u << m1), *part = t2 + (4u << m2);
         const uint64_t chunks = 1ull << H;
+        uint32_t *wlo = d_scratch1, *t1 = d_scratch2, *t2 = t1 + (4u << m1), *wtab = t2 + (4u << m2),
+                 *part = wtab + 4 * chunks;
         int dev = 0, sms = 0;
         cudaGetDevice(&dev);
         if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) {
@@ -544,7 +575,8 @@ void cuda_eval_at_point(const uint32_t *d_coeffs, const uint32_t *d_folding_fact
         }
         const unsigned grid = (unsigned)(chunks < (uint64_t)sms * 6u ? chunks : (uint64_t)sms * 6u);
         eval_tables_kernel<<<3, kEvTabThreads>>>(d_folding_factors, log_n, m1, m2, wlo, t1, t2);
-        eval_accum_kernel<<<grid, kEvAccThreads>>>(d_coeffs, wlo, t1, t2, m1, chunks, part);
+        eval_wtab_kernel<<<blocks_for(chunks, 256), 256>>>(t1, t2, m1, chunks, wtab);
+        eval_accum_kernel<<<grid, kEvAccThreads>>>(d_coeffs, wlo, wtab, chunks, part);
         eval_sum_kernel<<<1, kEvalThreads>>>(part, grid, nullptr, nullptr, 0, part + 4ull * grid);
         d_scratch1 = part + 4ull * grid;  // where the value lands
     } else {
