@@ -233,9 +233,12 @@ void cuda_barycentric_eval(const uint32_t *evals, const uint32_t *weights, uint3
  * poly_ops.rs:382-443): folds n = 2^k M31 coefficients with the k QM31
  * folding factors (AoS, factor l for level l, level 0 splitting the top
  * index bit: v[t] + f_l v[t + n/2^(l+1)]) into one QM31, written to the
- * HOST array h_result[4].  d_scratch1 holds at least 2n words (the
- * reference's n/2 QM31); d_scratch2 is not used.  Synchronous.  n = 1
- * gives the coefficient; n not a power of two is rejected. */
+ * HOST array h_result[4].  d_scratch1 and d_scratch2 hold 2n words each
+ * (the reference's n/2 QM31) and must not overlap.  For n >= 2^12 with a
+ * 16-byte-aligned d_scratch1 and a non-null d_scratch2: 2^13 words of
+ * d_scratch1 and at most 12 n / 2^11 + 8 words of d_scratch2 are used;
+ * otherwise at most 4 n / 2^11 + 4 words of d_scratch1.  Synchronous.
+ * n = 1 gives the coefficient; n not a power of two is rejected. */
 void cuda_eval_at_point(const uint32_t *d_coeffs, const uint32_t *d_folding_factors, uint32_t *h_result, uint32_t n,
                         uint32_t *d_scratch1, uint32_t *d_scratch2);
 /* replaces cuda_pack_leaves, pack_leaves.cu:44-52: output[c*16 + p][i] =
