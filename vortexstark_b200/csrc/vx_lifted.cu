@@ -14,8 +14,9 @@
 // and both authentication paths.
 //
 // Device work: equal-size columns share each NTT launch (one launch per
-// pass per size), the combination is computed inside the hashing kernels of
-// C's tree, every fold inside the hashing kernels of its layer, and the
+// pass per size), the combination is formed per size group in one launch and
+// lifted inside the hashing kernels of C's tree, every fold inside the
+// hashing kernels of its layer, and the
 // transcript steps inside the kernels that finish each tree.  The whole
 // schedule can be captured once as a CUDA graph.
 #include <cstring>
@@ -110,36 +111,97 @@ __device__ __forceinline__ uint32_t reduce34(uint64_t x) {
     return umin32(r, r - VX_P);
 }
 
-// C[i] = sum_c alpha^c * lift(col_c)[i], computed while C's tree hashes it.
-// Each coordinate is a 64-bit multiply-accumulate of 31-bit products (one
-// IMAD.WIDE per column and coordinate), folded every 3 columns so the sum
-// stays below 2^34 + 3 * 2^62 < 2^64, and reduced to canonical M31 once.
+// C[i] = sum_c alpha^c * lift(col_c)[i] in two steps.  Columns of one size
+// share their lift index, so with G_g = sum over group g's columns of
+// alpha^c * col_c (at the group's own 2^le rows), C[i] = sum_g G_g[lift_g(i)]:
+// combine_groups_kernel forms every G_g at HBM speed (each LDE word read
+// once, where a per-row combination re-reads a lifted column 2^(S-le) times),
+// writing the largest group's (le = S, lift index i) straight into C, and the
+// leaf of C's tree adds the smaller groups' values at their lifted rows,
+// writes the final C and hashes it.
+//
+// Each coordinate of G is a 64-bit multiply-accumulate of 31-bit products
+// (one IMAD.WIDE per column and coordinate), folded every 3 columns so the
+// sum stays below 2^34 + 3 * 2^62 < 2^64, and reduced to canonical M31 once.
+struct CombineGroupsArgs {
+    const uint32_t *lde[kMaxLiftCols];  // group g's first column; column j at + (j << le)
+    uint32_t *dst[kMaxLiftCols];        // group g's G: component k at + k * dstride
+    uint64_t dstride[kMaxLiftCols];
+    uint64_t rows_end[kMaxLiftCols];    // groups' rows laid end to end: group g ends at rows_end[g]
+    uint32_t le[kMaxLiftCols], cnt[kMaxLiftCols], first[kMaxLiftCols];
+    uint32_t n_groups;
+};
+// Four consecutive rows per thread (16-byte loads and stores: every group has
+// at least 8 rows, and columns and destinations are 64-word aligned), three
+// columns' loads in flight, the powers of alpha in shared memory.
+__global__ void __launch_bounds__(256) combine_groups_kernel(const __grid_constant__ CombineGroupsArgs a,
+                                                             const uint32_t *__restrict__ pw) {
+    __shared__ uint4 spw[kMaxLiftCols];
+    pdl_wait();
+    for (uint32_t c = threadIdx.x; c < kMaxLiftCols; c += blockDim.x) spw[c] = __ldg((const uint4 *)pw + c);
+    __syncthreads();
+    const uint64_t r = 4ull * ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x);
+    if (r >= a.rows_end[a.n_groups - 1]) return;
+    uint32_t g = 0;
+    while (r >= a.rows_end[g]) g++;
+    const uint64_t row = r - (g ? a.rows_end[g - 1] : 0ull);
+    const uint32_t cnt = a.cnt[g], first = a.first[g];
+    const uint64_t cs4 = 1ull << (a.le[g] - 2u);  // column stride in 16-byte units
+    const uint4 *cp = (const uint4 *)(a.lde[g] + row);
+    uint64_t s[4][4];  // [row][coordinate]
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) s[k][c] = 0;
+    auto mac = [&](const uint4 v, const uint4 p) {
+        const uint32_t vv[4] = {v.x, v.y, v.z, v.w}, pp[4] = {p.x, p.y, p.z, p.w};
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) s[k][c] += (uint64_t)pp[c] * vv[k];
+    };
+    auto fold = [&]() {
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) s[k][c] = fold64(s[k][c]);
+    };
+    uint32_t j = 0;
+    for (; j + 3u <= cnt; j += 3u) {
+        const uint4 v0 = __ldg(cp + j * cs4), v1 = __ldg(cp + (j + 1u) * cs4), v2 = __ldg(cp + (j + 2u) * cs4);
+        mac(v0, spw[first + j]);
+        mac(v1, spw[first + j + 1u]);
+        mac(v2, spw[first + j + 2u]);
+        fold();
+    }
+    for (; j < cnt; j++) mac(__ldg(cp + j * cs4), spw[first + j]);  // at most two more
+    fold();
+    uint32_t *d = a.dst[g] + row;
+    const uint64_t ds = a.dstride[g];
+#pragma unroll
+    for (int c = 0; c < 4; c++)
+        *(uint4 *)(d + c * ds) = make_uint4(reduce34(s[0][c]), reduce34(s[1][c]), reduce34(s[2][c]), reduce34(s[3][c]));
+}
+
+// Leaf of C's tree: the largest group's G (already in C) plus the smaller
+// groups' G at their lifted rows; writes the final C and hashes it.
 struct LeafCombine {
-    static constexpr bool kPlainAdds = true;  // 4 x n_cols wide multiplies per leaf
-    LeafLifted cols;
-    const uint32_t *pw;  // alpha^c as 4 words each
+    const uint32_t *g[kMaxLiftCols];  // smaller groups' G: component k at + k * gstride
+    uint64_t gstride[kMaxLiftCols];
+    uint32_t gshift[kMaxLiftCols];    // S - le + 1
+    uint32_t n_small;
     uint32_t *o0, *o1, *o2, *o3;
     __device__ __forceinline__ void init() {}
     __device__ __forceinline__ uint32_t load(uint64_t i, uint32_t m[16]) const {
-        uint64_t s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-        const uint32_t nc = cols.n_cols;
-        auto mac = [&](uint32_t c) {
-            const uint32_t v = cols.word(c, i);
-            const uint4 p = __ldg((const uint4 *)pw + c);
-            s0 += (uint64_t)p.x * v; s1 += (uint64_t)p.y * v;
-            s2 += (uint64_t)p.z * v; s3 += (uint64_t)p.w * v;
-        };
-        // three products (< 2^62 each) on a folded sum (< 2^34) stay below 2^64
-        uint32_t c = 0;
-        for (; c + 3u <= nc; c += 3u) {
-            mac(c); mac(c + 1u); mac(c + 2u);
-            s0 = fold64(s0); s1 = fold64(s1); s2 = fold64(s2); s3 = fold64(s3);
+        qm31 a{{o0[i], o1[i], o2[i], o3[i]}};
+        const uint32_t i32 = (uint32_t)i;
+        for (uint32_t k = 0; k < n_small; k++) {
+            const uint32_t *gp = g[k] + (((i32 >> gshift[k]) << 1) | (i32 & 1u));
+            const uint64_t gs = gstride[k];
+            a = qadd(a, qm31{{__ldg(gp), __ldg(gp + gs), __ldg(gp + 2 * gs), __ldg(gp + 3 * gs)}});
         }
-        for (; c < nc; c++) mac(c);  // at most two more
-        s0 = fold64(s0); s1 = fold64(s1); s2 = fold64(s2); s3 = fold64(s3);
-        const uint32_t a0 = reduce34(s0), a1 = reduce34(s1), a2 = reduce34(s2), a3 = reduce34(s3);
-        o0[i] = a0; o1[i] = a1; o2[i] = a2; o3[i] = a3;
-        m[0] = a0; m[1] = a1; m[2] = a2; m[3] = a3;
+        o0[i] = a.v[0]; o1[i] = a.v[1]; o2[i] = a.v[2]; o3[i] = a.v[3];
+        m[0] = a.v[0]; m[1] = a.v[1]; m[2] = a.v[2]; m[3] = a.v[3];
         return 16u;
     }
 };
@@ -309,6 +371,7 @@ struct vx_lifted {
     uint32_t *fold_circle = nullptr, *fold_line = nullptr;
     uint64_t fold_line_off[32];
     uint32_t *C[4];
+    uint32_t *G[kMaxLiftCols];  // combined codeword of each size group but the largest (4 components)
     uint32_t *F[kMaxFri][4];
     TreeLevels lv0, lv1, flv[kMaxFri];
     DevChannel *chan = nullptr;
@@ -376,9 +439,33 @@ int lift_stage(vx_lifted *h, uint32_t stage, cudaStream_t st, uint32_t *launches
         break;
     case 2: {  // C = sum alpha^c lift(col_c), committed; draw the first fold challenge
         powers_kernel<<<1, 32, 0, st>>>(h->alpha, h->pw, L.n_cols);
-        LeafCombine lc{h->cols, h->pw, h->C[0], h->C[1], h->C[2], h->C[3]};
+        CombineGroupsArgs ca;
+        memset(&ca, 0, sizeof(ca));
+        LeafCombine lc;
+        memset(&lc, 0, sizeof(lc));
+        uint64_t rows = 0;
+        for (uint32_t g = 0; g < h->n_groups; g++) {
+            const uint32_t le = h->glog[g] + B;
+            const bool top = g + 1 == h->n_groups;  // le == S
+            ca.lde[g] = h->lde[g];
+            ca.dst[g] = top ? h->C[0] : h->G[g];
+            ca.dstride[g] = top ? align64(1ull << S) : align64(1ull << le);
+            rows += 1ull << le;
+            ca.rows_end[g] = rows;
+            ca.le[g] = le; ca.cnt[g] = h->gcnt[g]; ca.first[g] = h->gfirst[g];
+            if (!top) {
+                lc.g[lc.n_small] = h->G[g];
+                lc.gstride[lc.n_small] = align64(1ull << le);
+                lc.gshift[lc.n_small] = S - le + 1u;
+                lc.n_small++;
+            }
+        }
+        ca.n_groups = h->n_groups;
+        VX_CUDA_TRY(launch_pdl(combine_groups_kernel, dim3(blocks_for(rows / 4, 256)), dim3(256), 0, st, ca,
+                               (const uint32_t *)h->pw));
+        lc.o0 = h->C[0]; lc.o1 = h->C[1]; lc.o2 = h->C[2]; lc.o3 = h->C[3];
         VX_CUDA_TRY(tree_build(lc, h->lv1, ChanStep{h->chan, proof + L.r1, h->alpha_f}, st));
-        *launches += 1 + tree_launches(h->lv1);
+        *launches += 2 + tree_launches(h->lv1);
         break;
     }
     case 3: {  // circle fold of C (stwo twiddles) into FRI layer 0
@@ -510,6 +597,8 @@ extern "C" int vx_lifted_create(uint32_t n_cols, const uint32_t *log_sizes, uint
     const uint64_t o_fl = w;
     for (uint32_t l = S - 1; l >= 4; l--) { h->fold_line_off[l] = w - o_fl; w += align64(1ull << (l - 1)); }
     uint64_t o_C = w; w += 4 * align64(1ull << S);
+    uint64_t o_G[kMaxLiftCols];
+    for (uint32_t g = 0; g + 1 < h->n_groups; g++) { o_G[g] = w; w += 4 * align64(1ull << (h->glog[g] + B)); }
     uint64_t o_F[kMaxFri];
     for (uint32_t k = 0; k < L.nfri; k++) { o_F[k] = w; w += 4 * align64(1ull << (S - 1 - k)); }
     // leaf-kernel shapes read once: the pools are sized and carved with them
@@ -542,6 +631,7 @@ extern "C" int vx_lifted_create(uint32_t n_cols, const uint32_t *log_sizes, uint
     h->fold_circle = b + o_fc;
     h->fold_line = b + o_fl;
     for (int c = 0; c < 4; c++) h->C[c] = b + o_C + c * align64(1ull << S);
+    for (uint32_t g = 0; g + 1 < h->n_groups; g++) h->G[g] = b + o_G[g];
     for (uint32_t k = 0; k < L.nfri; k++)
         for (int c = 0; c < 4; c++) h->F[k][c] = b + o_F[k] + c * align64(1ull << (S - 1 - k));
     tree_plan(S, b + o_t0, &h->lv0, kt);
