@@ -314,9 +314,10 @@ def batched_commit_benchmark(seed: int, steps: int, warmup: int, peak_gbs: float
     """Batched lifted commitment of uneven-size columns (34 M31 columns,
     8 x 2^16, 16 x 2^18, 10 x 2^20, blowup 4, one lifted tree with S = 22,
     a random QM31 combination folded by FRI, 80 queries), replayed as one
-    CUDA graph.  Device-resident throughput, end-to-end throughput with the
-    columns uploaded from pinned host memory and the words read back every
-    step, per-stage times and the two rooflines."""
+    CUDA graph.  Device-resident throughput (two commitments in flight on two
+    contexts, and one at a time), end-to-end throughput with the columns
+    uploaded from pinned host memory and the words read back every step,
+    per-stage times and the two rooflines."""
     import torch
 
     from vortexstark_b200.lifted import LiftedCommitter
@@ -380,6 +381,20 @@ def batched_commit_benchmark(seed: int, steps: int, warmup: int, peak_gbs: float
     p1.synchronize()
     pipe_ms = p0.elapsed_time(p1) / (2 * steps)
     pipe_equal = com.result_bytes() == com2.result_bytes()
+    # device-resident with two commitments in flight (the two contexts on
+    # their two streams, no uploads): one's latency-bound FRI tail overlaps
+    # the other's hashing
+    q0, q1, k2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    q0.record(st)
+    st2.wait_event(q0)
+    for i in range(2 * steps):
+        c, t = ctx[i % 2]
+        c.commit_async(t.cuda_stream, graph=True)
+    k2.record(st2)
+    st.wait_event(k2)
+    q1.record(st)
+    q1.synchronize()
+    dev2_ms = q0.elapsed_time(q1) / (2 * steps)
     com2.close()
     # per-stage device times
     names = ["lde", "lifted_tree", "combination_tree", "circle_fold", "line_folds", "queries", "openings"]
@@ -404,7 +419,9 @@ def batched_commit_benchmark(seed: int, steps: int, warmup: int, peak_gbs: float
         "workload": "lifted commitment: 34 M31 columns (8 x 2^16, 16 x 2^18, 10 x 2^20), blowup 4, "
                     "one lifted Blake2s tree (2^22 leaves of 34 words), QM31 combination + FRI to 8 values, "
                     "80 queries; one CUDA graph per commitment",
-        "value": 1e3 / dev_ms, "unit": "commitments/s", "ms_per_commit": dev_ms,
+        "value": 1e3 / dev2_ms, "unit": "commitments/s", "ms_per_commit": dev2_ms,
+        "in_flight": "two commitments: two contexts on two streams, graph replays, CUDA events around the loop",
+        "value_one_in_flight": 1e3 / dev_ms, "ms_per_commit_one_in_flight": dev_ms,
         "e2e": {"value": 1e3 / pipe_ms, "unit": "commitments/s", "ms_per_commit": pipe_ms,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": com.size,
                 "how": "two contexts on two streams, CUDA events around the loop: each commitment uploads its 34 "
