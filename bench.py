@@ -310,12 +310,12 @@ def lifted_workload(seed: int, logs=None):
 
 
 def batched_commit_benchmark(seed: int, steps: int, warmup: int, peak_gbs: float, probe_rate: float,
-                             cpu: bool = True):
+                             cpu: bool = True, contexts: int = 4):
     """Batched lifted commitment of uneven-size columns (34 M31 columns,
     8 x 2^16, 16 x 2^18, 10 x 2^20, blowup 4, one lifted tree with S = 22,
     a random QM31 combination folded by FRI, 80 queries), replayed as one
-    CUDA graph.  Device-resident throughput (two commitments in flight on two
-    contexts, and one at a time), end-to-end throughput with the columns
+    CUDA graph.  Device-resident throughput (`contexts` commitments in flight,
+    and one at a time), end-to-end throughput with the columns
     uploaded from pinned host memory and the words read back every step,
     per-stage times and the two rooflines."""
     import torch
@@ -355,47 +355,45 @@ def batched_commit_benchmark(seed: int, steps: int, warmup: int, peak_gbs: float
         lat.append(a.elapsed_time(b))
     com.result_bytes()
     e2e_ms = statistics.median(lat)
-    # end to end with two commitments in flight: a second context on a second
-    # stream, so one commitment's column upload (copy engine) overlaps the
-    # other's device work; every commitment still uploads all its columns and
-    # reads its words back inside the timed region
-    com2 = LiftedCommitter(LIFT_LOGS, 2, 80)
-    st2 = torch.cuda.Stream()
-    ctx = [(com, st), (com2, st2)]
-    for c, t in ctx:
-        c.upload_async(ptrs, t.cuda_stream)
-        c.commit_async(t.cuda_stream, graph=True)
-        c.fetch_async(t.cuda_stream)
-    torch.cuda.synchronize()
-    p0, p1, j2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
-    p0.record(st)
-    st2.wait_event(p0)
-    for i in range(2 * steps):
-        c, t = ctx[i % 2]
-        c.upload_async(ptrs, t.cuda_stream)
-        c.commit_async(t.cuda_stream, graph=True)
-        c.fetch_async(t.cuda_stream)
-    j2.record(st2)
-    st.wait_event(j2)
-    p1.record(st)
-    p1.synchronize()
-    pipe_ms = p0.elapsed_time(p1) / (2 * steps)
-    pipe_equal = com.result_bytes() == com2.result_bytes()
-    # device-resident with two commitments in flight (the two contexts on
-    # their two streams, no uploads): one's latency-bound FRI tail overlaps
-    # the other's hashing
-    q0, q1, k2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
-    q0.record(st)
-    st2.wait_event(q0)
-    for i in range(2 * steps):
-        c, t = ctx[i % 2]
-        c.commit_async(t.cuda_stream, graph=True)
-    k2.record(st2)
-    st.wait_event(k2)
-    q1.record(st)
-    q1.synchronize()
-    dev2_ms = q0.elapsed_time(q1) / (2 * steps)
-    com2.close()
+    # several commitments in flight: more contexts, each on its own stream,
+    # taken in turn.  End to end, one commitment's column upload (copy
+    # engine) overlaps the others' device work; every commitment still
+    # uploads all its columns and reads its words back inside the timed region
+    extra = [LiftedCommitter(LIFT_LOGS, 2, 80) for _ in range(contexts - 1)]
+    ctx = [(com, st)] + [(c, torch.cuda.Stream()) for c in extra]
+
+    def in_flight(upload: bool) -> float:
+        for c, t in ctx:
+            c.upload_async(ptrs, t.cuda_stream)
+            c.commit_async(t.cuda_stream, graph=True)
+            c.fetch_async(t.cuda_stream)
+        torch.cuda.synchronize()
+        q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        q0.record(st)
+        for _, t in ctx[1:]:
+            t.wait_event(q0)
+        for i in range(contexts * steps):
+            c, t = ctx[i % contexts]
+            if upload:
+                c.upload_async(ptrs, t.cuda_stream)
+            c.commit_async(t.cuda_stream, graph=True)
+            if upload:
+                c.fetch_async(t.cuda_stream)
+        for _, t in ctx[1:]:
+            j = torch.cuda.Event()
+            j.record(t)
+            st.wait_event(j)
+        q1.record(st)
+        q1.synchronize()
+        return q0.elapsed_time(q1) / (contexts * steps)
+
+    pipe_ms = in_flight(True)
+    pipe_equal = all(c.result_bytes() == com.result_bytes() for c, _ in ctx[1:])
+    # device-resident (no uploads): one's latency-bound FRI tail overlaps the
+    # others' hashing
+    dev2_ms = in_flight(False)
+    for c in extra:
+        c.close()
     # per-stage device times
     names = ["lde", "lifted_tree", "combination_tree", "circle_fold", "line_folds", "queries", "openings"]
     reps = 3
@@ -420,12 +418,13 @@ def batched_commit_benchmark(seed: int, steps: int, warmup: int, peak_gbs: float
                     "one lifted Blake2s tree (2^22 leaves of 34 words), QM31 combination + FRI to 8 values, "
                     "80 queries; one CUDA graph per commitment",
         "value": 1e3 / dev2_ms, "unit": "commitments/s", "ms_per_commit": dev2_ms,
-        "in_flight": "two commitments: two contexts on two streams, graph replays, CUDA events around the loop",
+        "in_flight": f"{contexts} commitments: {contexts} contexts on {contexts} streams taken in turn, graph "
+                     "replays, CUDA events around the loop",
         "value_one_in_flight": 1e3 / dev_ms, "ms_per_commit_one_in_flight": dev_ms,
         "e2e": {"value": 1e3 / pipe_ms, "unit": "commitments/s", "ms_per_commit": pipe_ms,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": com.size,
-                "how": "two contexts on two streams, CUDA events around the loop: each commitment uploads its 34 "
-                       "columns from pinned memory, commits and reads its words back",
+                "how": f"{contexts} contexts on {contexts} streams, CUDA events around the loop: each commitment "
+                       "uploads its 34 columns from pinned memory, commits and reads its words back",
                 "latency_ms": e2e_ms, "latency_how": "one commitment alone: upload, commit, read back (CUDA events)",
                 "contexts_bytes_equal": pipe_equal},
         "launches_per_commit": com.launches(), "device_bytes": com.device_bytes(),
