@@ -189,6 +189,8 @@ def _cols(seed, logs):
     ([2], 2, 8), ([3, 3], 1, 5), ([4, 4, 6], 2, 16), ([2, 5, 7], 3, 33), ([6] * 8, 2, 80),
     ([8] * 8 + [10] * 16 + [12] * 10, 2, 80),
     ([5] * 17 + [9] * 20, 2, 40),
+    # the smallest size group (8 LDE rows), and eight size groups in the group combination
+    ([2, 2, 3], 1, 6), ([2, 3, 4, 5, 6, 7, 8, 9], 2, 20),
     # size groups of 15..21 layers share one NTT launch per pass (up to four groups per launch); the others
     # run on their own: all merged, mixed, and more mergeable groups than one launch takes
     ([15] * 2 + [17] * 3 + [19] * 2, 2, 40),
